@@ -1,0 +1,155 @@
+/*
+ * radio_gridders.h — C ABI of the B200-native radio imager.
+ *
+ * Plain C: pointers, sizes and status codes only.  Every buffer argument may be
+ * a host pointer (pageable or pinned) or a CUDA device pointer; the library
+ * detects which (cudaPointerGetAttributes) and stages host buffers through the
+ * context's device memory.  Results are identical either way.
+ *
+ * The reference (KentJames/Radio-Gridders) has no library API: its paths sit
+ * behind CLI binaries and the host wrappers declared in
+ * src/grid/grid_common.cuh:45-64 and src/dft/dft_common.cuh:12-18, plus the CPU
+ * functions of src/reference/grid.h:113-137.  Each entry point below names the
+ * reference interface it replaces.  Differences from those interfaces:
+ *   - inputs are in-memory arrays, not file names (the crocodile HDF5 readers
+ *     are separate entry points: rg_hdf5_*);
+ *   - errors are returned as rg_status (never exit(), unlike
+ *     src/common/radio.cuh:27-43), with a thread-local message in
+ *     rg_last_error();
+ *   - nothing is leaked: device scratch lives in the context and is reused.
+ *
+ * Threading: a context belongs to one host thread at a time; calls on one
+ * context are serialised on its CUDA stream.  Different contexts are
+ * independent.
+ */
+#ifndef RADIO_GRIDDERS_H
+#define RADIO_GRIDDERS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum rg_status {
+    RG_OK = 0,
+    RG_ERR_INVALID_ARGUMENT = 1, /* bad sizes, NULL pointers, data outside the grid/kernel */
+    RG_ERR_CUDA = 2,             /* a CUDA runtime call failed */
+    RG_ERR_OUT_OF_MEMORY = 3,
+    RG_ERR_UNSUPPORTED = 4,      /* valid request outside this build's limits */
+    RG_ERR_IO = 5,               /* file missing or not in the expected format */
+    RG_ERR_NO_DEVICE = 6
+} rg_status;
+
+typedef struct rg_context rg_context;
+
+/* Flat visibilities: the reference's struct flat_vis_data
+ * (src/common/hdf5.cuh:31-37), produced by flatten_visibilities_CUDA
+ * (src/common/hdf5.c:827-872).  u, v, w in wavelengths; vis interleaved
+ * (re, im) float64, 2*n doubles. */
+typedef struct rg_vis {
+    const double *u;
+    const double *v;
+    const double *w;
+    const double *vis;
+    int64_t n;
+} rg_vis;
+
+/* Oversampled w-kernel table: struct w_kernel_data (src/reference/grid.h:34-49)
+ * with kern_by_w flattened.  data holds plane_count*ov*ov*size*size complex
+ * float64 taps (interleaved), index
+ * ((plane*ov + yf)*ov + xf)*size*size + y*size + x  (src/reference/grid.c:53-56);
+ * plane p is used for w nearest w_min + p*w_step (grid.c:168-170). */
+typedef struct rg_wkern {
+    const double *data;
+    int plane_count;
+    int size;
+    int oversampling;
+    double w_min;
+    double w_step;
+} rg_wkern;
+
+/* rg_grid_* flags */
+#define RG_GRID_ACCUMULATE 0 /* uvgrid += gridded visibilities (grid.c semantics) */
+#define RG_GRID_OVERWRITE 1  /* uvgrid  = gridded visibilities (prior contents ignored) */
+
+/* rg_dft_image precision modes (the precision study) */
+#define RG_DFT_FP32_NAIVE 0  /* phase argument and sincos in FP32 */
+#define RG_DFT_FP64_REDUCED 1 /* per-tile phase reduced in FP64, FP32 increments */
+#define RG_DFT_FP64 2        /* all FP64 */
+
+/* ---- context ----------------------------------------------------------- */
+
+/* Replaces the device selection and setup of src/grid/grid.cpp:161-165
+ * (-device) and src/dft/dft.cpp.  Creates a context on `device`. */
+rg_status rg_context_create(int device, rg_context **ctx);
+rg_status rg_context_destroy(rg_context *ctx);
+/* Use the caller's cudaStream_t (passed as void*) for subsequent calls; NULL
+ * restores the context's own stream. */
+rg_status rg_context_set_stream(rg_context *ctx, void *cuda_stream);
+/* Message describing the last failed call on this host thread. */
+const char *rg_last_error(void);
+/* Statistics of the last gridding call on this context: element 0 number of
+ * visibilities gridded, 1 active (tower, floor) sub-grids, 2 towers with data,
+ * 3 w-floors spanned, 4 visibilities dropped for lying outside every tower
+ * (cf. the per-baseline check at src/reference/grid.c:519-530), 5 kernel
+ * launches issued by the call.  Returns the count written (<= n). */
+int rg_last_stats(rg_context *ctx, int64_t *out, int n);
+
+/* ---- gridders ---------------------------------------------------------- */
+
+/* W-projection, Romein scatter.  Replaces grid_wprojection
+ * (src/reference/grid.h:121-122, grid.c:187-202) and the GPU wrapper
+ * wproj_CUDA_flat (src/grid/grid_common.cuh:59-62, grid_cuda.cu:826-921) up to
+ * the FFT.  uvgrid: grid_size*grid_size complex float64 (interleaved). */
+rg_status rg_grid_wprojection(rg_context *ctx, double *uvgrid, int grid_size, double theta,
+                              const rg_vis *vis, const rg_wkern *wkern, int flags);
+
+/* W-towers.  Replaces grid_wtowers (src/reference/grid.h:123-126,
+ * grid.c:295-555) and the GPU wrapper wtowers_CUDA_flat
+ * (src/grid/grid_common.cuh:52-55, grid_cuda.cu:522-744) up to the final FFT:
+ * the master uv grid after add-back, FP64. */
+rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double theta,
+                          const rg_vis *vis, const rg_wkern *wkern, int subgrid_size,
+                          int subgrid_margin, double wincrement, int flags);
+
+/* Uniform weighting: vis_out[i] = vis[i] / (visibilities in its nearest cell).
+ * Replaces weight() (src/reference/grid.h:116-117, grid.c:59-81) as called by
+ * src/reference/main.c:153.  vis_out: 2*n doubles (may alias vis->vis). */
+rg_status rg_weight(rg_context *ctx, int grid_size, double theta, const rg_vis *vis,
+                    double *vis_out);
+
+/* ---- image formation --------------------------------------------------- */
+
+/* make_hermitian (src/reference/grid.h:135, grid.c:639-662), in place. */
+rg_status rg_make_hermitian(rg_context *ctx, double *uvgrid, int grid_size);
+/* fft_shift (src/reference/grid.h:136, grid.c:665-680), in place. */
+rg_status rg_fft_shift(rg_context *ctx, double *uvgrid, int grid_size);
+/* Dirty image from a uv grid: make_hermitian, fft_shift, 2-D FFT (sign -1),
+ * fft_shift, real part (src/reference/main.c:258-294).  uvgrid is consumed
+ * (overwritten); image_out: grid_size*grid_size float64.  If
+ * taper_1d != NULL the image is divided by taper_1d[x]*taper_1d[y] (grid
+ * correction; the reference applies none). */
+rg_status rg_image_from_grid(rg_context *ctx, double *uvgrid, int grid_size,
+                             double *image_out, const double *taper_1d);
+/* Batched 2-D complex FFT (unnormalised, sign -1 or +1), the project's own
+ * kernels; exposed so they can be checked against cuFFT.  data: batch*ny*nx
+ * complex, float32 (complex_bytes 8) or float64 (complex_bytes 16). */
+rg_status rg_fft2d(rg_context *ctx, void *data, int batch, int ny, int nx, int sign,
+                   int complex_bytes);
+
+/* ---- direct DFT -------------------------------------------------------- */
+
+/* Direct Fourier transform image.  Replaces image_dft_host_flat
+ * (src/dft/dft_common.cuh:16-18, dft_cuda.cu:170-223) with the defects of
+ * src/dft/dft_cuda.cu:55-57 and :98-112 removed:
+ *   image[y][x] = factor * sum_k Re(V_k exp(-2 pi i (u_k l + v_k m + w_k (1 - n))))
+ *   l = theta (x - N/2)/N, m = theta (y - N/2)/N, n = sqrt(1 - l^2 - m^2).
+ * factor 2 matches the hermitian gridder pipeline, 1 the reference dft.out. */
+rg_status rg_dft_image(rg_context *ctx, double *image_out, int grid_size, double theta,
+                       const rg_vis *vis, int precision, double factor);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RADIO_GRIDDERS_H */

@@ -1,0 +1,293 @@
+"""ORACLE — test infrastructure, not the product.
+
+Only tests/, __graft_entry__.smoke() and bench.py (its CPU-baseline leg and its
+``--impl reference`` arm) import this package, and only as the checker.
+
+Two CPU implementations of the reference gridder are exposed through ctypes:
+
+* ``restated``: oracle/rg_oracle.c, a plain-C FP64 restatement of
+  src/reference/grid.c on flat visibility arrays, plus the FP64 DFT oracle;
+* ``reference``: the reference's own src/reference/grid.c compiled from its
+  sources here (oracle/Makefile -> oracle/_ref/libref_grid.so, IEEE build;
+  libref_grid_omp.so with the reference's flags and -DOMP_TOWERS for timing),
+  driven through in-memory struct vis_data / struct w_kernel_data mirrors of
+  src/reference/grid.h:7-49.
+
+Parity pin: tests/test_oracle_pin.py checks ``restated`` == ``reference``
+bit-for-bit; tests/golden/ holds fixtures produced by ``reference``.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD = os.path.join(HERE, "_build")
+REF = os.path.join(HERE, "_ref")
+REFERENCE_SRC = "/root/reference/src/reference"
+
+_c_double_p = ct.POINTER(ct.c_double)
+
+
+def build(reference: bool = True) -> None:
+    """Compile the restatement (always) and the reference build (when the
+    reference sources are present on this machine)."""
+    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+    if reference and os.path.isdir(REFERENCE_SRC):
+        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ct.c_void_p)
+
+
+# --------------------------------------------------------------------------
+# restatement
+# --------------------------------------------------------------------------
+
+class _Wk(ct.Structure):
+    _fields_ = [("data", ct.c_void_p), ("plane_count", ct.c_int), ("size", ct.c_int),
+                ("oversampling", ct.c_int), ("w_min", ct.c_double), ("w_step", ct.c_double)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(BUILD, "librgoracle.so")
+        if not os.path.exists(path):
+            build(reference=False)
+        L = ct.CDLL(path)
+        i64, vp, d, i = ct.c_int64, ct.c_void_p, ct.c_double, ct.c_int
+        L.rgo_grid_wprojection.argtypes = [vp, i, d, i64, vp, vp, vp, vp, ct.POINTER(_Wk)]
+        L.rgo_grid_wprojection.restype = ct.c_uint64
+        L.rgo_grid_wtowers.argtypes = [vp, i, d, i64, vp, vp, vp, vp, ct.POINTER(_Wk), i, i, d, vp]
+        L.rgo_grid_wtowers.restype = ct.c_uint64
+        L.rgo_weight.argtypes = [i, d, i64, vp, vp, vp]
+        L.rgo_make_hermitian.argtypes = [vp, i]
+        L.rgo_fft_shift.argtypes = [vp, i]
+        L.rgo_image_from_grid.argtypes = [vp, i, vp]
+        L.rgo_dft_image.argtypes = [vp, i, d, i64, vp, vp, vp, vp, d]
+        L.rgo_frac_coord.argtypes = [i, i, i, d, d, d, d, d, ct.POINTER(i), ct.POINTER(i)]
+        _lib = L
+    return _lib
+
+
+def _wk_struct(wk):
+    data = np.ascontiguousarray(wk.data, dtype=np.complex128)
+    s = _Wk(data.ctypes.data, wk.plane_count, wk.size, wk.oversampling, wk.w_min, wk.w_step)
+    return s, data
+
+
+def _flat(u, v, w, vis):
+    return (np.ascontiguousarray(u, np.float64), np.ascontiguousarray(v, np.float64),
+            np.ascontiguousarray(w, np.float64), np.ascontiguousarray(vis, np.complex128))
+
+
+def grid_wprojection(grid_size, theta, u, v, w, vis, wk):
+    u, v, w, vis = _flat(u, v, w, vis)
+    grid = np.zeros((grid_size, grid_size), np.complex128)
+    s, keep = _wk_struct(wk)
+    lib().rgo_grid_wprojection(_ptr(grid), grid_size, theta, len(u), _ptr(u), _ptr(v),
+                               _ptr(w), _ptr(vis), ct.byref(s))
+    return grid
+
+
+def grid_wtowers(grid_size, theta, u, v, w, vis, wk, subgrid, margin, winc,
+                 return_counts=False):
+    u, v, w, vis = _flat(u, v, w, vis)
+    grid = np.zeros((grid_size, grid_size), np.complex128)
+    s, keep = _wk_struct(wk)
+    counts = np.zeros(len(u), np.int32)
+    lib().rgo_grid_wtowers(_ptr(grid), grid_size, theta, len(u), _ptr(u), _ptr(v),
+                           _ptr(w), _ptr(vis), ct.byref(s), subgrid, margin, winc,
+                           _ptr(counts))
+    return (grid, counts) if return_counts else grid
+
+
+def weight(grid_size, theta, u, v, vis):
+    u, v, _, vis = _flat(u, v, u, vis)
+    out = vis.copy()
+    lib().rgo_weight(grid_size, theta, len(u), _ptr(u), _ptr(v), _ptr(out))
+    return out
+
+
+def make_hermitian(grid):
+    g = np.ascontiguousarray(grid, np.complex128).copy()
+    lib().rgo_make_hermitian(_ptr(g), g.shape[0])
+    return g
+
+
+def fft_shift(grid):
+    g = np.ascontiguousarray(grid, np.complex128).copy()
+    lib().rgo_fft_shift(_ptr(g), g.shape[0])
+    return g
+
+
+def image_from_grid(grid):
+    g = np.ascontiguousarray(grid, np.complex128).copy()
+    img = np.zeros(g.shape, np.float64)
+    lib().rgo_image_from_grid(_ptr(g), g.shape[0], _ptr(img))
+    return img
+
+
+def dft_image(grid_size, theta, u, v, w, vis, factor=2.0):
+    u, v, w, vis = _flat(u, v, w, vis)
+    img = np.zeros((grid_size, grid_size), np.float64)
+    lib().rgo_dft_image(_ptr(img), grid_size, theta, len(u), _ptr(u), _ptr(v), _ptr(w),
+                        _ptr(vis), factor)
+    return img
+
+
+def frac_coord(grid_size, ksize, ov, theta, u, v, du=0.0, dv=0.0):
+    go, so = ct.c_int(), ct.c_int()
+    lib().rgo_frac_coord(grid_size, ksize, ov, theta, u, v, du, dv, ct.byref(go), ct.byref(so))
+    return go.value, so.value
+
+
+# --------------------------------------------------------------------------
+# the reference's own grid.c (struct mirrors of src/reference/grid.h:7-49)
+# --------------------------------------------------------------------------
+
+class BlData(ct.Structure):
+    _fields_ = [("antenna1", ct.c_int), ("antenna2", ct.c_int),
+                ("time_count", ct.c_int), ("freq_count", ct.c_int),
+                ("time", _c_double_p), ("freq", _c_double_p), ("uvw", _c_double_p),
+                ("vis", ct.c_void_p), ("awkern", ct.c_void_p),
+                ("u_min", ct.c_double), ("u_max", ct.c_double),
+                ("v_min", ct.c_double), ("v_max", ct.c_double),
+                ("w_min", ct.c_double), ("w_max", ct.c_double),
+                ("t_min", ct.c_double), ("t_max", ct.c_double),
+                ("f_min", ct.c_double), ("f_max", ct.c_double),
+                ("flops", ct.c_uint64)]
+
+
+class VisData(ct.Structure):
+    _fields_ = [("antenna_count", ct.c_int), ("bl_count", ct.c_int),
+                ("bl", ct.POINTER(BlData))]
+
+
+class WKern(ct.Structure):
+    _fields_ = [("data", ct.c_void_p), ("w", ct.c_double)]
+
+
+class WKernData(ct.Structure):
+    _fields_ = [("plane_count", ct.c_int), ("kern", ct.POINTER(WKern)),
+                ("kern_by_w", ct.POINTER(WKern)), ("w_min", ct.c_double),
+                ("w_max", ct.c_double), ("w_step", ct.c_double),
+                ("size_x", ct.c_int), ("size_y", ct.c_int), ("oversampling", ct.c_int)]
+
+
+_ref_libs = {}
+
+
+def reference_available(omp=False):
+    return os.path.exists(os.path.join(REF, "libref_grid_omp.so" if omp else "libref_grid.so"))
+
+
+def ref_lib(omp=False):
+    name = "libref_grid_omp.so" if omp else "libref_grid.so"
+    if name not in _ref_libs:
+        path = os.path.join(REF, name)
+        if not os.path.exists(path):
+            build(reference=True)
+        L = ct.CDLL(path)
+        vp = ct.c_void_p
+        L.grid_wprojection.argtypes = [vp, ct.c_int, ct.c_double, ct.POINTER(VisData),
+                                       ct.POINTER(WKernData)]
+        L.grid_wprojection.restype = ct.c_uint64
+        L.grid_wtowers.argtypes = [vp, ct.c_int, ct.c_double, ct.POINTER(VisData),
+                                   ct.POINTER(WKernData), ct.c_int, ct.c_int, ct.c_double]
+        L.grid_wtowers.restype = ct.c_uint64
+        L.weight.argtypes = [vp, ct.c_int, ct.c_double, ct.POINTER(VisData)]
+        L.make_hermitian.argtypes = [vp, ct.c_int]
+        L.fft_shift.argtypes = [vp, ct.c_int]
+        _ref_libs[name] = L
+    return _ref_libs[name]
+
+
+class RefInputs:
+    """Keeps the numpy buffers alive behind the ctypes structs."""
+
+    def __init__(self, obs, wk=None):
+        nbl = obs.uvw.shape[0]
+        self.arrays = []
+        self.bl = (BlData * nbl)()
+        c = 299792458.0
+        vis = np.ascontiguousarray(obs.vis, np.complex128)
+        self.vis = vis
+        for b in range(nbl):
+            uvw = np.ascontiguousarray(obs.uvw[b], np.float64)
+            fr = np.ascontiguousarray(obs.freq[b], np.float64)
+            tm = np.ascontiguousarray(obs.time, np.float64)
+            vb = np.ascontiguousarray(vis[b])
+            self.arrays += [uvw, fr, tm, vb]
+            e = self.bl[b]
+            e.antenna1, e.antenna2 = int(obs.antenna1[b]), int(obs.antenna2[b])
+            e.time_count, e.freq_count = uvw.shape[0], fr.shape[0]
+            e.time = tm.ctypes.data_as(_c_double_p)
+            e.freq = fr.ctypes.data_as(_c_double_p)
+            e.uvw = uvw.ctypes.data_as(_c_double_p)
+            e.vis = vb.ctypes.data
+            e.awkern = None
+            # per-baseline statistics as load_vis_group computes them
+            # (src/reference/hdf5.c:143-171)
+            e.u_min, e.u_max = float(uvw[:, 0].min()), float(uvw[:, 0].max())
+            e.v_min, e.v_max = float(uvw[:, 1].min()), float(uvw[:, 1].max())
+            e.w_min, e.w_max = float(uvw[:, 2].min()), float(uvw[:, 2].max())
+            e.t_min, e.t_max = float(tm.min()), float(tm.max())
+            e.f_min, e.f_max = float(fr.min()), float(fr.max())
+            e.flops = 0
+        self.vd = VisData(int(max(obs.antenna2.max(), obs.antenna1.max()) + 1), nbl, self.bl)
+        if wk is not None:
+            self.wk_data = np.ascontiguousarray(wk.data, np.complex128)
+            n = wk.plane_count
+            self.kern = (WKern * n)()
+            per = wk.oversampling * wk.oversampling * wk.size * wk.size
+            for p in range(n):
+                self.kern[p].data = self.wk_data.ctypes.data + p * per * 16
+                self.kern[p].w = wk.w_min + p * wk.w_step
+            self.wkd = WKernData(n, self.kern, self.kern, wk.w_min, wk.w_max, wk.w_step,
+                                 wk.size, wk.size, wk.oversampling)
+
+    def vis_out(self):
+        return np.ascontiguousarray(self.vis).ravel()
+
+
+def ref_grid_wprojection(grid_size, theta, obs, wk):
+    r = RefInputs(obs, wk)
+    grid = np.zeros((grid_size, grid_size), np.complex128)
+    ref_lib().grid_wprojection(_ptr(grid), grid_size, theta, ct.byref(r.vd), ct.byref(r.wkd))
+    return grid
+
+
+def ref_grid_wtowers(grid_size, theta, obs, wk, subgrid, margin, winc, omp=False):
+    r = RefInputs(obs, wk)
+    grid = np.zeros((grid_size, grid_size), np.complex128)
+    ref_lib(omp).grid_wtowers(_ptr(grid), grid_size, theta, ct.byref(r.vd), ct.byref(r.wkd),
+                              subgrid, margin, winc)
+    return grid
+
+
+def ref_weight(grid_size, theta, obs):
+    r = RefInputs(obs)
+    wgrid = np.zeros(grid_size * grid_size, np.uint32)
+    ref_lib().weight(_ptr(wgrid), grid_size, theta, ct.byref(r.vd))
+    return r.vis_out()
+
+
+def ref_make_hermitian(grid):
+    g = np.ascontiguousarray(grid, np.complex128).copy()
+    ref_lib().make_hermitian(_ptr(g), g.shape[0])
+    return g
+
+
+def ref_fft_shift(grid):
+    g = np.ascontiguousarray(grid, np.complex128).copy()
+    ref_lib().fft_shift(_ptr(g), g.shape[0])
+    return g

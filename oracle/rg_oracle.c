@@ -1,0 +1,332 @@
+/*
+ * ORACLE — test infrastructure only (see rg_oracle.h).  FP64 restatement of
+ * the reference CPU gridder, src/reference/grid.c, on flat visibility arrays.
+ * Each function names the reference lines it follows.  Arithmetic is written
+ * in the same expression order as the reference so that, compiled with IEEE
+ * semantics (no -ffast-math), results are bit-identical to grid.c itself.
+ */
+#include "rg_oracle.h"
+#include "rg_fft.h"
+
+#include <assert.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* grid.c:37-57 */
+void rgo_frac_coord(int grid_size, int kernel_size, int oversample, double theta,
+                    double u, double v, double d_u, double d_v,
+                    int *grid_offset, int *sub_offset)
+{
+    double x = theta * (u - d_u);
+    double y = theta * (v - d_v);
+    int cell_x = (int)floor(x + .5 / oversample);
+    int cell_y = (int)floor(y + .5 / oversample);
+    int frac_x = (int)floor((x - (double)cell_x) * oversample + .5);
+    int frac_y = (int)floor((y - (double)cell_y) * oversample + .5);
+    *grid_offset = (cell_y + grid_size / 2 - kernel_size / 2) * grid_size +
+                   (cell_x + grid_size / 2 - kernel_size / 2);
+    *sub_offset = kernel_size * kernel_size * (frac_y * oversample + frac_x);
+}
+
+/* grid.c:157-185: convolve one visibility onto the grid with the conjugated
+ * nearest-w, nearest-sub-cell kernel.  No bounds check (as the reference). */
+static uint64_t w_project_one(double complex *grid, int grid_size, double theta,
+                              double u, double v, double w, double complex vis,
+                              double d_u, double d_v, double d_w, const rgo_wkern *wk)
+{
+    int goff, soff;
+    rgo_frac_coord(grid_size, wk->size, wk->oversampling, theta, u, v, d_u, d_v,
+                   &goff, &soff);
+    double wr = w - d_w;
+    int plane = (int)floor((wr - wk->w_min) / wk->w_step + .5);
+    assert(plane >= 0 && plane < wk->plane_count);
+    const int ks = wk->size;
+    const double complex *taps =
+        wk->data + (size_t)plane * wk->oversampling * wk->oversampling * ks * ks;
+    /* The reference has no bounds check (grid.c:177-182).  With a W-towers
+     * margin equal to the kernel size, a visibility within 1/(2 ov) cell of a
+     * tower's low edge puts its footprint one cell before the sub-grid: the
+     * reference's linear index then lands on the previous row (kept here) or,
+     * on row -1, before the buffer (undefined behaviour there, dropped here). */
+    const long long limit = (long long)grid_size * grid_size;
+    for (int y = 0; y < ks; y++)
+        for (int x = 0; x < ks; x++) {
+            long long idx = (long long)goff + (long long)y * grid_size + x;
+            if (idx < 0 || idx >= limit) continue;
+            grid[idx] += vis * conj(taps[soff + y * ks + x]);
+        }
+    return 8 * (uint64_t)ks * (uint64_t)ks;
+}
+
+/* grid.c:187-202 */
+uint64_t rgo_grid_wprojection(double complex *uvgrid, int grid_size, double theta,
+                              int64_t nvis, const double *u, const double *v,
+                              const double *w, const double complex *vis,
+                              const rgo_wkern *wk)
+{
+    uint64_t flops = 0;
+    for (int64_t i = 0; i < nvis; i++)
+        flops += w_project_one(uvgrid, grid_size, theta, u[i], v[i], w[i], vis[i],
+                               0, 0, 0, wk);
+    return flops;
+}
+
+/* Integer power by binary exponentiation, grid.c:280-293. */
+static double complex int_power(double complex base, int e)
+{
+    if (e < 0) return 1 / int_power(base, -e);
+    if (e == 1) return base;
+    double complex acc = 1;
+    while (e) {
+        if (e & 1) acc *= base;
+        e >>= 1;
+        base *= base;
+    }
+    return acc;
+}
+
+/* Chunk bounds of tower (cx, cy), grid.c:425-442. */
+static void tower_bounds(int c, int chunk_size, int grid_size, double theta,
+                         int *x_min, double *lo, double *hi, double *mid)
+{
+    *x_min = chunk_size * c - grid_size / 2;
+    *lo = ((double)*x_min - 0.5) / theta;
+    *hi = *lo + chunk_size / theta;
+    *mid = (double)(*x_min + chunk_size / 2) / theta;
+}
+
+/* grid.c:295-555 (serial).  The reference scans every baseline of a tower's bin
+ * once per w-floor and grids the visibilities passing the half-open (u,v,w)
+ * cut in baseline/time/frequency order.  Here the same cut is applied once per
+ * visibility (testing the neighbouring towers/floors with the reference's exact
+ * comparisons) and a stable counting sort keeps that order per (tower, floor),
+ * which yields the same additions in the same order. */
+uint64_t rgo_grid_wtowers(double complex *uvgrid, int grid_size, double theta,
+                          int64_t nvis, const double *u, const double *v,
+                          const double *w, const double complex *vis,
+                          const rgo_wkern *wk, int subgrid_size, int subgrid_margin,
+                          double wincrement, int32_t *gridded_count)
+{
+    const int S = subgrid_size, M = subgrid_margin;
+    assert(M >= wk->size);
+    assert(S % 2 == 0 && M % 2 == 0);
+
+    /* Fresnel transfer pattern between neighbouring w-floors, grid.c:304-319 */
+    double complex *wtransfer = (double complex *)malloc(sizeof(double complex) * S * S);
+    for (int y = 0; y < S; y++)
+        for (int x = 0; x < S; x++) {
+            double l = theta * (double)(x - S / 2) / S;
+            double m = theta * (double)(y - S / 2) / S;
+            double ph = wincrement * (1 - sqrt(1 - l * l - m * m));
+            wtransfer[y * S + x] = cexp(2 * M_PI * I * ph);
+        }
+    rgo_fft_shift(wtransfer, S);
+
+    const int chunk = S - M;
+    const int nchunk = grid_size / chunk + 1;
+
+    /* w range, always including 0 (grid.c:357-367) */
+    double wlo = 0, whi = 0;
+    for (int64_t i = 0; i < nvis; i++) {
+        if (w[i] < wlo) wlo = w[i];
+        if (w[i] > whi) whi = w[i];
+    }
+    const int wp_min = (int)floor(wlo / wincrement + 0.5);
+    const int wp_max = (int)floor(whi / wincrement + 0.5);
+    const int nfloor = wp_max - wp_min + 1;
+    const int64_t nbins = (int64_t)nchunk * nchunk * nfloor;
+
+    /* assign visibilities to (tower, floor) bins with the reference's cuts */
+    int64_t cap = nvis + 16, npairs = 0;
+    int64_t *pair_bin = (int64_t *)malloc(sizeof(int64_t) * cap);
+    int64_t *pair_vis = (int64_t *)malloc(sizeof(int64_t) * cap);
+    for (int64_t i = 0; i < nvis; i++) {
+        int cxc = (int)floor((u[i] * theta + 0.5 + grid_size / 2) / chunk);
+        int cyc = (int)floor((v[i] * theta + 0.5 + grid_size / 2) / chunk);
+        int wpc = (int)floor(w[i] / wincrement + 0.5);
+        for (int cy = cyc - 1; cy <= cyc + 1; cy++) {
+            if (cy < 0 || cy >= nchunk) continue;
+            int y_min; double vlo, vhi, vmid;
+            tower_bounds(cy, chunk, grid_size, theta, &y_min, &vlo, &vhi, &vmid);
+            if (v[i] < vlo || v[i] >= vhi) continue;
+            for (int cx = cxc - 1; cx <= cxc + 1; cx++) {
+                if (cx < 0 || cx >= nchunk) continue;
+                int x_min; double ulo, uhi, umid;
+                tower_bounds(cx, chunk, grid_size, theta, &x_min, &ulo, &uhi, &umid);
+                if (u[i] < ulo || u[i] >= uhi) continue;
+                for (int wp = wpc - 1; wp <= wpc + 1; wp++) {
+                    if (wp < wp_min || wp > wp_max) continue;
+                    double wflo = ((double)wp - 0.5) * wincrement;
+                    double wfhi = ((double)wp + 0.5) * wincrement;
+                    if (w[i] < wflo || w[i] >= wfhi) continue;
+                    if (npairs == cap) {
+                        cap *= 2;
+                        pair_bin = (int64_t *)realloc(pair_bin, sizeof(int64_t) * cap);
+                        pair_vis = (int64_t *)realloc(pair_vis, sizeof(int64_t) * cap);
+                    }
+                    pair_bin[npairs] = ((int64_t)cy * nchunk + cx) * nfloor + (wp - wp_min);
+                    pair_vis[npairs] = i;
+                    npairs++;
+                }
+            }
+        }
+    }
+    /* stable counting sort by bin */
+    int64_t *start = (int64_t *)calloc((size_t)nbins + 1, sizeof(int64_t));
+    for (int64_t p = 0; p < npairs; p++) start[pair_bin[p] + 1]++;
+    for (int64_t b = 0; b < nbins; b++) start[b + 1] += start[b];
+    int64_t *order = (int64_t *)malloc(sizeof(int64_t) * (npairs + 1));
+    int64_t *fill = (int64_t *)malloc(sizeof(int64_t) * (size_t)nbins);
+    memcpy(fill, start, sizeof(int64_t) * (size_t)nbins);
+    for (int64_t p = 0; p < npairs; p++) order[fill[pair_bin[p]]++] = pair_vis[p];
+    free(fill);
+    if (gridded_count) memset(gridded_count, 0, sizeof(int32_t) * (size_t)nvis);
+
+    double complex *subgrid = (double complex *)calloc((size_t)S * S, sizeof(double complex));
+    double complex *subimg = (double complex *)calloc((size_t)S * S, sizeof(double complex));
+    uint64_t flops = 0;
+    const int sg_norm = S * S;
+    double complex *uvgrid_mid = uvgrid + (grid_size + 1) * grid_size / 2;
+
+    for (int c = 0; c < nchunk * nchunk; c++) {
+        int cx = c % nchunk, cy = c / nchunk;
+        int x_min, y_min;
+        double ulo, uhi, umid, vlo, vhi, vmid;
+        tower_bounds(cx, chunk, grid_size, theta, &x_min, &ulo, &uhi, &umid);
+        tower_bounds(cy, chunk, grid_size, theta, &y_min, &vlo, &vhi, &vmid);
+
+        memset(subgrid, 0, sizeof(double complex) * S * S);
+        memset(subimg, 0, sizeof(double complex) * S * S);
+        int have_vis = 0, last_wp = wp_min;
+        for (int wp = wp_min; wp <= wp_max; wp++) {
+            int64_t b = (int64_t)c * nfloor + (wp - wp_min);
+            if (start[b] == start[b + 1]) continue; /* grid.c:462 */
+            double w_mid = (double)wp * wincrement;
+            for (int64_t p = start[b]; p < start[b + 1]; p++) {
+                int64_t i = order[p];
+                flops += w_project_one(subgrid, S, theta, u[i], v[i], w[i], vis[i],
+                                       umid, vmid, w_mid, wk);
+                if (gridded_count) gridded_count[i]++;
+            }
+            have_vis = 1;
+            /* back to the image plane, step the accumulated sub-image to this
+             * floor and add (grid.c:467-483) */
+            rgo_fft2d(subgrid, subgrid, S, S, +1);
+            for (int k = 0; k < S * S; k++) {
+                double complex step = int_power(wtransfer[k], wp - last_wp);
+                subimg[k] = step * subimg[k] + subgrid[k];
+                subgrid[k] = 0;
+            }
+            last_wp = wp;
+        }
+        if (!have_vis) continue;
+        /* to w = 0 (grid.c:490-496), back to the uv plane (grid.c:499) */
+        if (last_wp != 0)
+            for (int k = 0; k < S * S; k++) subimg[k] /= int_power(wtransfer[k], last_wp);
+        rgo_fft2d(subimg, subimg, S, S, -1);
+        /* add the sub-grid, margins included, clipped to the grid (grid.c:503-516) */
+        int x0 = x_min - M / 2, x1 = x0 + S;
+        int y0 = y_min - M / 2, y1 = y0 + S;
+        if (x0 < -grid_size / 2) x0 = -grid_size / 2;
+        if (y0 < -grid_size / 2) y0 = -grid_size / 2;
+        if (x1 > grid_size / 2) x1 = grid_size / 2;
+        if (y1 > grid_size / 2) y1 = grid_size / 2;
+        for (int y = y0; y < y1; y++)
+            for (int x = x0; x < x1; x++)
+                uvgrid_mid[x + y * grid_size] +=
+                    (subimg[(x - x_min + M / 2) + (y - y_min + M / 2) * S] / sg_norm);
+    }
+
+    free(subgrid); free(subimg); free(order); free(start);
+    free(pair_bin); free(pair_vis); free(wtransfer);
+    return flops;
+}
+
+/* grid.c:27-35 */
+static int nearest_cell(int grid_size, double theta, double u, double v)
+{
+    int x = (int)floor(theta * u + .5);
+    int y = (int)floor(theta * v + .5);
+    return (y + grid_size / 2) * grid_size + (x + grid_size / 2);
+}
+
+/* grid.c:59-81 */
+void rgo_weight(int grid_size, double theta, int64_t nvis, const double *u,
+                const double *v, double complex *vis)
+{
+    unsigned int *count = (unsigned int *)calloc((size_t)grid_size * grid_size,
+                                                 sizeof(unsigned int));
+    for (int64_t i = 0; i < nvis; i++) count[nearest_cell(grid_size, theta, u[i], v[i])]++;
+    for (int64_t i = 0; i < nvis; i++) vis[i] /= count[nearest_cell(grid_size, theta, u[i], v[i])];
+    free(count);
+}
+
+/* grid.c:639-662: G(k) += conj(G(-k)) pairwise; the zero frequency of an
+ * even-sized grid sits at (N/2, N/2), so row 0 and column 0 are skipped. */
+void rgo_make_hermitian(double complex *uvgrid, int grid_size)
+{
+    double complex *lo = (grid_size % 2 == 0) ? uvgrid + grid_size + 1 : uvgrid;
+    double complex *hi = uvgrid + (size_t)grid_size * grid_size - 1;
+    while (lo < hi) {
+        double complex keep = *lo;
+        *lo++ += conj(*hi);
+        *hi-- += conj(keep);
+    }
+    assert(lo == hi && lo == uvgrid + (grid_size + 1) * (grid_size / 2));
+    *lo += conj(*lo);
+}
+
+/* grid.c:665-680: exchange quadrants (both axes shift by N/2). */
+void rgo_fft_shift(double complex *uvgrid, int grid_size)
+{
+    assert(grid_size % 2 == 0);
+    const long long n2 = (long long)grid_size * grid_size;
+    const long long jump = (long long)(grid_size + 1) * (grid_size / 2);
+    for (int y = 0; y < grid_size; y++)
+        for (int x = 0; x < grid_size / 2; x++) {
+            long long a = (long long)y * grid_size + x;
+            long long b = (a + jump) % n2;
+            double complex t = uvgrid[a];
+            uvgrid[a] = uvgrid[b];
+            uvgrid[b] = t;
+        }
+}
+
+/* main.c:258-294 */
+void rgo_image_from_grid(double complex *uvgrid, int grid_size, double *image)
+{
+    rgo_make_hermitian(uvgrid, grid_size);
+    rgo_fft_shift(uvgrid, grid_size);
+    rgo_fft2d(uvgrid, uvgrid, grid_size, grid_size, -1);
+    rgo_fft_shift(uvgrid, grid_size);
+    for (long long k = 0; k < (long long)grid_size * grid_size; k++) image[k] = creal(uvgrid[k]);
+}
+
+void rgo_dft_image(double *image, int grid_size, double theta, int64_t nvis,
+                   const double *u, const double *v, const double *w,
+                   const double complex *vis, double factor)
+{
+    const int N = grid_size;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int y = 0; y < N; y++) {
+        double m = theta * (double)(y - N / 2) / N;
+        for (int x = 0; x < N; x++) {
+            double l = theta * (double)(x - N / 2) / N;
+            double one_minus_n = 1.0 - sqrt(1.0 - l * l - m * m);
+            double sum = 0.0, comp = 0.0;
+            for (int64_t k = 0; k < nvis; k++) {
+                double ph = u[k] * l + v[k] * m + w[k] * one_minus_n;
+                ph -= nearbyint(ph);
+                double a = 2.0 * M_PI * ph;
+                double term = creal(vis[k]) * cos(a) + cimag(vis[k]) * sin(a);
+                double t = sum + term; /* Neumaier compensated sum */
+                if (fabs(sum) >= fabs(term)) comp += (sum - t) + term;
+                else comp += (term - t) + sum;
+                sum = t;
+            }
+            image[(size_t)y * N + x] = factor * (sum + comp);
+        }
+    }
+}

@@ -1,0 +1,280 @@
+"""B200-native radio imager: Python mirror of the reference's gridder interface.
+
+The compute path is the CUDA library ``librg_b200.so`` built from ``csrc/``
+(sm_100a) and bound here with ctypes; there is no CPU fallback — if the
+library is missing or no B200 is present, every call raises.
+
+Function names and argument meaning follow the reference's CPU gridder API
+(src/reference/grid.h:113-137): ``grid_wprojection``, ``grid_wtowers``,
+``weight``, ``make_hermitian``, ``fft_shift``, plus the image pipeline of
+src/reference/main.c:258-294 (``image_from_grid``) and the direct DFT imager of
+src/dft/dft_cuda.cu (``dft_image``).  Like the reference, the gridders
+accumulate into ``uvgrid``; errors raise :class:`RGError` instead of exiting.
+
+Buffers may be numpy arrays (host; staged through device memory) or CUDA
+tensors / any object with ``data_ptr()`` (used in place).
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librg_b200.so")
+
+RG_GRID_ACCUMULATE = 0
+RG_GRID_OVERWRITE = 1
+RG_DFT_FP32_NAIVE = 0
+RG_DFT_FP64_REDUCED = 1
+RG_DFT_FP64 = 2
+
+STATUS = {0: "RG_OK", 1: "RG_ERR_INVALID_ARGUMENT", 2: "RG_ERR_CUDA", 3: "RG_ERR_OUT_OF_MEMORY",
+          4: "RG_ERR_UNSUPPORTED", 5: "RG_ERR_IO", 6: "RG_ERR_NO_DEVICE"}
+
+# every symbol include/radio_gridders.h declares
+EXPORTS = [
+    "rg_context_create", "rg_context_destroy", "rg_context_set_stream", "rg_last_error",
+    "rg_last_stats", "rg_grid_wprojection", "rg_grid_wtowers", "rg_weight",
+    "rg_make_hermitian", "rg_fft_shift", "rg_image_from_grid", "rg_fft2d", "rg_dft_image",
+]
+
+
+class RGError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+def build() -> None:
+    """Compile csrc/ for sm_100a into librg_b200.so (make, in-tree)."""
+    subprocess.run(["make", "-s", "-C", HERE, "-j", str(min(8, os.cpu_count() or 1))], check=True)
+
+
+class _Vis(ct.Structure):
+    _fields_ = [("u", ct.c_void_p), ("v", ct.c_void_p), ("w", ct.c_void_p),
+                ("vis", ct.c_void_p), ("n", ct.c_int64)]
+
+
+class _WKern(ct.Structure):
+    _fields_ = [("data", ct.c_void_p), ("plane_count", ct.c_int), ("size", ct.c_int),
+                ("oversampling", ct.c_int), ("w_min", ct.c_double), ("w_step", ct.c_double)]
+
+
+_lib = None
+
+
+def lib():
+    """Load librg_b200.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RGError(4, f"{LIB_PATH} is not built; run radio-gridders_b200 build()")
+        L = ct.CDLL(LIB_PATH)
+        vp, i, d, i64 = ct.c_void_p, ct.c_int, ct.c_double, ct.c_int64
+        L.rg_context_create.argtypes = [i, ct.POINTER(vp)]
+        L.rg_context_destroy.argtypes = [vp]
+        L.rg_context_set_stream.argtypes = [vp, vp]
+        L.rg_last_error.restype = ct.c_char_p
+        L.rg_last_stats.argtypes = [vp, ct.POINTER(i64), i]
+        L.rg_last_stats.restype = i
+        L.rg_grid_wprojection.argtypes = [vp, vp, i, d, ct.POINTER(_Vis), ct.POINTER(_WKern), i]
+        L.rg_grid_wtowers.argtypes = [vp, vp, i, d, ct.POINTER(_Vis), ct.POINTER(_WKern), i, i, d, i]
+        L.rg_weight.argtypes = [vp, i, d, ct.POINTER(_Vis), vp]
+        L.rg_make_hermitian.argtypes = [vp, vp, i]
+        L.rg_fft_shift.argtypes = [vp, vp, i]
+        L.rg_image_from_grid.argtypes = [vp, vp, i, vp, vp]
+        L.rg_fft2d.argtypes = [vp, vp, i, i, i, i, i]
+        L.rg_dft_image.argtypes = [vp, vp, i, d, ct.POINTER(_Vis), i, d]
+        for name in EXPORTS:
+            getattr(L, name)  # raises AttributeError if a declared symbol is missing
+        _lib = L
+    return _lib
+
+
+def _check(status):
+    if status != 0:
+        raise RGError(status, lib().rg_last_error().decode(errors="replace"))
+
+
+def _ptr(a):
+    """Address of a numpy array (must be C-contiguous) or a tensor-like."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("arrays must be C-contiguous")
+        return a.ctypes.data
+    raise TypeError(f"unsupported buffer type {type(a)}")
+
+
+def _as_f64(a):
+    if hasattr(a, "data_ptr"):
+        return a
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _as_c128(a):
+    if hasattr(a, "data_ptr"):
+        return a
+    return np.ascontiguousarray(a, dtype=np.complex128)
+
+
+class Visibilities:
+    """Flat visibilities (struct flat_vis_data, src/common/hdf5.cuh:31-37):
+    u, v, w in wavelengths (float64), vis complex128."""
+
+    def __init__(self, u, v, w, vis):
+        self.u, self.v, self.w = _as_f64(u), _as_f64(v), _as_f64(w)
+        self.vis = _as_c128(vis)
+        n = len(self.u) if not hasattr(self.u, "numel") else self.u.numel()
+        self.n = int(n)
+
+    def struct(self):
+        return _Vis(_ptr(self.u), _ptr(self.v), _ptr(self.w), _ptr(self.vis), self.n)
+
+
+def _wkern_struct(wk, data=None):
+    """wk: simulate.WKernel-like (data [planes, ov, ov, size, size], w_min, w_step)."""
+    arr = data if data is not None else _as_c128(wk.data)
+    shape = tuple(arr.shape)
+    return _WKern(_ptr(arr), int(shape[0]), int(shape[3]), int(shape[1]), float(wk.w_min),
+                  float(wk.w_step)), arr
+
+
+class Context:
+    """A device context (streams and scratch memory), rg_context_create."""
+
+    def __init__(self, device: int = 0):
+        self._h = ct.c_void_p()
+        _check(lib().rg_context_create(device, ct.byref(self._h)))
+
+    def close(self):
+        if self._h:
+            lib().rg_context_destroy(self._h)
+            self._h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, stream_ptr):
+        _check(lib().rg_context_set_stream(self._h, stream_ptr))
+
+    def last_stats(self):
+        out = (ct.c_int64 * 8)()
+        n = lib().rg_last_stats(self._h, out, 8)
+        keys = ["gridded", "active_subgrids", "towers_with_data", "floors", "dropped", "launches"]
+        return {k: int(out[j]) for j, k in enumerate(keys[:n])}
+
+    # ---- gridders (src/reference/grid.h:121-126) -------------------------
+    def grid_wprojection(self, uvgrid, grid_size, theta, vis: Visibilities, wkern,
+                         flags=RG_GRID_ACCUMULATE, wkern_data=None):
+        s, keep = _wkern_struct(wkern, wkern_data)
+        vs = vis.struct()
+        _check(lib().rg_grid_wprojection(self._h, _ptr(uvgrid), int(grid_size), float(theta),
+                                         ct.byref(vs), ct.byref(s), int(flags)))
+        return uvgrid
+
+    def grid_wtowers(self, uvgrid, grid_size, theta, vis: Visibilities, wkern, subgrid_size,
+                     subgrid_margin, wincrement, flags=RG_GRID_ACCUMULATE, wkern_data=None):
+        s, keep = _wkern_struct(wkern, wkern_data)
+        vs = vis.struct()
+        _check(lib().rg_grid_wtowers(self._h, _ptr(uvgrid), int(grid_size), float(theta),
+                                     ct.byref(vs), ct.byref(s), int(subgrid_size),
+                                     int(subgrid_margin), float(wincrement), int(flags)))
+        return uvgrid
+
+    def weight(self, grid_size, theta, vis: Visibilities, out=None):
+        if out is None:
+            out = np.empty(vis.n, np.complex128)
+        vs = vis.struct()
+        _check(lib().rg_weight(self._h, int(grid_size), float(theta), ct.byref(vs), _ptr(out)))
+        return out
+
+    # ---- image formation (src/reference/grid.c:639-680, main.c:258-294) ----
+    def make_hermitian(self, uvgrid):
+        _check(lib().rg_make_hermitian(self._h, _ptr(uvgrid), int(uvgrid.shape[0])))
+        return uvgrid
+
+    def fft_shift(self, uvgrid):
+        _check(lib().rg_fft_shift(self._h, _ptr(uvgrid), int(uvgrid.shape[0])))
+        return uvgrid
+
+    def image_from_grid(self, uvgrid, image=None, taper_1d=None):
+        n = int(uvgrid.shape[0])
+        if image is None:
+            image = np.empty((n, n), np.float64)
+        t = None if taper_1d is None else np.ascontiguousarray(taper_1d, np.float64)
+        _check(lib().rg_image_from_grid(self._h, _ptr(uvgrid), n, _ptr(image), _ptr(t)))
+        return image
+
+    def fft2d(self, data, sign):
+        """Batched 2-D FFT in place on [batch, ny, nx] complex64/complex128."""
+        shape = data.shape
+        batch = int(np.prod(shape[:-2])) if len(shape) > 2 else 1
+        cb = 8 if str(data.dtype).endswith("complex64") else 16
+        _check(lib().rg_fft2d(self._h, _ptr(data), batch, int(shape[-2]), int(shape[-1]),
+                              int(sign), cb))
+        return data
+
+    # ---- direct DFT (src/dft/dft_cuda.cu) ----------------------------------
+    def dft_image(self, grid_size, theta, vis: Visibilities, precision=RG_DFT_FP64_REDUCED,
+                  factor=2.0, image=None):
+        if image is None:
+            image = np.empty((grid_size, grid_size), np.float64)
+        vs = vis.struct()
+        _check(lib().rg_dft_image(self._h, _ptr(image), int(grid_size), float(theta),
+                                  ct.byref(vs), int(precision), float(factor)))
+        return image
+
+
+_default = None
+
+
+def default_context() -> Context:
+    global _default
+    if _default is None:
+        _default = Context(0)
+    return _default
+
+
+# Module-level mirror of the reference's function names ----------------------
+
+def grid_wprojection(uvgrid, grid_size, theta, vis, wkern):
+    return default_context().grid_wprojection(uvgrid, grid_size, theta, vis, wkern)
+
+
+def grid_wtowers(uvgrid, grid_size, theta, vis, wkern, subgrid_size, subgrid_margin, wincrement):
+    return default_context().grid_wtowers(uvgrid, grid_size, theta, vis, wkern, subgrid_size,
+                                          subgrid_margin, wincrement)
+
+
+def weight(grid_size, theta, vis):
+    return default_context().weight(grid_size, theta, vis)
+
+
+def make_hermitian(uvgrid):
+    return default_context().make_hermitian(uvgrid)
+
+
+def fft_shift(uvgrid):
+    return default_context().fft_shift(uvgrid)
+
+
+def image_from_grid(uvgrid, taper_1d=None):
+    return default_context().image_from_grid(uvgrid, taper_1d=taper_1d)
+
+
+def dft_image(grid_size, theta, vis, precision=RG_DFT_FP64_REDUCED, factor=2.0):
+    return default_context().dft_image(grid_size, theta, vis, precision, factor)

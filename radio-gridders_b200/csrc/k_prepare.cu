@@ -1,0 +1,324 @@
+// Visibility preparation: per-visibility FP64 coordinate work done once, so the
+// gridder reads a 16-byte record and an FP32 visibility.
+//
+// Coordinates follow the reference's arithmetic operation for operation, with
+// explicit round-to-nearest intrinsics so nothing is contracted into an FMA:
+//   frac_coord          src/reference/grid.c:37-57
+//   w-plane selection   src/reference/grid.c:168-170
+//   tower/floor cuts    src/reference/grid.c:357-367, 425-458, 244-254
+// Record layout (int4): x = bin (tower*nfloor + floor, -1 = not gridded),
+// y = (row0 << 16) | (col0 & 0xffff)  (footprint origin, int16 each, may be -1),
+// z = tap base index into the FP32 kernel table, w = unused.
+#include <cfloat>
+
+#include "rg_internal.h"
+
+namespace rg {
+
+__device__ __forceinline__ bool finite3(double a, double b, double c)
+{
+    return isfinite(a) && isfinite(b) && isfinite(c);
+}
+
+// block-wide min/max of w (min starts at 0, max at 0: grid.c:357-367)
+__global__ void minmax_w_kernel(const double *__restrict__ u, const double *__restrict__ v,
+                                const double *__restrict__ w, int64_t n,
+                                unsigned long long *out_bits, unsigned *err)
+{
+    double lo = 0.0, hi = 0.0;
+    bool bad = false;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double ww = w[i];
+        if (!finite3(u[i], v[i], ww)) {
+            bad = true;
+            continue;
+        }
+        lo = fmin(lo, ww);
+        hi = fmax(hi, ww);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    __shared__ double slo[32], shi[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        slo[wid] = lo;
+        shi[wid] = hi;
+    }
+    if (bad) atomicOr(err, DERR_NONFINITE);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < (int)(blockDim.x >> 5); k++) {
+            lo = fmin(lo, slo[k]);
+            hi = fmax(hi, shi[k]);
+        }
+        // min <= 0 and max >= 0: IEEE bit patterns order monotonically in
+        // magnitude within one sign, so unsigned max works for both.
+        if (lo < 0.0) atomicMax(out_bits + 0, (unsigned long long)__double_as_longlong(lo));
+        if (hi > 0.0) atomicMax(out_bits + 1, (unsigned long long)__double_as_longlong(hi));
+    }
+}
+
+void launch_minmax_w(cudaStream_t s, const double *u, const double *v, const double *w, int64_t n,
+                     double *out2, unsigned *err)
+{
+    // out2 as bit patterns: [0] = -0.0 (min so far), [1] = +0.0
+    unsigned long long init[2] = {0x8000000000000000ull, 0ull};
+    cudaMemcpyAsync(out2, init, sizeof(init), cudaMemcpyHostToDevice, s);
+    int blocks = (int)((n + 255) / 256);
+    if (blocks > 4096) blocks = 4096;
+    if (blocks < 1) blocks = 1;
+    minmax_w_kernel<<<blocks, 256, 0, s>>>(u, v, w, n, (unsigned long long *)out2, err);
+}
+
+struct Bounds {
+    double lo, hi, mid;
+    int origin;
+};
+
+// tower bounds along one axis, grid.c:425-442
+__device__ __forceinline__ Bounds tower_axis(int c, int chunk, int grid_size, double theta)
+{
+    Bounds b;
+    b.origin = chunk * c - grid_size / 2;
+    b.lo = __ddiv_rn(__dsub_rn((double)b.origin, 0.5), theta);
+    b.hi = __dadd_rn(b.lo, __ddiv_rn((double)chunk, theta));
+    b.mid = __ddiv_rn((double)(b.origin + chunk / 2), theta);
+    return b;
+}
+
+// frac_coord along one axis: cell and sub-cell index
+__device__ __forceinline__ void frac_axis(double coord, double mid, double theta, int ov,
+                                          double half_over_ov, int &cell, int &frac)
+{
+    const double x = __dmul_rn(theta, __dsub_rn(coord, mid));
+    cell = (int)floor(__dadd_rn(x, half_over_ov));
+    frac = (int)floor(__dadd_rn(__dmul_rn(__dsub_rn(x, (double)cell), (double)ov), 0.5));
+}
+
+__global__ void prepare_towers_kernel(const double *__restrict__ u, const double *__restrict__ v,
+                                      const double *__restrict__ w, const double2 *__restrict__ vis,
+                                      int64_t n, TowerGeom g, int wp_min, int nfloor,
+                                      int4 *__restrict__ rec, float2 *__restrict__ visf,
+                                      int *__restrict__ active, unsigned *err,
+                                      unsigned long long *counters)
+{
+    const double half_over_ov = 0.5 / (double)g.ov;
+    const int wp_max = wp_min + nfloor - 1;
+    const int taps_total = g.planes * g.ov * g.ov * g.ksize * g.ksize;
+    unsigned local_err = 0, gridded = 0, dropped = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double uu = u[i], vv = v[i], ww = w[i];
+        const double2 vz = vis[i];
+        visf[i] = make_float2((float)vz.x, (float)vz.y);
+        int4 r = make_int4(-1, 0, 0, 0);
+        if (!finite3(uu, vv, ww)) {
+            local_err |= DERR_NONFINITE;
+            rec[i] = r;
+            continue;
+        }
+        const double half_n = (double)(g.grid_size / 2);
+        const int cxc = (int)floor((uu * g.theta + 0.5 + half_n) / g.chunk);
+        const int cyc = (int)floor((vv * g.theta + 0.5 + half_n) / g.chunk);
+        const int wpc = (int)floor(ww / g.winc + 0.5);
+        int found_cx = -1, found_cy = -1, found_wp = 0;
+        Bounds bx, by;
+        for (int cy = cyc - 1; cy <= cyc + 1 && found_cy < 0; cy++) {
+            if (cy < 0 || cy >= g.nchunk) continue;
+            Bounds t = tower_axis(cy, g.chunk, g.grid_size, g.theta);
+            if (vv < t.lo || vv >= t.hi) continue;
+            found_cy = cy;
+            by = t;
+        }
+        for (int cx = cxc - 1; cx <= cxc + 1 && found_cx < 0; cx++) {
+            if (cx < 0 || cx >= g.nchunk) continue;
+            Bounds t = tower_axis(cx, g.chunk, g.grid_size, g.theta);
+            if (uu < t.lo || uu >= t.hi) continue;
+            found_cx = cx;
+            bx = t;
+        }
+        bool have_wp = false;
+        for (int wp = wpc - 1; wp <= wpc + 1 && !have_wp; wp++) {
+            if (wp < wp_min || wp > wp_max) continue;
+            const double wlo = __dmul_rn(__dsub_rn((double)wp, 0.5), g.winc);
+            const double whi = __dmul_rn(__dadd_rn((double)wp, 0.5), g.winc);
+            if (ww < wlo || ww >= whi) continue;
+            have_wp = true;
+            found_wp = wp;
+        }
+        if (found_cx < 0 || found_cy < 0 || !have_wp) {
+            dropped++;
+            rec[i] = r;
+            continue;
+        }
+        int cell_x, frac_x, cell_y, frac_y;
+        frac_axis(uu, bx.mid, g.theta, g.ov, half_over_ov, cell_x, frac_x);
+        frac_axis(vv, by.mid, g.theta, g.ov, half_over_ov, cell_y, frac_y);
+        const double wmid = __dmul_rn((double)found_wp, g.winc);
+        const double wr = __dsub_rn(ww, wmid);
+        const int plane = (int)floor(__dadd_rn(__ddiv_rn(__dsub_rn(wr, g.wk_wmin), g.wk_wstep), 0.5));
+        const int ks2 = g.ksize * g.ksize;
+        const long long tap = (long long)plane * g.ov * g.ov * ks2 +
+                              (long long)ks2 * (frac_y * g.ov + frac_x);
+        if (plane < 0 || plane >= g.planes || tap < 0 || tap + ks2 > taps_total) {
+            local_err |= DERR_PLANE_RANGE;
+            rec[i] = r;
+            continue;
+        }
+        const int col0 = cell_x + g.subgrid / 2 - g.ksize / 2;
+        const int row0 = cell_y + g.subgrid / 2 - g.ksize / 2;
+        const int tower = found_cy * g.nchunk + found_cx;
+        const int bin = tower * nfloor + (found_wp - wp_min);
+        r.x = bin;
+        r.y = (row0 << 16) | (col0 & 0xffff);
+        r.z = (int)tap;
+        rec[i] = r;
+        active[bin] = 1;
+        gridded++;
+    }
+    if (local_err) atomicOr(err, local_err);
+    // warp-aggregated counters
+    for (int o = 16; o > 0; o >>= 1) {
+        gridded += __shfl_xor_sync(0xffffffffu, gridded, o);
+        dropped += __shfl_xor_sync(0xffffffffu, dropped, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (gridded) atomicAdd(counters + 0, (unsigned long long)gridded);
+        if (dropped) atomicAdd(counters + 1, (unsigned long long)dropped);
+    }
+}
+
+void launch_prepare_towers(cudaStream_t s, const double *u, const double *v, const double *w,
+                           const double2 *vis, int64_t n, TowerGeom g, int wp_min, int nfloor,
+                           int4 *rec, float2 *visf, int *active, unsigned *err,
+                           unsigned long long *counters)
+{
+    int blocks = (int)((n + 255) / 256);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    if (blocks < 1) blocks = 1;
+    prepare_towers_kernel<<<blocks, 256, 0, s>>>(u, v, w, vis, n, g, wp_min, nfloor, rec, visf,
+                                                 active, err, counters);
+}
+
+__global__ void prepare_wproj_kernel(const double *__restrict__ u, const double *__restrict__ v,
+                                     const double *__restrict__ w, const double2 *__restrict__ vis,
+                                     int64_t n, int grid_size, double theta, int ksize, int ov,
+                                     int planes, double wk_wmin, double wk_wstep,
+                                     int4 *__restrict__ rec, float2 *__restrict__ visf,
+                                     unsigned *err)
+{
+    const double half_over_ov = 0.5 / (double)ov;
+    const int ks2 = ksize * ksize;
+    const long long taps_total = (long long)planes * ov * ov * ks2;
+    unsigned local_err = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double uu = u[i], vv = v[i], ww = w[i];
+        const double2 vz = vis[i];
+        visf[i] = make_float2((float)vz.x, (float)vz.y);
+        int4 r = make_int4(-1, 0, 0, 0);
+        if (!finite3(uu, vv, ww)) {
+            local_err |= DERR_NONFINITE;
+            rec[i] = r;
+            continue;
+        }
+        int cell_x, frac_x, cell_y, frac_y;
+        frac_axis(uu, 0.0, theta, ov, half_over_ov, cell_x, frac_x);
+        frac_axis(vv, 0.0, theta, ov, half_over_ov, cell_y, frac_y);
+        const int plane = (int)floor(__dadd_rn(__ddiv_rn(__dsub_rn(__dsub_rn(ww, 0.0), wk_wmin), wk_wstep), 0.5));
+        const long long tap = (long long)plane * ov * ov * ks2 + (long long)ks2 * (frac_y * ov + frac_x);
+        if (plane < 0 || plane >= planes || tap < 0 || tap + ks2 > taps_total) {
+            local_err |= DERR_PLANE_RANGE;
+            rec[i] = r;
+            continue;
+        }
+        const int col0 = cell_x + grid_size / 2 - ksize / 2;
+        const int row0 = cell_y + grid_size / 2 - ksize / 2;
+        if (col0 < -ksize || col0 > grid_size || row0 < -ksize || row0 > grid_size) {
+            local_err |= DERR_GRID_RANGE;
+            rec[i] = r;
+            continue;
+        }
+        r.x = 0;
+        r.y = (row0 << 16) | (col0 & 0xffff);
+        r.z = (int)tap;
+        rec[i] = r;
+    }
+    if (local_err) atomicOr(err, local_err);
+}
+
+void launch_prepare_wproj(cudaStream_t s, const double *u, const double *v, const double *w,
+                          const double2 *vis, int64_t n, int grid_size, double theta, int ksize,
+                          int ov, int planes, double wk_wmin, double wk_wstep, int4 *rec,
+                          float2 *visf, unsigned *err)
+{
+    int blocks = (int)((n + 255) / 256);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    if (blocks < 1) blocks = 1;
+    prepare_wproj_kernel<<<blocks, 256, 0, s>>>(u, v, w, vis, n, grid_size, theta, ksize, ov,
+                                                planes, wk_wmin, wk_wstep, rec, visf, err);
+}
+
+// Single-CTA compaction of active (tower, floor) bins into slots, in bin order,
+// so each tower's slots are contiguous and ordered by floor.
+__global__ void compact_bins_kernel(const int *__restrict__ active, int nbins, int nfloor,
+                                    int *__restrict__ slot_of_bin, int *__restrict__ bin_of_slot,
+                                    int *__restrict__ n_active, int *__restrict__ tower_first,
+                                    int *__restrict__ tower_count, int ntowers)
+{
+    __shared__ int warp_sums[32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int base = 0; base < nbins; base += blockDim.x) {
+        const int b = base + threadIdx.x;
+        const int a = (b < nbins && active[b]) ? 1 : 0;
+        int incl = a;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) warp_sums[wid] = incl;
+        __syncthreads();
+        if (wid == 0) {
+            int x = lane < nw ? warp_sums[lane] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += t;
+            }
+            if (lane < nw) warp_sums[lane] = x;
+        }
+        __syncthreads();
+        const int excl = carry + (wid > 0 ? warp_sums[wid - 1] : 0) + incl - a;
+        if (b < nbins) slot_of_bin[b] = excl;  // exclusive prefix for now
+        if (a) bin_of_slot[excl] = b;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += warp_sums[nw - 1];
+        __syncthreads();
+    }
+    const int total = carry;
+    for (int t = threadIdx.x; t < ntowers; t += blockDim.x) {
+        const int first = slot_of_bin[t * nfloor];
+        const int next = (t + 1 < ntowers) ? slot_of_bin[(t + 1) * nfloor] : total;
+        tower_first[t] = first;
+        tower_count[t] = next - first;
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < nbins; b += blockDim.x)
+        if (!active[b]) slot_of_bin[b] = -1;
+    if (threadIdx.x == 0) *n_active = total;
+}
+
+void launch_compact_bins(cudaStream_t s, const int *active, int nbins, int nfloor, int *slot_of_bin,
+                         int *bin_of_slot, int *n_active, int *tower_first, int *tower_count,
+                         int ntowers)
+{
+    compact_bins_kernel<<<1, 1024, 0, s>>>(active, nbins, nfloor, slot_of_bin, bin_of_slot,
+                                           n_active, tower_first, tower_count, ntowers);
+}
+
+}  // namespace rg

@@ -1,0 +1,107 @@
+// Romein scatter gridder (Romein 2012, "An efficient work-distribution
+// strategy for gridding radio-telescope data on GPUs"), FP32.
+//
+// A CTA has K*K threads; thread (myU, myV) owns the grid points whose column is
+// congruent to myU and row to myV modulo K.  For each visibility with footprint
+// origin (col0, row0) exactly one tap of the K x K footprint falls on a point
+// the thread owns: column col0 + ((myU - col0) mod K), likewise for rows.  The
+// thread keeps a register sum for its current point and only flushes it (one
+// 8-byte vector atomic) when the point or the (tower, floor) sub-grid changes,
+// so visibilities that move slowly along a baseline track coalesce in
+// registers.  Per tap: sum += vis * conj(tap), the reference's
+// grid += v * conj(wk) (src/reference/grid.c:177-182).
+//
+// The linear index (row0 + cv) * side + (col0 + cu) is the reference's
+// grid_offset + y*size + x; points outside [0, side^2) are dropped (the
+// reference does not check, grid.c:177-182; its GPU gridder drops them,
+// src/grid/grid_cuda.cu:25-41).
+//
+// Visibilities are staged through shared memory in batches (coalesced 16-byte
+// record and 8-byte visibility loads); taps are read through the read-only
+// cache, one oversampled K x K slice per visibility.
+#include "rg_internal.h"
+
+namespace rg {
+
+template <int K>
+__global__ void __launch_bounds__(K *K) romein_kernel(
+    const int4 *__restrict__ rec, const float2 *__restrict__ visf, int64_t n,
+    const float2 *__restrict__ taps, float2 *__restrict__ grids,
+    const int *__restrict__ slot_of_bin, int64_t grid_stride, int side, int64_t chunk)
+{
+    constexpr int BATCH = K * K;
+    __shared__ int4 srec[BATCH];
+    __shared__ float2 svis[BATCH];
+    const int myU = threadIdx.x % K, myV = threadIdx.x / K;
+    const int64_t limit = (int64_t)side * side;
+
+    for (int64_t c0 = (int64_t)blockIdx.x * chunk; c0 < n; c0 += (int64_t)gridDim.x * chunk) {
+        const int64_t c1 = c0 + chunk < n ? c0 + chunk : n;
+        int cur_bin = -1;
+        int64_t cur_idx = 0;
+        float2 sum = make_float2(0.f, 0.f);
+        for (int64_t b0 = c0; b0 < c1; b0 += BATCH) {
+            const int cnt = (int)(c1 - b0 < BATCH ? c1 - b0 : BATCH);
+            __syncthreads();
+            if ((int)threadIdx.x < cnt) {
+                srec[threadIdx.x] = rec[b0 + threadIdx.x];
+                svis[threadIdx.x] = visf[b0 + threadIdx.x];
+            }
+            __syncthreads();
+            for (int j = 0; j < cnt; j++) {
+                const int4 r = srec[j];
+                if (r.x < 0) continue;
+                const int col0 = (int)(short)(r.y & 0xffff);
+                const int row0 = r.y >> 16;
+                const int cu = (myU - col0) & (K - 1);
+                const int cv = (myV - row0) & (K - 1);
+                const int64_t idx = (int64_t)(row0 + cv) * side + (col0 + cu);
+                if (r.x != cur_bin || idx != cur_idx) {
+                    if (cur_bin >= 0 && cur_idx >= 0 && cur_idx < limit)
+                        atomicAdd(grids + (int64_t)slot_of_bin[cur_bin] * grid_stride + cur_idx, sum);
+                    cur_bin = r.x;
+                    cur_idx = idx;
+                    sum = make_float2(0.f, 0.f);
+                }
+                const float2 t = __ldg(taps + r.z + cv * K + cu);
+                const float2 vz = svis[j];
+                sum.x = fmaf(vz.x, t.x, fmaf(vz.y, t.y, sum.x));
+                sum.y = fmaf(vz.y, t.x, fmaf(-vz.x, t.y, sum.y));
+            }
+        }
+        if (cur_bin >= 0 && cur_idx >= 0 && cur_idx < limit)
+            atomicAdd(grids + (int64_t)slot_of_bin[cur_bin] * grid_stride + cur_idx, sum);
+    }
+}
+
+void launch_romein(cudaStream_t s, const int4 *rec, const float2 *visf, int64_t n,
+                   const float2 *taps, float2 *grids, const int *slot_of_bin, int64_t grid_stride,
+                   int grid_side, int ksize, int sm_count)
+{
+    const int64_t chunk = 1024;
+    int64_t blocks = (n + chunk - 1) / chunk;
+    const int64_t cap = (int64_t)sm_count * 8;
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    switch (ksize) {
+        case 4:
+            romein_kernel<4><<<(unsigned)blocks, 16, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin,
+                                                             grid_stride, grid_side, chunk);
+            break;
+        case 8:
+            romein_kernel<8><<<(unsigned)blocks, 64, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin,
+                                                             grid_stride, grid_side, chunk);
+            break;
+        case 16:
+            romein_kernel<16><<<(unsigned)blocks, 256, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin,
+                                                               grid_stride, grid_side, chunk);
+            break;
+        case 32:
+            romein_kernel<32><<<(unsigned)blocks, 1024, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin,
+                                                                grid_stride, grid_side, chunk);
+            break;
+        default: break;
+    }
+}
+
+}  // namespace rg

@@ -1,0 +1,78 @@
+// W-towers helpers: the Fresnel phase table and the owner-computes add-back of
+// the towers' sub-grids into the FP64 master grid.
+#include "rg_internal.h"
+
+namespace rg {
+
+// ph[y*S + x] = winc (1 - sqrt(1 - l^2 - m^2)) for the fft-shifted pixel (y, x),
+// i.e. the reference's transfer pattern phase before cexp, at centred
+// coordinates ((x + S/2) mod S, (y + S/2) mod S) (src/reference/grid.c:304-319
+// followed by fft_shift); the column stage raises exp(2 pi i ph) to the power
+// -wp by multiplying the phase.  Round-to-nearest intrinsics: no contraction.
+__global__ void fresnel_table_kernel(double *__restrict__ ph, int S, double theta, double winc)
+{
+    const int64_t total = (int64_t)S * S;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int y = (int)(k / S), x = (int)(k % S);
+        const int xc = (x + S / 2) % S, yc = (y + S / 2) % S;
+        const double l = __ddiv_rn(__dmul_rn(theta, (double)(xc - S / 2)), (double)S);
+        const double m = __ddiv_rn(__dmul_rn(theta, (double)(yc - S / 2)), (double)S);
+        const double r = __dsqrt_rn(__dsub_rn(__dsub_rn(1.0, __dmul_rn(l, l)), __dmul_rn(m, m)));
+        ph[k] = __dmul_rn(winc, __dsub_rn(1.0, r));
+    }
+}
+
+void launch_fresnel_table(cudaStream_t s, double *ph, int subgrid, double theta, double winc)
+{
+    const int64_t total = (int64_t)subgrid * subgrid;
+    int blocks = (int)((total + 255) / 256);
+    if (blocks > 4096) blocks = 4096;
+    fresnel_table_kernel<<<blocks, 256, 0, s>>>(ph, subgrid, theta, winc);
+}
+
+// Owner-computes add-back (src/reference/grid.c:503-516): every master pixel
+// sums, in tower order (cy, then cx), the overlapping towers' forward-
+// transformed sub-images divided by S^2, in FP64.  Deterministic.
+__global__ void add_back_kernel(const float2 *__restrict__ subimg, const int *__restrict__ tower_count,
+                                double2 *__restrict__ master, int N, int S, int M, int chunk,
+                                int nchunk, int overwrite)
+{
+    const int gx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (gx >= N || gy >= N) return;
+    const int ax = gx + M / 2, ay = gy + M / 2;  // x + N/2 + M/2 with x = gx - N/2
+    int cx_hi = ax / chunk, cy_hi = ay / chunk;
+    int cx_lo = (ax - S) >= 0 ? (ax - S) / chunk + 1 : 0;
+    int cy_lo = (ay - S) >= 0 ? (ay - S) / chunk + 1 : 0;
+    if (cx_hi >= nchunk) cx_hi = nchunk - 1;
+    if (cy_hi >= nchunk) cy_hi = nchunk - 1;
+    const int64_t at = (int64_t)gy * N + gx;
+    double2 acc = overwrite ? make_double2(0.0, 0.0) : master[at];
+    const double norm = (double)(S * S);
+    for (int cy = cy_lo; cy <= cy_hi; cy++) {
+        const int sy = ay - chunk * cy;
+        if (sy < 0 || sy >= S) continue;
+        for (int cx = cx_lo; cx <= cx_hi; cx++) {
+            const int sx = ax - chunk * cx;
+            if (sx < 0 || sx >= S) continue;
+            const int t = cy * nchunk + cx;
+            if (tower_count[t] == 0) continue;
+            const float2 z = subimg[(int64_t)t * S * S + (int64_t)sy * S + sx];
+            acc.x += (double)z.x / norm;
+            acc.y += (double)z.y / norm;
+        }
+    }
+    master[at] = acc;
+}
+
+void launch_add_back(cudaStream_t s, const float2 *subimg, const int *tower_count, double2 *master,
+                     int grid_size, int subgrid, int margin, int chunk, int nchunk, int overwrite)
+{
+    dim3 blk(32, 8);
+    dim3 grd((grid_size + 31) / 32, (grid_size + 7) / 8);
+    add_back_kernel<<<grd, blk, 0, s>>>(subimg, tower_count, master, grid_size, subgrid, margin,
+                                        chunk, nchunk, overwrite);
+}
+
+}  // namespace rg

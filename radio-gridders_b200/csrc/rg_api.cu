@@ -1,0 +1,622 @@
+// C-ABI layer: argument checks, host/device staging, scratch management and
+// the launch sequences of each entry point (include/radio_gridders.h).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "rg_internal.h"
+
+namespace rg {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+rg_status fail(rg_status st, const std::string &msg)
+{
+    set_error(msg);
+    return st;
+}
+
+rg_status cuda_fail(cudaError_t e, const char *what)
+{
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    return fail(e == cudaErrorMemoryAllocation ? RG_ERR_OUT_OF_MEMORY : RG_ERR_CUDA, m);
+}
+
+bool is_device_pointer(const void *p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+rg_status scratch(rg_context *ctx, const char *name, size_t bytes, void **out)
+{
+    Buffer &b = ctx->scratch[name];
+    if (bytes == 0) bytes = 16;
+    if (b.bytes < bytes) {
+        if (b.ptr) {
+            cudaStreamSynchronize(ctx->stream);
+            cudaFree(b.ptr);
+            b.ptr = nullptr;
+            b.bytes = 0;
+        }
+        size_t want = bytes + bytes / 8;  // some headroom against regrowth
+        if (cudaMalloc(&b.ptr, want) != cudaSuccess) {
+            cudaGetLastError();
+            b.ptr = nullptr;
+            if (cudaMalloc(&b.ptr, bytes) != cudaSuccess) {
+                cudaGetLastError();
+                b.ptr = nullptr;
+                return fail(RG_ERR_OUT_OF_MEMORY,
+                            std::string("device allocation failed for scratch '") + name + "' (" +
+                                std::to_string(bytes) + " bytes)");
+            }
+            want = bytes;
+        }
+        b.bytes = want;
+    }
+    *out = b.ptr;
+    return RG_OK;
+}
+
+rg_status stage_in(rg_context *ctx, const void *ptr, size_t bytes, const char *name, const void **dev)
+{
+    if (bytes == 0) {
+        *dev = ptr;
+        return RG_OK;
+    }
+    if (is_device_pointer(ptr)) {
+        *dev = ptr;
+        return RG_OK;
+    }
+    void *d = nullptr;
+    RG_CHECK(scratch(ctx, name, bytes, &d));
+    RG_CUDA(cudaMemcpyAsync(d, ptr, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    *dev = d;
+    return RG_OK;
+}
+
+// Output view: device pointer itself, or a scratch buffer copied back by finish_out.
+struct OutView {
+    void *user = nullptr;
+    void *dev = nullptr;
+    size_t bytes = 0;
+    bool host = false;
+};
+
+static rg_status out_view(rg_context *ctx, void *ptr, size_t bytes, const char *name, bool load,
+                          OutView *ov)
+{
+    ov->user = ptr;
+    ov->bytes = bytes;
+    if (is_device_pointer(ptr)) {
+        ov->dev = ptr;
+        ov->host = false;
+        return RG_OK;
+    }
+    ov->host = true;
+    RG_CHECK(scratch(ctx, name, bytes, &ov->dev));
+    if (load) RG_CUDA(cudaMemcpyAsync(ov->dev, ptr, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    return RG_OK;
+}
+
+static rg_status finish_out(rg_context *ctx, const OutView &ov)
+{
+    if (ov.host) RG_CUDA(cudaMemcpyAsync(ov.user, ov.dev, ov.bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    return RG_OK;
+}
+
+static rg_status check_launch(const char *what)
+{
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    return RG_OK;
+}
+
+// Device error word + counters in one small scratch area.
+struct Diag {
+    unsigned *err;
+    unsigned long long *counters;  // [0] gridded, [1] dropped
+};
+
+static rg_status diag_begin(rg_context *ctx, Diag *d)
+{
+    void *p = nullptr;
+    RG_CHECK(scratch(ctx, "diag", 64, &p));
+    RG_CUDA(cudaMemsetAsync(p, 0, 64, ctx->stream));
+    d->err = (unsigned *)p;
+    d->counters = (unsigned long long *)((char *)p + 16);
+    return RG_OK;
+}
+
+static rg_status diag_end(rg_context *ctx, const Diag &d, unsigned long long *counters_out)
+{
+    unsigned char host[64];
+    RG_CUDA(cudaMemcpyAsync(host, d.err, 64, cudaMemcpyDeviceToHost, ctx->stream));
+    RG_CUDA(cudaStreamSynchronize(ctx->stream));
+    unsigned err;
+    std::memcpy(&err, host, sizeof(err));
+    if (counters_out) std::memcpy(counters_out, host + 16, 2 * sizeof(unsigned long long));
+    if (err & DERR_NONFINITE) return fail(RG_ERR_INVALID_ARGUMENT, "non-finite u, v or w in the visibilities");
+    if (err & DERR_PLANE_RANGE)
+        return fail(RG_ERR_INVALID_ARGUMENT, "a visibility's w (or sub-cell index) falls outside the w-kernel table");
+    if (err & DERR_GRID_RANGE)
+        return fail(RG_ERR_INVALID_ARGUMENT, "a visibility's kernel footprint lies outside the grid");
+    if (err & DERR_CAPACITY) return fail(RG_ERR_UNSUPPORTED, "internal capacity exceeded");
+    return RG_OK;
+}
+
+static rg_status check_vis(const rg_vis *vis)
+{
+    if (!vis) return fail(RG_ERR_INVALID_ARGUMENT, "vis is NULL");
+    if (vis->n < 0) return fail(RG_ERR_INVALID_ARGUMENT, "vis->n is negative");
+    if (vis->n > 0 && (!vis->u || !vis->v || !vis->w || !vis->vis))
+        return fail(RG_ERR_INVALID_ARGUMENT, "vis arrays must be non-NULL when n > 0");
+    if (vis->n > (int64_t)1 << 31) return fail(RG_ERR_UNSUPPORTED, "more than 2^31 visibilities in one call");
+    return RG_OK;
+}
+
+static rg_status check_wkern(const rg_wkern *wk)
+{
+    if (!wk || !wk->data) return fail(RG_ERR_INVALID_ARGUMENT, "w-kernel table is NULL");
+    if (wk->size != 4 && wk->size != 8 && wk->size != 16 && wk->size != 32)
+        return fail(RG_ERR_UNSUPPORTED, "kernel support must be 4, 8, 16 or 32 cells");
+    if (wk->oversampling < 1 || wk->oversampling > 64)
+        return fail(RG_ERR_INVALID_ARGUMENT, "oversampling must be in [1, 64]");
+    if (wk->plane_count < 1) return fail(RG_ERR_INVALID_ARGUMENT, "plane_count must be >= 1");
+    if (!(wk->w_step > 0.0) || !std::isfinite(wk->w_min))
+        return fail(RG_ERR_INVALID_ARGUMENT, "w_step must be > 0 and w_min finite");
+    const double taps = (double)wk->plane_count * wk->oversampling * wk->oversampling * wk->size * wk->size;
+    if (taps > 2.0e9) return fail(RG_ERR_UNSUPPORTED, "w-kernel table too large");
+    return RG_OK;
+}
+
+struct DevVis {
+    const double *u, *v, *w;
+    const double2 *vis;
+    int64_t n;
+};
+
+static rg_status stage_vis(rg_context *ctx, const rg_vis *vis, DevVis *dv)
+{
+    const size_t b = sizeof(double) * (size_t)vis->n;
+    const void *p;
+    RG_CHECK(stage_in(ctx, vis->u, b, "in_u", &p));
+    dv->u = (const double *)p;
+    RG_CHECK(stage_in(ctx, vis->v, b, "in_v", &p));
+    dv->v = (const double *)p;
+    RG_CHECK(stage_in(ctx, vis->w, b, "in_w", &p));
+    dv->w = (const double *)p;
+    RG_CHECK(stage_in(ctx, vis->vis, 2 * b, "in_vis", &p));
+    dv->vis = (const double2 *)p;
+    dv->n = vis->n;
+    return RG_OK;
+}
+
+static rg_status stage_taps(rg_context *ctx, const rg_wkern *wk, float2 **taps)
+{
+    const int64_t ntaps = (int64_t)wk->plane_count * wk->oversampling * wk->oversampling * wk->size * wk->size;
+    const void *src;
+    RG_CHECK(stage_in(ctx, wk->data, sizeof(double2) * ntaps, "in_wkern", &src));
+    void *dst;
+    RG_CHECK(scratch(ctx, "taps32", sizeof(float2) * ntaps, &dst));
+    launch_convert_table(ctx->stream, (const double2 *)src, (float2 *)dst, ntaps);
+    ctx->launches++;
+    *taps = (float2 *)dst;
+    return check_launch("convert w-kernel table");
+}
+
+static bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+static rg_status get_twiddles32(rg_context *ctx, int n, float2 **tw)
+{
+    std::string name = "tw32_" + std::to_string(n);
+    auto it = ctx->scratch.find(name);
+    bool fresh = it == ctx->scratch.end();
+    void *p;
+    RG_CHECK(scratch(ctx, name.c_str(), sizeof(float2) * n, &p));
+    if (fresh) fft32_init_twiddles(ctx->stream, (float2 *)p, n);
+    *tw = (float2 *)p;
+    return RG_OK;
+}
+
+}  // namespace rg
+
+using namespace rg;
+
+extern "C" {
+
+const char *rg_last_error(void) { return g_last_error.c_str(); }
+
+rg_status rg_context_create(int device, rg_context **out)
+{
+    if (!out) return fail(RG_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return fail(RG_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= count) return fail(RG_ERR_INVALID_ARGUMENT, "device index out of range");
+    RG_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    RG_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10)
+        return fail(RG_ERR_UNSUPPORTED, std::string("this build targets sm_100a (B200); device is ") + prop.name);
+    rg_context *ctx = new rg_context();
+    ctx->device = device;
+    ctx->sm_count = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return fail(RG_ERR_CUDA, "cudaStreamCreate failed");
+    }
+    ctx->stream = ctx->own_stream;
+    *out = ctx;
+    return RG_OK;
+}
+
+rg_status rg_context_destroy(rg_context *ctx)
+{
+    if (!ctx) return RG_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto &kv : ctx->scratch)
+        if (kv.second.ptr) cudaFree(kv.second.ptr);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return RG_OK;
+}
+
+rg_status rg_context_set_stream(rg_context *ctx, void *stream)
+{
+    if (!ctx) return fail(RG_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    return RG_OK;
+}
+
+int rg_last_stats(rg_context *ctx, int64_t *out, int n)
+{
+    if (!ctx || !out) return 0;
+    int k = n < 8 ? n : 8;
+    for (int i = 0; i < k; i++) out[i] = ctx->stats[i];
+    return k;
+}
+
+rg_status rg_grid_wprojection(rg_context *ctx, double *uvgrid, int grid_size, double theta,
+                              const rg_vis *vis, const rg_wkern *wkern, int flags)
+{
+    if (!ctx || !uvgrid) return fail(RG_ERR_INVALID_ARGUMENT, "ctx and uvgrid must be non-NULL");
+    if (grid_size < 2 || grid_size > 16384) return fail(RG_ERR_UNSUPPORTED, "grid_size must be in [2, 16384]");
+    if (!(theta > 0.0) || !std::isfinite(theta)) return fail(RG_ERR_INVALID_ARGUMENT, "theta must be > 0");
+    RG_CHECK(check_vis(vis));
+    RG_CHECK(check_wkern(wkern));
+    RG_CUDA(cudaSetDevice(ctx->device));
+    ctx->launches = 0;
+    const int N = grid_size;
+    const int64_t cells = (int64_t)N * N;
+    DevVis dv;
+    RG_CHECK(stage_vis(ctx, vis, &dv));
+    float2 *taps;
+    RG_CHECK(stage_taps(ctx, wkern, &taps));
+    Diag d;
+    RG_CHECK(diag_begin(ctx, &d));
+    void *rec, *visf, *grid32, *zero_slot;
+    RG_CHECK(scratch(ctx, "rec", sizeof(int4) * (size_t)dv.n, &rec));
+    RG_CHECK(scratch(ctx, "visf", sizeof(float2) * (size_t)dv.n, &visf));
+    RG_CHECK(scratch(ctx, "grid32", sizeof(float2) * (size_t)cells, &grid32));
+    RG_CHECK(scratch(ctx, "zero_slot", 16, &zero_slot));
+    RG_CUDA(cudaMemsetAsync(zero_slot, 0, 16, ctx->stream));
+    RG_CUDA(cudaMemsetAsync(grid32, 0, sizeof(float2) * (size_t)cells, ctx->stream));
+    if (dv.n > 0) {
+        launch_prepare_wproj(ctx->stream, dv.u, dv.v, dv.w, dv.vis, dv.n, N, theta, wkern->size,
+                             wkern->oversampling, wkern->plane_count, wkern->w_min, wkern->w_step,
+                             (int4 *)rec, (float2 *)visf, d.err);
+        launch_romein(ctx->stream, (const int4 *)rec, (const float2 *)visf, dv.n, taps,
+                      (float2 *)grid32, (const int *)zero_slot, 0, N, wkern->size, ctx->sm_count);
+        ctx->launches += 2;
+        RG_CHECK(check_launch("W-projection gridding"));
+    }
+    OutView ov;
+    RG_CHECK(out_view(ctx, uvgrid, sizeof(double2) * (size_t)cells, "out_grid",
+                      !(flags & RG_GRID_OVERWRITE), &ov));
+    launch_add_f32_to_f64(ctx->stream, (const float2 *)grid32, (double2 *)ov.dev, cells,
+                          (flags & RG_GRID_OVERWRITE) ? 1 : 0);
+    ctx->launches++;
+    RG_CHECK(check_launch("grid accumulation"));
+    RG_CHECK(finish_out(ctx, ov));
+    RG_CHECK(diag_end(ctx, d, nullptr));
+    ctx->stats[0] = dv.n;
+    ctx->stats[1] = 1;
+    ctx->stats[2] = 1;
+    ctx->stats[3] = 0;
+    ctx->stats[4] = 0;
+    ctx->stats[5] = ctx->launches;
+    return RG_OK;
+}
+
+rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double theta,
+                          const rg_vis *vis, const rg_wkern *wkern, int subgrid_size,
+                          int subgrid_margin, double wincrement, int flags)
+{
+    if (!ctx || !uvgrid) return fail(RG_ERR_INVALID_ARGUMENT, "ctx and uvgrid must be non-NULL");
+    if (grid_size < 2 || grid_size > 16384) return fail(RG_ERR_UNSUPPORTED, "grid_size must be in [2, 16384]");
+    if (!(theta > 0.0) || !std::isfinite(theta)) return fail(RG_ERR_INVALID_ARGUMENT, "theta must be > 0");
+    if (!(wincrement > 0.0) || !std::isfinite(wincrement))
+        return fail(RG_ERR_INVALID_ARGUMENT, "wincrement must be > 0");
+    RG_CHECK(check_vis(vis));
+    RG_CHECK(check_wkern(wkern));
+    const int S = subgrid_size, M = subgrid_margin, K = wkern->size;
+    // src/reference/grid.c:300-302
+    if (M < K) return fail(RG_ERR_INVALID_ARGUMENT, "subgrid margin must be >= the kernel support");
+    if (S % 2 || M % 2) return fail(RG_ERR_INVALID_ARGUMENT, "subgrid size and margin must be even");
+    if (M >= S) return fail(RG_ERR_INVALID_ARGUMENT, "subgrid margin must be smaller than the subgrid");
+    if (!fft32_supported(S)) return fail(RG_ERR_UNSUPPORTED, "subgrid size must be a power of two in [64, 1024]");
+    RG_CUDA(cudaSetDevice(ctx->device));
+    ctx->launches = 0;
+    const int N = grid_size;
+    const int64_t cells = (int64_t)N * N;
+    const int chunk = S - M;
+    const int nchunk = N / chunk + 1;
+    const int ntowers = nchunk * nchunk;
+    cudaStream_t st = ctx->stream;
+
+    DevVis dv;
+    RG_CHECK(stage_vis(ctx, vis, &dv));
+    float2 *taps;
+    RG_CHECK(stage_taps(ctx, wkern, &taps));
+    Diag d;
+    RG_CHECK(diag_begin(ctx, &d));
+    OutView ov;
+    RG_CHECK(out_view(ctx, uvgrid, sizeof(double2) * (size_t)cells, "out_grid",
+                      !(flags & RG_GRID_OVERWRITE), &ov));
+
+    // w range -> floors (grid.c:357-367)
+    void *mm;
+    RG_CHECK(scratch(ctx, "wminmax", 16, &mm));
+    launch_minmax_w(st, dv.u, dv.v, dv.w, dv.n, (double *)mm, d.err);
+    ctx->launches++;
+    RG_CHECK(check_launch("w range"));
+    double wr[2];
+    unsigned err0 = 0;
+    RG_CUDA(cudaMemcpyAsync(wr, mm, 16, cudaMemcpyDeviceToHost, st));
+    RG_CUDA(cudaMemcpyAsync(&err0, d.err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    RG_CUDA(cudaStreamSynchronize(st));
+    if (err0 & DERR_NONFINITE) return fail(RG_ERR_INVALID_ARGUMENT, "non-finite u, v or w in the visibilities");
+    const int wp_min = (int)std::floor(wr[0] / wincrement + 0.5);
+    const int wp_max = (int)std::floor(wr[1] / wincrement + 0.5);
+    const int64_t nfloor64 = (int64_t)wp_max - wp_min + 1;
+    const int64_t nbins64 = nfloor64 * ntowers;
+    if (nfloor64 > (1 << 20) || nbins64 > (int64_t)1 << 28)
+        return fail(RG_ERR_UNSUPPORTED, "too many (tower, w-floor) bins; increase wincrement");
+    const int nfloor = (int)nfloor64, nbins = (int)nbins64;
+
+    void *active, *rec, *visf, *slot_of_bin, *bin_of_slot, *nact, *tfirst, *tcount;
+    RG_CHECK(scratch(ctx, "active", sizeof(int) * (size_t)nbins, &active));
+    RG_CHECK(scratch(ctx, "rec", sizeof(int4) * (size_t)dv.n, &rec));
+    RG_CHECK(scratch(ctx, "visf", sizeof(float2) * (size_t)dv.n, &visf));
+    RG_CHECK(scratch(ctx, "slot_of_bin", sizeof(int) * (size_t)nbins, &slot_of_bin));
+    RG_CHECK(scratch(ctx, "bin_of_slot", sizeof(int) * (size_t)nbins, &bin_of_slot));
+    RG_CHECK(scratch(ctx, "n_active", 16, &nact));
+    RG_CHECK(scratch(ctx, "tower_first", sizeof(int) * (size_t)ntowers, &tfirst));
+    RG_CHECK(scratch(ctx, "tower_count", sizeof(int) * (size_t)ntowers, &tcount));
+    RG_CUDA(cudaMemsetAsync(active, 0, sizeof(int) * (size_t)nbins, st));
+
+    TowerGeom g;
+    g.grid_size = N;
+    g.subgrid = S;
+    g.margin = M;
+    g.chunk = chunk;
+    g.nchunk = nchunk;
+    g.ksize = K;
+    g.ov = wkern->oversampling;
+    g.planes = wkern->plane_count;
+    g.theta = theta;
+    g.winc = wincrement;
+    g.wk_wmin = wkern->w_min;
+    g.wk_wstep = wkern->w_step;
+    if (dv.n > 0) {
+        launch_prepare_towers(st, dv.u, dv.v, dv.w, dv.vis, dv.n, g, wp_min, nfloor, (int4 *)rec,
+                              (float2 *)visf, (int *)active, d.err, d.counters);
+        ctx->launches++;
+    }
+    launch_compact_bins(st, (const int *)active, nbins, nfloor, (int *)slot_of_bin, (int *)bin_of_slot,
+                        (int *)nact, (int *)tfirst, (int *)tcount, ntowers);
+    ctx->launches++;
+    RG_CHECK(check_launch("tower binning"));
+    int n_active = 0;
+    RG_CUDA(cudaMemcpyAsync(&n_active, nact, sizeof(int), cudaMemcpyDeviceToHost, st));
+    RG_CUDA(cudaStreamSynchronize(st));
+
+    const int64_t sub_cells = (int64_t)S * S;
+    void *slots = nullptr, *subimg = nullptr, *ph = nullptr;
+    float2 *tw;
+    RG_CHECK(get_twiddles32(ctx, S, &tw));
+    RG_CHECK(scratch(ctx, "subimg", sizeof(float2) * (size_t)(sub_cells * ntowers), &subimg));
+    // Fresnel phase table, cached per (S, theta, winc)
+    {
+        char key[160];
+        std::snprintf(key, sizeof(key), "ph_%d_%.17g_%.17g", S, theta, wincrement);
+        bool fresh = ctx->scratch.find(key) == ctx->scratch.end();
+        RG_CHECK(scratch(ctx, key, sizeof(double) * (size_t)sub_cells, &ph));
+        if (fresh) {
+            launch_fresnel_table(st, (double *)ph, S, theta, wincrement);
+            ctx->launches++;
+        }
+    }
+    if (n_active > 0) {
+        RG_CHECK(scratch(ctx, "slots", sizeof(float2) * (size_t)(sub_cells * n_active), &slots));
+        RG_CUDA(cudaMemsetAsync(slots, 0, sizeof(float2) * (size_t)(sub_cells * n_active), st));
+        launch_romein(st, (const int4 *)rec, (const float2 *)visf, dv.n, taps, (float2 *)slots,
+                      (const int *)slot_of_bin, sub_cells, S, K, ctx->sm_count);
+        launch_fft32_rows(st, (float2 *)slots, (int64_t)n_active * S, S, +1, tw);
+        launch_tower_columns(st, (float2 *)slots, (const int *)bin_of_slot, (const int *)tfirst,
+                             (const int *)tcount, ntowers, nfloor, wp_min, wincrement,
+                             (const double *)ph, (float2 *)subimg, S, tw);
+        launch_fft32_rows(st, (float2 *)subimg, (int64_t)ntowers * S, S, -1, tw);
+        ctx->launches += 4;
+        RG_CHECK(check_launch("tower gridding / transforms"));
+    }
+    launch_add_back(st, (const float2 *)subimg, (const int *)tcount, (double2 *)ov.dev, N, S, M, chunk,
+                    nchunk, (flags & RG_GRID_OVERWRITE) ? 1 : 0);
+    ctx->launches++;
+    RG_CHECK(check_launch("add-back"));
+    RG_CHECK(finish_out(ctx, ov));
+    unsigned long long counters[2] = {0, 0};
+    RG_CHECK(diag_end(ctx, d, counters));
+    std::vector<int> tc(ntowers);
+    RG_CUDA(cudaMemcpy(tc.data(), tcount, sizeof(int) * ntowers, cudaMemcpyDeviceToHost));
+    int with_data = 0;
+    for (int c : tc) with_data += c > 0;
+    ctx->stats[0] = (int64_t)counters[0];
+    ctx->stats[1] = n_active;
+    ctx->stats[2] = with_data;
+    ctx->stats[3] = nfloor;
+    ctx->stats[4] = (int64_t)counters[1];
+    ctx->stats[5] = ctx->launches;
+    return RG_OK;
+}
+
+rg_status rg_weight(rg_context *ctx, int grid_size, double theta, const rg_vis *vis, double *vis_out)
+{
+    if (!ctx || !vis_out) return fail(RG_ERR_INVALID_ARGUMENT, "ctx and vis_out must be non-NULL");
+    if (grid_size < 2) return fail(RG_ERR_INVALID_ARGUMENT, "grid_size must be >= 2");
+    RG_CHECK(check_vis(vis));
+    RG_CUDA(cudaSetDevice(ctx->device));
+    DevVis dv;
+    RG_CHECK(stage_vis(ctx, vis, &dv));
+    const int64_t cells = (int64_t)grid_size * grid_size;
+    void *count;
+    RG_CHECK(scratch(ctx, "wcount", sizeof(unsigned) * (size_t)cells, &count));
+    RG_CUDA(cudaMemsetAsync(count, 0, sizeof(unsigned) * (size_t)cells, ctx->stream));
+    OutView ov;
+    RG_CHECK(out_view(ctx, vis_out, sizeof(double2) * (size_t)dv.n, "out_vis", false, &ov));
+    if (dv.n > 0) {
+        launch_weight_count(ctx->stream, dv.u, dv.v, dv.n, grid_size, theta, (unsigned *)count);
+        launch_weight_apply(ctx->stream, dv.u, dv.v, dv.vis, (double2 *)ov.dev, dv.n, grid_size, theta,
+                            (const unsigned *)count);
+        RG_CHECK(check_launch("weighting"));
+    }
+    RG_CHECK(finish_out(ctx, ov));
+    RG_CUDA(cudaStreamSynchronize(ctx->stream));
+    return RG_OK;
+}
+
+static rg_status grid_inplace(rg_context *ctx, double *uvgrid, int grid_size, int op)
+{
+    if (!ctx || !uvgrid) return fail(RG_ERR_INVALID_ARGUMENT, "ctx and uvgrid must be non-NULL");
+    if (grid_size < 2 || (op == 1 && grid_size % 2))
+        return fail(RG_ERR_INVALID_ARGUMENT, "grid_size must be >= 2 (and even for fft_shift)");
+    RG_CUDA(cudaSetDevice(ctx->device));
+    const int64_t cells = (int64_t)grid_size * grid_size;
+    OutView ov;
+    RG_CHECK(out_view(ctx, uvgrid, sizeof(double2) * (size_t)cells, "out_grid", true, &ov));
+    if (op == 0) launch_make_hermitian(ctx->stream, (double2 *)ov.dev, grid_size);
+    else launch_fft_shift(ctx->stream, (double2 *)ov.dev, grid_size);
+    RG_CHECK(check_launch(op == 0 ? "make_hermitian" : "fft_shift"));
+    RG_CHECK(finish_out(ctx, ov));
+    RG_CUDA(cudaStreamSynchronize(ctx->stream));
+    return RG_OK;
+}
+
+rg_status rg_make_hermitian(rg_context *ctx, double *uvgrid, int grid_size)
+{
+    return grid_inplace(ctx, uvgrid, grid_size, 0);
+}
+
+rg_status rg_fft_shift(rg_context *ctx, double *uvgrid, int grid_size)
+{
+    return grid_inplace(ctx, uvgrid, grid_size, 1);
+}
+
+rg_status rg_image_from_grid(rg_context *ctx, double *uvgrid, int grid_size, double *image_out,
+                             const double *taper_1d)
+{
+    if (!ctx || !uvgrid || !image_out) return fail(RG_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (!fft64_supported(grid_size) || grid_size < 2)
+        return fail(RG_ERR_UNSUPPORTED, "image formation needs a power-of-two grid_size in [2, 4096]");
+    RG_CUDA(cudaSetDevice(ctx->device));
+    const int N = grid_size;
+    const int64_t cells = (int64_t)N * N;
+    OutView g;
+    RG_CHECK(out_view(ctx, uvgrid, sizeof(double2) * (size_t)cells, "img_grid", true, &g));
+    void *tmp;
+    RG_CHECK(scratch(ctx, "img_tmp", sizeof(double2) * (size_t)cells, &tmp));
+    const void *taper = nullptr;
+    if (taper_1d) RG_CHECK(stage_in(ctx, taper_1d, sizeof(double) * N, "img_taper", &taper));
+    OutView img;
+    RG_CHECK(out_view(ctx, image_out, sizeof(double) * (size_t)cells, "img_out", false, &img));
+    launch_make_hermitian(ctx->stream, (double2 *)g.dev, N);
+    launch_fft_shift(ctx->stream, (double2 *)g.dev, N);
+    launch_fft64_2d(ctx->stream, (double2 *)g.dev, (double2 *)tmp, 1, N, N, -1);
+    launch_fft_shift(ctx->stream, (double2 *)g.dev, N);
+    launch_real_part(ctx->stream, (const double2 *)g.dev, (double *)img.dev, N, (const double *)taper);
+    RG_CHECK(check_launch("image formation"));
+    RG_CHECK(finish_out(ctx, g));
+    RG_CHECK(finish_out(ctx, img));
+    RG_CUDA(cudaStreamSynchronize(ctx->stream));
+    return RG_OK;
+}
+
+rg_status rg_fft2d(rg_context *ctx, void *data, int batch, int ny, int nx, int sign, int complex_bytes)
+{
+    if (!ctx || !data) return fail(RG_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (batch < 1 || (sign != -1 && sign != 1)) return fail(RG_ERR_INVALID_ARGUMENT, "bad batch or sign");
+    RG_CUDA(cudaSetDevice(ctx->device));
+    const size_t bytes = (size_t)complex_bytes * batch * ny * nx;
+    if (complex_bytes == 8) {
+        if (ny != nx || !fft32_supported(nx))
+            return fail(RG_ERR_UNSUPPORTED, "FP32 transforms need square power-of-two sizes in [64, 1024]");
+        OutView ov;
+        RG_CHECK(out_view(ctx, data, bytes, "fft_data", true, &ov));
+        float2 *tw;
+        RG_CHECK(get_twiddles32(ctx, nx, &tw));
+        launch_fft32_rows(ctx->stream, (float2 *)ov.dev, (int64_t)batch * ny, nx, sign, tw);
+        launch_fft32_cols(ctx->stream, (float2 *)ov.dev, batch, nx, sign, tw);
+        RG_CHECK(check_launch("fft32"));
+        RG_CHECK(finish_out(ctx, ov));
+    } else if (complex_bytes == 16) {
+        if (!fft64_supported(nx) || !fft64_supported(ny))
+            return fail(RG_ERR_UNSUPPORTED, "FP64 transforms need power-of-two sizes <= 4096");
+        OutView ov;
+        RG_CHECK(out_view(ctx, data, bytes, "fft_data", true, &ov));
+        void *tmp;
+        RG_CHECK(scratch(ctx, "fft_tmp", bytes, &tmp));
+        launch_fft64_2d(ctx->stream, (double2 *)ov.dev, (double2 *)tmp, batch, ny, nx, sign);
+        RG_CHECK(check_launch("fft64"));
+        RG_CHECK(finish_out(ctx, ov));
+    } else {
+        return fail(RG_ERR_INVALID_ARGUMENT, "complex_bytes must be 8 or 16");
+    }
+    RG_CUDA(cudaStreamSynchronize(ctx->stream));
+    return RG_OK;
+}
+
+rg_status rg_dft_image(rg_context *ctx, double *image_out, int grid_size, double theta,
+                       const rg_vis *vis, int precision, double factor)
+{
+    if (!ctx || !image_out) return fail(RG_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (grid_size < 1 || grid_size > 65536) return fail(RG_ERR_INVALID_ARGUMENT, "bad grid_size");
+    if (precision < 0 || precision > 2) return fail(RG_ERR_INVALID_ARGUMENT, "unknown precision mode");
+    RG_CHECK(check_vis(vis));
+    RG_CUDA(cudaSetDevice(ctx->device));
+    DevVis dv;
+    RG_CHECK(stage_vis(ctx, vis, &dv));
+    OutView ov;
+    RG_CHECK(out_view(ctx, image_out, sizeof(double) * (size_t)grid_size * grid_size, "dft_out", false, &ov));
+    launch_dft(ctx->stream, dv.u, dv.v, dv.w, dv.vis, dv.n, (double *)ov.dev, grid_size, theta, precision,
+               factor, ctx->sm_count);
+    RG_CHECK(check_launch("dft"));
+    RG_CHECK(finish_out(ctx, ov));
+    RG_CUDA(cudaStreamSynchronize(ctx->stream));
+    return RG_OK;
+}
+
+}  // extern "C"

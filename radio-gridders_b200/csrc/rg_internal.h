@@ -1,0 +1,147 @@
+// Internal declarations shared by the C-ABI layer (rg_api.cu) and the kernel
+// files.  Not installed; the public interface is include/radio_gridders.h.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <string>
+
+#include "../../include/radio_gridders.h"
+
+namespace rg {
+
+// ---------------------------------------------------------------------------
+// status / errors
+// ---------------------------------------------------------------------------
+void set_error(const std::string &msg);
+rg_status fail(rg_status st, const std::string &msg);
+rg_status cuda_fail(cudaError_t e, const char *what);
+
+#define RG_CUDA(call)                                                  \
+    do {                                                               \
+        cudaError_t rg_e_ = (call);                                    \
+        if (rg_e_ != cudaSuccess) return ::rg::cuda_fail(rg_e_, #call); \
+    } while (0)
+
+#define RG_CHECK(call)                     \
+    do {                                   \
+        rg_status rg_s_ = (call);          \
+        if (rg_s_ != RG_OK) return rg_s_;  \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// device error word written by kernels (bit flags)
+// ---------------------------------------------------------------------------
+enum DeviceError : unsigned {
+    DERR_NONFINITE = 1u << 0,     // NaN/Inf in u, v, w
+    DERR_PLANE_RANGE = 1u << 1,   // w outside the kernel table
+    DERR_GRID_RANGE = 1u << 2,    // footprint leaves the grid (W-projection)
+    DERR_CAPACITY = 1u << 3,      // internal capacity exceeded
+};
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+struct Buffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace rg
+
+struct rg_context {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::map<std::string, rg::Buffer> scratch;
+    void *pinned = nullptr;  // small pinned host buffer for scalars
+    int64_t stats[8] = {0};
+    int launches = 0;
+};
+
+namespace rg {
+
+// Device scratch that persists in the context and grows on demand.
+rg_status scratch(rg_context *ctx, const char *name, size_t bytes, void **out);
+
+// Device view of a caller buffer: the pointer itself when device-accessible,
+// else a scratch copy (host -> device on the context stream).
+rg_status stage_in(rg_context *ctx, const void *ptr, size_t bytes, const char *name,
+                   const void **dev);
+bool is_device_pointer(const void *p);
+
+// ---------------------------------------------------------------------------
+// kernel launchers (defined in k_*.cu)
+// ---------------------------------------------------------------------------
+
+// k_image.cu
+void launch_convert_table(cudaStream_t s, const double2 *src, float2 *dst, int64_t n);
+void launch_make_hermitian(cudaStream_t s, double2 *grid, int n);
+void launch_fft_shift(cudaStream_t s, double2 *grid, int n);
+void launch_real_part(cudaStream_t s, const double2 *grid, double *img, int n,
+                      const double *taper);
+void launch_weight_count(cudaStream_t s, const double *u, const double *v, int64_t nvis,
+                         int n, double theta, unsigned *count);
+void launch_weight_apply(cudaStream_t s, const double *u, const double *v,
+                         const double2 *vis, double2 *out, int64_t nvis, int n, double theta,
+                         const unsigned *count);
+void launch_add_f32_to_f64(cudaStream_t s, const float2 *src, double2 *dst, int64_t n,
+                           int overwrite);
+
+// k_fft.cu — FP32 four-step FFTs for power-of-two n in [64, 1024]
+bool fft32_supported(int n);
+void fft32_init_twiddles(cudaStream_t s, float2 *tw, int n);  // tw: n entries
+// batched row transforms: rows = count of rows of length n (contiguous)
+void launch_fft32_rows(cudaStream_t s, float2 *data, int64_t rows, int n, int sign,
+                       const float2 *tw);
+// column transforms of `batch` n x n arrays
+void launch_fft32_cols(cudaStream_t s, float2 *data, int batch, int n, int sign,
+                       const float2 *tw);
+// FP64 transforms for image formation (n power of two, <= 4096)
+bool fft64_supported(int n);
+void launch_fft64_2d(cudaStream_t s, double2 *data, double2 *tmp, int batch, int ny, int nx,
+                     int sign);
+
+// k_prepare.cu
+struct TowerGeom {
+    int grid_size, subgrid, margin, chunk, nchunk, ksize, ov, planes;
+    double theta, winc, wk_wmin, wk_wstep;
+};
+void launch_minmax_w(cudaStream_t s, const double *u, const double *v, const double *w,
+                     int64_t n, double *out4, unsigned *err);
+void launch_prepare_towers(cudaStream_t s, const double *u, const double *v, const double *w,
+                           const double2 *vis, int64_t n, TowerGeom g, int wp_min, int nfloor,
+                           int4 *rec, float2 *visf, int *active, unsigned *err,
+                           unsigned long long *counters);
+void launch_prepare_wproj(cudaStream_t s, const double *u, const double *v, const double *w,
+                          const double2 *vis, int64_t n, int grid_size, double theta,
+                          int ksize, int ov, int planes, double wk_wmin, double wk_wstep,
+                          int4 *rec, float2 *visf, unsigned *err);
+void launch_compact_bins(cudaStream_t s, const int *active, int nbins, int nfloor, int *slot_of_bin,
+                         int *bin_of_slot, int *n_active, int *tower_first, int *tower_count,
+                         int ntowers);
+
+// k_romein.cu
+void launch_romein(cudaStream_t s, const int4 *rec, const float2 *visf, int64_t n,
+                   const float2 *taps, float2 *grids, const int *slot_of_bin,
+                   int64_t grid_stride, int grid_side, int ksize, int sm_count);
+
+// k_towers.cu
+void launch_fresnel_table(cudaStream_t s, double *ph, int subgrid, double theta, double winc);
+void launch_tower_columns(cudaStream_t s, float2 *slots, const int *bin_of_slot,
+                          const int *tower_first, const int *tower_count, int ntowers,
+                          int nfloor, int wp_min, double winc, const double *ph,
+                          float2 *subimg, int subgrid, const float2 *tw);
+void launch_add_back(cudaStream_t s, const float2 *subimg, const int *tower_count,
+                     double2 *master, int grid_size, int subgrid, int margin, int chunk,
+                     int nchunk, int overwrite);
+
+// k_dft.cu
+void launch_dft(cudaStream_t s, const double *u, const double *v, const double *w,
+                const double2 *vis, int64_t n, double *image, int grid_size, double theta,
+                int precision, double factor, int sm_count);
+
+}  // namespace rg
