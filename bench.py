@@ -1,0 +1,388 @@
+#!/usr/bin/env python
+"""W-towers gridding throughput on B200 (visibilities per second).
+
+One step = one rg_grid_wtowers call over one observation resident in HBM:
+w-range reduction, per-visibility tower/floor binning and coordinates, Romein
+gridding of every active (tower, w-floor) sub-grid, backward row transforms,
+the fused column-transform / Fresnel-step / w=0-transfer / forward-column
+stage, forward row transforms and the FP64 add-back into the master grid — the
+loop of the reference's grid_wtowers (src/reference/grid.c:295-555) and
+wtowers_CUDA_flat (src/grid/grid_cuda.cu:522-744) up to the final FFT.
+
+Workload (N = 1): the W-towers configuration — 2048 x 2048 grid (theta 0.1,
+lambda 20480), 512-cell sub-grids with 16-cell margins, w-increment 10,
+SKA-Low-like 256 stations (32,640 baselines x 16 dumps x 4 channels =
+2,088,960 visibilities), 16 x 16 taps at 8x oversampling.  Synthetic, seeded.
+With --gpus N each rank grids its own 32-minute snapshot (hour angles offset
+by rank) and the FP64 master grids are summed onto rank 0 with one NCCL
+reduce: per-GPU work is fixed (weak scaling).
+
+``--impl reference`` times the reference's own CPU grid_wtowers
+(src/reference/grid.c, compiled from its sources into oracle/_ref with its
+makefile flags and -DOMP_TOWERS) on the host cores, same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "W-towers vis/s on 1 B200 at <=1e-4 RMS vs FP64 DFT; learned vs table kernel"
+GRID, THETA, LAM, SUBGRID, MARGIN, WINC = 2048, 0.1, 20480.0, 512, 16, 10.0
+KSIZE, OVER = 16, 8
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def workload(rank: int):
+    """Rank r observes the r-th consecutive 32-minute snapshot of the same field."""
+    sim = importlib.import_module("radio-gridders_b200.simulate")
+    obs = sim.wtowers_plain(seed=1, ha_offset_hours=rank * 32.0 / 60.0)
+    wk = sim.generate_wkernel(THETA, np.arange(-5, 6, 1.0), KSIZE, OVER)
+    return obs, wk
+
+
+def peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for n, val in zip(names, parts[5:9]):
+                    if val.lower().startswith("active"):
+                        reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_bytes(stats, nvis, ntowers_data):
+    """Bytes per step of the reference dataflow (one HBM pass per stage):
+    20 B per visibility (3 x f32 uvw + c64), 48 S^2 per active (tower, floor),
+    24 S^2 per tower with data, 32 N^2 for the FP64 master read + write."""
+    s2 = SUBGRID * SUBGRID
+    return (20 * nvis + 48 * s2 * stats["active_subgrids"] + 24 * s2 * ntowers_data
+            + 32 * GRID * GRID)
+
+
+def stage_bytes(stage, stats, nvis):
+    """Algorithmic bytes of one launch of each stage (for the roofline)."""
+    s2 = SUBGRID * SUBGRID
+    na, nt = stats["active_subgrids"], stats["towers_with_data"]
+    ntow = (GRID // (SUBGRID - MARGIN) + 1) ** 2
+    return {
+        "zero_subgrids": 8 * s2 * na,                       # write
+        "romein": 24 * nvis + 8 * s2 * na,                  # records + vis in, sub-grids out
+        "fft_rows_backward": 16 * s2 * na,                  # read + write every sub-grid
+        "tower_columns": 8 * s2 * na + 8 * s2 * nt,         # read sub-grids, write sub-images
+        "fft_rows_forward": 16 * s2 * ntow,                 # read + write every sub-image
+        "add_back": 8 * s2 * nt + 16 * GRID * GRID,         # read sub-images, write master
+        "prepare": 40 * nvis + 24 * nvis,                   # f64 uvw + c128 in, record + c64 out
+    }.get(stage)
+
+
+def cpu_baseline(obs, wk, reps=1):
+    """The reference's own grid_wtowers (OMP_TOWERS build) on the host cores;
+    falls back to the single-threaded C restatement if the reference build is
+    absent.  Baselines whose footprint would fall before the reference's
+    sub-grid buffer are left out (grid.c:177-182 has no bounds check)."""
+    import oracle
+    cores = len(os.sched_getaffinity(0))
+    mask = oracle.reference_safe_baselines(obs, GRID, THETA, SUBGRID, MARGIN, KSIZE, OVER)
+    sub = oracle.subset_baselines(obs, mask)
+    if oracle.reference_available(omp=True):
+        times = []
+        for _ in range(reps):
+            t = time.perf_counter()
+            oracle.ref_grid_wtowers(GRID, THETA, sub, wk, SUBGRID, MARGIN, WINC, omp=True)
+            times.append(time.perf_counter() - t)
+        dt = min(times)
+        return {"value": sub.nvis / dt, "unit": "vis/s", "cores": cores, "kind": "reference",
+                "sample": (f"full workload less {int((~mask).sum())} of {len(mask)} baselines "
+                           f"whose footprints would leave the reference's sub-grid buffer; "
+                           f"{sub.nvis} vis, {dt:.2f} s, best of {reps}"),
+                "seconds": dt}
+    u, v, w, vis = sub.flat()
+    t = time.perf_counter()
+    oracle.grid_wtowers(GRID, THETA, u, v, w, vis, wk, SUBGRID, MARGIN, WINC)
+    dt = time.perf_counter() - t
+    return {"value": sub.nvis / dt, "unit": "vis/s", "cores": 1, "kind": "port",
+            "sample": f"full workload, {sub.nvis} vis, C restatement single-threaded, {dt:.2f} s",
+            "seconds": dt}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    import oracle
+    obs, wk = workload(0)
+    cores = len(os.sched_getaffinity(0))
+    if not oracle.reference_available(omp=True):
+        kind = "port"
+    else:
+        kind = "reference"
+    res = None
+    times = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(obs, wk)
+        if i >= args.warmup:
+            times.append(r["seconds"])
+        res = r
+    per = statistics.mean(times) if times else res["seconds"]
+    nvis = int(round(res["value"] * res["seconds"]))
+    value = nvis / per
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "vis/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": "wtowers_plain", "grid_size": GRID, "theta": THETA,
+                       "subgrid": SUBGRID, "margin": MARGIN, "winc": WINC},
+            "cpu_baseline": {"value": value, "unit": "vis/s", "cores": res["cores"] if kind == "reference" else 1,
+                             "kind": kind, "sample": res["sample"]},
+            "e2e": {"value": value, "unit": "vis/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    rg = importlib.import_module("radio-gridders_b200")
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    obs, wk = workload(rank)
+    u, v, w, vis = obs.flat()
+    nvis = len(u)
+
+    ctx = rg.Context(local_rank)
+    stream = torch.cuda.current_stream(dev)
+    ctx.set_stream(stream.cuda_stream)
+
+    # inputs resident in HBM
+    du = torch.from_numpy(u).to(dev)
+    dv = torch.from_numpy(v).to(dev)
+    dw = torch.from_numpy(w).to(dev)
+    dvis = torch.from_numpy(vis).to(dev)
+    dwk = torch.from_numpy(np.ascontiguousarray(wk.data)).to(dev)
+    grid = torch.zeros((GRID, GRID), dtype=torch.complex128, device=dev)
+    V = rg.Visibilities(du, dv, dw, dvis)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step():
+        ctx.grid_wtowers(grid, GRID, THETA, V, wk, SUBGRID, MARGIN, WINC,
+                         flags=rg.RG_GRID_OVERWRITE, wkern_data=dwk)
+        if world > 1:
+            dist.reduce(grid, dst=0)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    stats = ctx.last_stats()
+
+    # timed region
+    ctx.set_profiling(True)
+    clocks = Clocks(local_rank)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    step_ms, stage_ms, launches = [], {}, 0
+    for _ in range(args.steps):
+        flush.fill_(1)  # evict L2 between steps (outside the step's events)
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        step()
+        s1.record(stream)
+        s1.synchronize()
+        step_ms.append(s0.elapsed_time(s1))
+        for name, ms in ctx.last_timings():
+            stage_ms.setdefault(name, []).append(ms)
+        launches += ctx.last_stats()["launches"]
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ctx.set_profiling(False)
+
+    total = torch.tensor([sum(step_ms)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(total, op=dist.ReduceOp.MAX)
+    ms_per_step = total.item() / args.steps
+    value = nvis * world / (ms_per_step * 1e-3)
+
+    # end to end through the C ABI with pinned host buffers
+    hu = torch.from_numpy(u).pin_memory().numpy()
+    hv = torch.from_numpy(v).pin_memory().numpy()
+    hw = torch.from_numpy(w).pin_memory().numpy()
+    hvis = torch.from_numpy(vis).pin_memory().numpy()
+    hwk = torch.from_numpy(np.ascontiguousarray(wk.data)).pin_memory().numpy()
+    hgrid = torch.zeros((GRID, GRID), dtype=torch.complex128).pin_memory().numpy()
+    HV = rg.Visibilities(hu, hv, hw, hvis)
+    for _ in range(2):
+        ctx.grid_wtowers(hgrid, GRID, THETA, HV, wk, SUBGRID, MARGIN, WINC,
+                         flags=rg.RG_GRID_OVERWRITE, wkern_data=hwk)
+    torch.cuda.synchronize()
+    e2e_ms = []
+    for _ in range(args.steps):
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        ctx.grid_wtowers(hgrid, GRID, THETA, HV, wk, SUBGRID, MARGIN, WINC,
+                         flags=rg.RG_GRID_OVERWRITE, wkern_data=hwk)
+        t1.record(stream)
+        t1.synchronize()
+        e2e_ms.append(t0.elapsed_time(t1))
+    e2e_t = torch.tensor([sum(e2e_ms) / len(e2e_ms)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = nvis * world / (e2e_t.item() * 1e-3)
+    h2d = 8 * 3 * nvis + 16 * nvis + 16 * wk.data.size
+    d2h = 16 * GRID * GRID
+
+    if rank != 0:
+        return 0
+    # roofline of the dominant stage (HBM-bound)
+    peak, peak_kind = peaks()
+    kernel_stages = {k: statistics.mean(v) for k, v in stage_ms.items()
+                     if k not in ("stage_in", "stage_out", "w_range", "compact")}
+    dom = max(kernel_stages, key=kernel_stages.get)
+    dom_ms = kernel_stages[dom]
+    dom_bytes = stage_bytes(dom, stats, nvis)
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(REPO, "profiles", "wtowers_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get(dom)
+    path_bytes = algorithmic_bytes(stats, nvis, stats["towers_with_data"])
+    line = {
+        "impl": "b200", "metric": METRIC, "value": value, "unit": "vis/s", "n_gpus": world,
+        "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Earth-rotation synthesis, power-law point sources)",
+        "config": {"workload": "wtowers_plain: 2048x2048 grid (theta 0.1, lambda 20480), subgrid 512, "
+                               "margin 16, winc 10, 2,088,960 vis (256 stations, 16 dumps x 4 ch), "
+                               "16x16 taps x8 oversampled, 11 w-planes",
+                   "grid_size": GRID, "subgrid": SUBGRID, "margin": MARGIN, "winc": WINC,
+                   "vis_per_gpu": nvis, "active_subgrids": stats["active_subgrids"],
+                   "towers_with_data": stats["towers_with_data"], "floors": stats["floors"],
+                   "parallelism": f"{world} rank(s), one snapshot each, master grids reduced over NCCL",
+                   "l2": "256 MiB buffer written between steps, outside each step's event pair",
+                   "precision": "FP32 sub-grids and transforms; FP64 coordinates, Fresnel phase and master grid"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": dom_bytes, "launch_ms": dom_ms,
+                     "traffic": traffic},
+        "path_roofline": {"algorithmic_bytes_per_step": path_bytes,
+                          "achieved_gbs": path_bytes / (ms_per_step * 1e-3) / 1e9,
+                          "frac": path_bytes / (ms_per_step * 1e-3) / 1e9 / peak},
+        "stage_ms": {k: round(statistics.mean(v), 4) for k, v in stage_ms.items()},
+        "e2e": {"value": e2e_value, "unit": "vis/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_t.item()},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(obs, wk)
+        cb.pop("seconds", None)
+        line["cpu_baseline"] = cb
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        return run_b200(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -96,6 +96,13 @@ const char *rg_last_error(void);
  * launches issued by the call.  Returns the count written (<= n). */
 int rg_last_stats(rg_context *ctx, int64_t *out, int n);
 
+/* Per-stage timing (the reference's cudaEvent timing around gridding,
+ * src/grid/grid_cuda.cu:677-734).  When enabled, every stage of a call is
+ * bracketed by CUDA events on the context stream; rg_last_timings then returns
+ * the stage names and milliseconds of the last call (count written). */
+rg_status rg_context_set_profiling(rg_context *ctx, int enabled);
+int rg_last_timings(rg_context *ctx, const char **names, float *ms, int n);
+
 /* ---- gridders ---------------------------------------------------------- */
 
 /* W-projection, Romein scatter.  Replaces grid_wprojection

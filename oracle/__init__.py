@@ -186,6 +186,26 @@ class WKernData(ct.Structure):
 _ref_libs = {}
 
 
+class quiet_stdout:
+    """Silence C-level stdout (the reference prints progress with printf,
+    e.g. grid.c:406) so it cannot mix into a caller's output."""
+
+    def __enter__(self):
+        import sys
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+        return self
+
+    def __exit__(self, *exc):
+        ct.CDLL(None).fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+        return False
+
+
 def reference_available(omp=False):
     return os.path.exists(os.path.join(REF, "libref_grid_omp.so" if omp else "libref_grid.so"))
 
@@ -262,15 +282,17 @@ class RefInputs:
 def ref_grid_wprojection(grid_size, theta, obs, wk):
     r = RefInputs(obs, wk)
     grid = np.zeros((grid_size, grid_size), np.complex128)
-    ref_lib().grid_wprojection(_ptr(grid), grid_size, theta, ct.byref(r.vd), ct.byref(r.wkd))
+    with quiet_stdout():
+        ref_lib().grid_wprojection(_ptr(grid), grid_size, theta, ct.byref(r.vd), ct.byref(r.wkd))
     return grid
 
 
 def ref_grid_wtowers(grid_size, theta, obs, wk, subgrid, margin, winc, omp=False):
     r = RefInputs(obs, wk)
     grid = np.zeros((grid_size, grid_size), np.complex128)
-    ref_lib(omp).grid_wtowers(_ptr(grid), grid_size, theta, ct.byref(r.vd), ct.byref(r.wkd),
-                              subgrid, margin, winc)
+    with quiet_stdout():
+        ref_lib(omp).grid_wtowers(_ptr(grid), grid_size, theta, ct.byref(r.vd), ct.byref(r.wkd),
+                                  subgrid, margin, winc)
     return grid
 
 
@@ -291,3 +313,40 @@ def ref_fft_shift(grid):
     g = np.ascontiguousarray(grid, np.complex128).copy()
     ref_lib().fft_shift(_ptr(g), g.shape[0])
     return g
+
+
+def reference_safe_baselines(obs, grid_size, theta, subgrid, margin, ksize, ov):
+    """Boolean mask of baselines the reference's grid_wtowers can grid without
+    writing outside its sub-grid buffer.
+
+    With margin == kernel support, a visibility within 1/(2 ov) cell of a
+    tower's low edge gets a footprint origin on row -1 (or row 0, column -1) of
+    the sub-grid; grid.c's w_project has no bounds check (grid.c:177-182) and
+    writes before the buffer.  Such baselines are left out when the reference
+    itself is run; the restatement and the GPU path drop only the taps that
+    leave the buffer."""
+    u, v, w, _ = obs.flat()
+    chunk = subgrid - margin
+    row0 = _origin(v, theta, grid_size, chunk, subgrid, ksize, ov)
+    col0 = _origin(u, theta, grid_size, chunk, subgrid, ksize, ov)
+    bad = (row0 <= 0) | (col0 <= 0)
+    nbl = obs.uvw.shape[0]
+    return ~bad.reshape(nbl, -1).any(axis=1)
+
+
+def _origin(x, theta, n, chunk, s, k, ov):
+    c = np.floor((x * theta + 0.5 + n // 2) / chunk)
+    mid = (c * chunk - n // 2 + chunk // 2) / theta
+    cell = np.floor(theta * (x - mid) + 0.5 / ov)
+    return cell + s // 2 - k // 2
+
+
+def subset_baselines(obs, mask):
+    import copy
+    o = copy.copy(obs)
+    o.uvw = obs.uvw[mask]
+    o.freq = obs.freq[mask]
+    o.vis = obs.vis[mask]
+    o.antenna1 = obs.antenna1[mask]
+    o.antenna2 = obs.antenna2[mask]
+    return o

@@ -37,7 +37,7 @@ STATUS = {0: "RG_OK", 1: "RG_ERR_INVALID_ARGUMENT", 2: "RG_ERR_CUDA", 3: "RG_ERR
 # every symbol include/radio_gridders.h declares
 EXPORTS = [
     "rg_context_create", "rg_context_destroy", "rg_context_set_stream", "rg_last_error",
-    "rg_last_stats", "rg_grid_wprojection", "rg_grid_wtowers", "rg_weight",
+    "rg_last_stats", "rg_context_set_profiling", "rg_last_timings", "rg_grid_wprojection", "rg_grid_wtowers", "rg_weight",
     "rg_make_hermitian", "rg_fft_shift", "rg_image_from_grid", "rg_fft2d", "rg_dft_image",
 ]
 
@@ -80,6 +80,9 @@ def lib():
         L.rg_last_error.restype = ct.c_char_p
         L.rg_last_stats.argtypes = [vp, ct.POINTER(i64), i]
         L.rg_last_stats.restype = i
+        L.rg_context_set_profiling.argtypes = [vp, i]
+        L.rg_last_timings.argtypes = [vp, ct.POINTER(ct.c_char_p), ct.POINTER(ct.c_float), i]
+        L.rg_last_timings.restype = i
         L.rg_grid_wprojection.argtypes = [vp, vp, i, d, ct.POINTER(_Vis), ct.POINTER(_WKern), i]
         L.rg_grid_wtowers.argtypes = [vp, vp, i, d, ct.POINTER(_Vis), ct.POINTER(_WKern), i, i, d, i]
         L.rg_weight.argtypes = [vp, i, d, ct.POINTER(_Vis), vp]
@@ -170,6 +173,16 @@ class Context:
 
     def set_stream(self, stream_ptr):
         _check(lib().rg_context_set_stream(self._h, stream_ptr))
+
+    def set_profiling(self, enabled=True):
+        _check(lib().rg_context_set_profiling(self._h, 1 if enabled else 0))
+
+    def last_timings(self):
+        """[(stage, ms)] of the last call when profiling is enabled."""
+        names = (ct.c_char_p * 64)()
+        ms = (ct.c_float * 64)()
+        n = lib().rg_last_timings(self._h, names, ms, 64)
+        return [(names[k].decode(), float(ms[k])) for k in range(n)]
 
     def last_stats(self):
         out = (ct.c_int64 * 8)()

@@ -213,7 +213,45 @@ static rg_status stage_taps(rg_context *ctx, const rg_wkern *wk, float2 **taps)
     return check_launch("convert w-kernel table");
 }
 
-static bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+void begin_call(rg_context *ctx)
+{
+    ctx->n_events = 0;
+    ctx->timings.clear();
+    ctx->launches = 0;
+}
+
+void begin_stage(rg_context *ctx, const char *name)
+{
+    if (!ctx->profiling) return;
+    if (ctx->n_events == (int)ctx->events.size()) {
+        rg_stage_event e;
+        cudaEventCreate(&e.start);
+        cudaEventCreate(&e.stop);
+        ctx->events.push_back(e);
+    }
+    rg_stage_event &e = ctx->events[ctx->n_events];
+    e.name = name;
+    cudaEventRecord(e.start, ctx->stream);
+}
+
+void end_stage(rg_context *ctx)
+{
+    if (!ctx->profiling) return;
+    cudaEventRecord(ctx->events[ctx->n_events].stop, ctx->stream);
+    ctx->n_events++;
+}
+
+void collect_timings(rg_context *ctx)
+{
+    ctx->timings.clear();
+    if (!ctx->profiling) return;
+    for (int i = 0; i < ctx->n_events; i++) {
+        float ms = 0.f;
+        cudaEventSynchronize(ctx->events[i].stop);
+        cudaEventElapsedTime(&ms, ctx->events[i].start, ctx->events[i].stop);
+        ctx->timings.emplace_back(ctx->events[i].name, ms);
+    }
+}
 
 static rg_status get_twiddles32(rg_context *ctx, int n, float2 **tw)
 {
@@ -270,6 +308,10 @@ rg_status rg_context_destroy(rg_context *ctx)
     cudaStreamSynchronize(ctx->stream);
     for (auto &kv : ctx->scratch)
         if (kv.second.ptr) cudaFree(kv.second.ptr);
+    for (auto &e : ctx->events) {
+        cudaEventDestroy(e.start);
+        cudaEventDestroy(e.stop);
+    }
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return RG_OK;
@@ -280,6 +322,26 @@ rg_status rg_context_set_stream(rg_context *ctx, void *stream)
     if (!ctx) return fail(RG_ERR_INVALID_ARGUMENT, "ctx is NULL");
     ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
     return RG_OK;
+}
+
+rg_status rg_context_set_profiling(rg_context *ctx, int enabled)
+{
+    if (!ctx) return fail(RG_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    ctx->profiling = enabled != 0;
+    return RG_OK;
+}
+
+int rg_last_timings(rg_context *ctx, const char **names, float *ms, int n)
+{
+    if (!ctx) return 0;
+    int k = 0;
+    for (auto &t : ctx->timings) {
+        if (k >= n) break;
+        if (names) names[k] = t.first.c_str();
+        if (ms) ms[k] = t.second;
+        k++;
+    }
+    return k;
 }
 
 int rg_last_stats(rg_context *ctx, int64_t *out, int n)
@@ -299,13 +361,15 @@ rg_status rg_grid_wprojection(rg_context *ctx, double *uvgrid, int grid_size, do
     RG_CHECK(check_vis(vis));
     RG_CHECK(check_wkern(wkern));
     RG_CUDA(cudaSetDevice(ctx->device));
-    ctx->launches = 0;
+    begin_call(ctx);
     const int N = grid_size;
     const int64_t cells = (int64_t)N * N;
     DevVis dv;
+    begin_stage(ctx, "stage_in");
     RG_CHECK(stage_vis(ctx, vis, &dv));
     float2 *taps;
     RG_CHECK(stage_taps(ctx, wkern, &taps));
+    end_stage(ctx);
     Diag d;
     RG_CHECK(diag_begin(ctx, &d));
     void *rec, *visf, *grid32, *zero_slot;
@@ -316,23 +380,32 @@ rg_status rg_grid_wprojection(rg_context *ctx, double *uvgrid, int grid_size, do
     RG_CUDA(cudaMemsetAsync(zero_slot, 0, 16, ctx->stream));
     RG_CUDA(cudaMemsetAsync(grid32, 0, sizeof(float2) * (size_t)cells, ctx->stream));
     if (dv.n > 0) {
+        begin_stage(ctx, "prepare");
         launch_prepare_wproj(ctx->stream, dv.u, dv.v, dv.w, dv.vis, dv.n, N, theta, wkern->size,
                              wkern->oversampling, wkern->plane_count, wkern->w_min, wkern->w_step,
                              (int4 *)rec, (float2 *)visf, d.err);
+        end_stage(ctx);
+        begin_stage(ctx, "romein");
         launch_romein(ctx->stream, (const int4 *)rec, (const float2 *)visf, dv.n, taps,
                       (float2 *)grid32, (const int *)zero_slot, 0, N, wkern->size, ctx->sm_count);
+        end_stage(ctx);
         ctx->launches += 2;
         RG_CHECK(check_launch("W-projection gridding"));
     }
     OutView ov;
     RG_CHECK(out_view(ctx, uvgrid, sizeof(double2) * (size_t)cells, "out_grid",
                       !(flags & RG_GRID_OVERWRITE), &ov));
+    begin_stage(ctx, "to_fp64");
     launch_add_f32_to_f64(ctx->stream, (const float2 *)grid32, (double2 *)ov.dev, cells,
                           (flags & RG_GRID_OVERWRITE) ? 1 : 0);
+    end_stage(ctx);
     ctx->launches++;
     RG_CHECK(check_launch("grid accumulation"));
+    begin_stage(ctx, "stage_out");
     RG_CHECK(finish_out(ctx, ov));
+    end_stage(ctx);
     RG_CHECK(diag_end(ctx, d, nullptr));
+    collect_timings(ctx);
     ctx->stats[0] = dv.n;
     ctx->stats[1] = 1;
     ctx->stats[2] = 1;
@@ -360,7 +433,7 @@ rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double
     if (M >= S) return fail(RG_ERR_INVALID_ARGUMENT, "subgrid margin must be smaller than the subgrid");
     if (!fft32_supported(S)) return fail(RG_ERR_UNSUPPORTED, "subgrid size must be a power of two in [64, 1024]");
     RG_CUDA(cudaSetDevice(ctx->device));
-    ctx->launches = 0;
+    begin_call(ctx);
     const int N = grid_size;
     const int64_t cells = (int64_t)N * N;
     const int chunk = S - M;
@@ -369,6 +442,7 @@ rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double
     cudaStream_t st = ctx->stream;
 
     DevVis dv;
+    begin_stage(ctx, "stage_in");
     RG_CHECK(stage_vis(ctx, vis, &dv));
     float2 *taps;
     RG_CHECK(stage_taps(ctx, wkern, &taps));
@@ -377,11 +451,14 @@ rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double
     OutView ov;
     RG_CHECK(out_view(ctx, uvgrid, sizeof(double2) * (size_t)cells, "out_grid",
                       !(flags & RG_GRID_OVERWRITE), &ov));
+    end_stage(ctx);
 
     // w range -> floors (grid.c:357-367)
     void *mm;
     RG_CHECK(scratch(ctx, "wminmax", 16, &mm));
+    begin_stage(ctx, "w_range");
     launch_minmax_w(st, dv.u, dv.v, dv.w, dv.n, (double *)mm, d.err);
+    end_stage(ctx);
     ctx->launches++;
     RG_CHECK(check_launch("w range"));
     double wr[2];
@@ -422,13 +499,17 @@ rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double
     g.winc = wincrement;
     g.wk_wmin = wkern->w_min;
     g.wk_wstep = wkern->w_step;
+    begin_stage(ctx, "prepare");
     if (dv.n > 0) {
         launch_prepare_towers(st, dv.u, dv.v, dv.w, dv.vis, dv.n, g, wp_min, nfloor, (int4 *)rec,
                               (float2 *)visf, (int *)active, d.err, d.counters);
         ctx->launches++;
     }
+    end_stage(ctx);
+    begin_stage(ctx, "compact");
     launch_compact_bins(st, (const int *)active, nbins, nfloor, (int *)slot_of_bin, (int *)bin_of_slot,
                         (int *)nact, (int *)tfirst, (int *)tcount, ntowers);
+    end_stage(ctx);
     ctx->launches++;
     RG_CHECK(check_launch("tower binning"));
     int n_active = 0;
@@ -453,24 +534,39 @@ rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double
     }
     if (n_active > 0) {
         RG_CHECK(scratch(ctx, "slots", sizeof(float2) * (size_t)(sub_cells * n_active), &slots));
+        begin_stage(ctx, "zero_subgrids");
         RG_CUDA(cudaMemsetAsync(slots, 0, sizeof(float2) * (size_t)(sub_cells * n_active), st));
+        end_stage(ctx);
+        begin_stage(ctx, "romein");
         launch_romein(st, (const int4 *)rec, (const float2 *)visf, dv.n, taps, (float2 *)slots,
                       (const int *)slot_of_bin, sub_cells, S, K, ctx->sm_count);
+        end_stage(ctx);
+        begin_stage(ctx, "fft_rows_backward");
         launch_fft32_rows(st, (float2 *)slots, (int64_t)n_active * S, S, +1, tw);
+        end_stage(ctx);
+        begin_stage(ctx, "tower_columns");
         launch_tower_columns(st, (float2 *)slots, (const int *)bin_of_slot, (const int *)tfirst,
                              (const int *)tcount, ntowers, nfloor, wp_min, wincrement,
                              (const double *)ph, (float2 *)subimg, S, tw);
+        end_stage(ctx);
+        begin_stage(ctx, "fft_rows_forward");
         launch_fft32_rows(st, (float2 *)subimg, (int64_t)ntowers * S, S, -1, tw);
+        end_stage(ctx);
         ctx->launches += 4;
         RG_CHECK(check_launch("tower gridding / transforms"));
     }
+    begin_stage(ctx, "add_back");
     launch_add_back(st, (const float2 *)subimg, (const int *)tcount, (double2 *)ov.dev, N, S, M, chunk,
                     nchunk, (flags & RG_GRID_OVERWRITE) ? 1 : 0);
+    end_stage(ctx);
     ctx->launches++;
     RG_CHECK(check_launch("add-back"));
+    begin_stage(ctx, "stage_out");
     RG_CHECK(finish_out(ctx, ov));
+    end_stage(ctx);
     unsigned long long counters[2] = {0, 0};
     RG_CHECK(diag_end(ctx, d, counters));
+    collect_timings(ctx);
     std::vector<int> tc(ntowers);
     RG_CUDA(cudaMemcpy(tc.data(), tcount, sizeof(int) * ntowers, cudaMemcpyDeviceToHost));
     int with_data = 0;

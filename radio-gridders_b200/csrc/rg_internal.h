@@ -6,6 +6,7 @@
 
 #include <cstdint>
 #include <map>
+#include <vector>
 #include <string>
 
 #include "../../include/radio_gridders.h"
@@ -51,8 +52,17 @@ struct Buffer {
 
 }  // namespace rg
 
+struct rg_stage_event {
+    std::string name;
+    cudaEvent_t start = nullptr, stop = nullptr;
+};
+
 struct rg_context {
     int device = 0;
+    bool profiling = false;
+    std::vector<rg_stage_event> events;  // pool, reused across calls
+    int n_events = 0;                    // used by the current call
+    std::vector<std::pair<std::string, float>> timings;  // last call
     int sm_count = 148;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
@@ -63,6 +73,13 @@ struct rg_context {
 };
 
 namespace rg {
+
+// Stage timing: begin_stage/end_stage bracket launches with events when the
+// context is profiling; collect_timings (after a stream sync) fills timings.
+void begin_call(rg_context *ctx);
+void begin_stage(rg_context *ctx, const char *name);
+void end_stage(rg_context *ctx);
+void collect_timings(rg_context *ctx);
 
 // Device scratch that persists in the context and grows on demand.
 rg_status scratch(rg_context *ctx, const char *name, size_t bytes, void **out);

@@ -322,7 +322,8 @@ def wproj_plain(seed: int = 0, n_ant: int = 27, n_dump: int = 64, theta: float =
 
 def wtowers_plain(seed: int = 1, n_st: int = 256, n_dump: int = 16, n_chan: int = 4,
                   theta: float = 0.1, lam: float = 20480.0, ksize: int = 16,
-                  n_src: int = 50, dump_s: float = 120.0, r_max: float = 20_000.0):
+                  n_src: int = 50, dump_s: float = 120.0, r_max: float = 20_000.0,
+                  ha_offset_hours: float = 0.0):
     """W-towers workload: 2048x2048 grid (theta 0.1, lambda 20480), SKA-Low-like
     256 stations on a seeded log-radial layout (20 m .. 20 km radius, i.e.
     baselines to 40 km), 32,640 baselines x 16 dumps x 4 channels = 2,088,960
@@ -333,12 +334,12 @@ def wtowers_plain(seed: int = 1, n_st: int = 256, n_dump: int = 16, n_chan: int 
     rng = np.random.default_rng(seed)
     enu = log_radial(rng, n_st, 20.0, r_max)
     lat = dec = -26.8
-    ha = (np.arange(n_dump) - (n_dump - 1) / 2) * dump_s / 3600.0
+    ha = (np.arange(n_dump) - (n_dump - 1) / 2) * dump_s / 3600.0 + ha_offset_hours
     n_grid = int(theta * lam)
     limit = (n_grid / 2 - ksize / 2 - 2) / theta
     rel = 1.0 + 0.005 * np.arange(n_chan)
-    f0 = fit_scale(enu, lat, dec, ha, rel, limit)  # frequency knob (Hz * c units)
-    freqs = rel * f0 * C_LIGHT
+    f0 = fit_scale(enu, lat, dec, ha, rel, limit)  # frequency knob: base frequency in Hz
+    freqs = rel * f0
     src = random_sources(rng, n_src, theta, "powerlaw")
     obs = observe(enu, lat, dec, ha, freqs, src)
     obs.meta = dict(name="wtowers_plain", theta=theta, lam=lam, grid_size=n_grid,
@@ -348,12 +349,13 @@ def wtowers_plain(seed: int = 1, n_st: int = 256, n_dump: int = 16, n_chan: int 
 
 def wtowers_full(seed: int = 4, n_st: int = 512, n_dump: int = 32, n_chan: int = 2,
                  theta: float = 0.1, lam: float = 40960.0, ksize: int = 16,
-                 n_src: int = 100, dump_s: float = 60.0, r_max: float = 20_000.0):
+                 n_src: int = 100, dump_s: float = 60.0, r_max: float = 20_000.0,
+                 ha_offset_hours: float = 0.0):
     """Full-scale W-towers workload: 4096x4096 grid (theta 0.1, lambda 40960),
     512 stations -> 130,816 baselines x 32 dumps x 2 channels = 8,372,224
     visibilities, 100 power-law sources; same knobs as wtowers_plain."""
     return _rename(wtowers_plain(seed, n_st, n_dump, n_chan, theta, lam, ksize, n_src,
-                                 dump_s, r_max), "wtowers_full")
+                                 dump_s, r_max, ha_offset_hours), "wtowers_full")
 
 
 def _rename(obs, name):
