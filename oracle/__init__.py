@@ -239,7 +239,7 @@ class RefInputs:
         self.arrays = []
         self.bl = (BlData * nbl)()
         c = 299792458.0
-        vis = np.ascontiguousarray(obs.vis, np.complex128)
+        vis = np.array(obs.vis, dtype=np.complex128, order="C", copy=True)  # weight() writes it
         self.vis = vis
         for b in range(nbl):
             uvw = np.ascontiguousarray(obs.uvw[b], np.float64)

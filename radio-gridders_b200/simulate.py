@@ -199,7 +199,7 @@ class Observation:
         v = (self.uvw[:, :, 1:2] * f / C_LIGHT).ravel()
         w = (self.uvw[:, :, 2:3] * f / C_LIGHT).ravel()
         return (np.ascontiguousarray(u), np.ascontiguousarray(v),
-                np.ascontiguousarray(w), np.ascontiguousarray(self.vis.ravel()))
+                np.ascontiguousarray(w), np.array(self.vis.ravel(), copy=True))
 
 
 def enu_to_xyz(enu: np.ndarray, lat_rad: float) -> np.ndarray:

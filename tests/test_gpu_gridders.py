@@ -1,0 +1,159 @@
+"""CUDA gridders against the oracle and the reference's golden outputs.
+
+Bar (north star): relative RMS of the uv grid <= 1e-5 against the FP64 CPU
+gridder; the FP32 sub-grids and atomics leave ~1e-7."""
+import numpy as np
+import pytest
+
+from conftest import rel_rms
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+def V(rg, u, v, w, vis):
+    return rg.Visibilities(u, v, w, vis)
+
+
+def test_wprojection_golden(rg, ctx, golden, golden_kernels):
+    wk, _ = golden_kernels
+    n = int(golden["grid_size"])
+    g = np.zeros((n, n), np.complex128)
+    ctx.grid_wprojection(g, n, float(golden["theta"]),
+                         V(rg, golden["u"], golden["v"], golden["w"], golden["vis"]), wk)
+    assert rel_rms(g, golden["grid_wprojection"]) < TOL
+
+
+def test_wtowers_golden(rg, ctx, golden, golden_kernels):
+    _, wkt = golden_kernels
+    n = int(golden["grid_size"])
+    g = np.zeros((n, n), np.complex128)
+    ctx.grid_wtowers(g, n, float(golden["theta"]),
+                     V(rg, golden["u"], golden["v"], golden["w"], golden["vis"]), wkt,
+                     int(golden["subgrid"]), int(golden["margin"]), float(golden["winc"]))
+    assert rel_rms(g, golden["grid_wtowers"]) < TOL
+    st = ctx.last_stats()
+    assert st["gridded"] == len(golden["u"]) and st["dropped"] == 0
+
+
+@pytest.fixture(scope="module")
+def wproj_data(sim):
+    obs = sim.wproj_plain()
+    u, v, w, vis = obs.flat()
+    return obs, u, v, w, vis
+
+
+@pytest.mark.parametrize("ksize,ov", [(16, 8), (8, 4), (32, 2)])
+def test_wprojection_vs_oracle(rg, ctx, sim, oracle, wproj_data, ksize, ov):
+    obs, u, v, w, vis = wproj_data
+    n, th = obs.meta["grid_size"], obs.meta["theta"]
+    if ksize == 32:  # keep the 32-tap footprint inside the grid
+        keep = (np.abs(u) * th < n / 2 - 18) & (np.abs(v) * th < n / 2 - 18)
+        u, v, w, vis = u[keep], v[keep], w[keep], vis[keep]
+    wk = sim.wkernel_for(w, th, 10.0, size=ksize, oversampling=ov)
+    g = np.zeros((n, n), np.complex128)
+    ctx.grid_wprojection(g, n, th, V(rg, u, v, w, vis), wk)
+    ref = oracle.grid_wprojection(n, th, u, v, w, vis, wk)
+    assert rel_rms(g, ref) < TOL
+
+
+@pytest.mark.parametrize("sub,margin,winc", [(128, 16, 10.0), (64, 16, 10.0), (256, 32, 20.0),
+                                             (512, 16, 10.0), (128, 24, 3.0)])
+def test_wtowers_vs_oracle(rg, ctx, sim, oracle, wproj_data, sub, margin, winc):
+    obs, u, v, w, vis = wproj_data
+    n, th = obs.meta["grid_size"], obs.meta["theta"]
+    wkt = sim.generate_wkernel(th, np.arange(-winc / 2 - 1, winc / 2 + 1.5, 1.0))
+    g = np.zeros((n, n), np.complex128)
+    ctx.grid_wtowers(g, n, th, V(rg, u, v, w, vis), wkt, sub, margin, winc)
+    ref, counts = oracle.grid_wtowers(n, th, u, v, w, vis, wkt, sub, margin, winc, return_counts=True)
+    assert rel_rms(g, ref) < TOL
+    st = ctx.last_stats()
+    assert st["gridded"] == int((counts > 0).sum()) and st["dropped"] == int((counts == 0).sum())
+
+
+def test_device_and_host_buffers_agree(rg, ctx, sim, wproj_data):
+    torch = pytest.importorskip("torch")
+    obs, u, v, w, vis = wproj_data
+    n, th = obs.meta["grid_size"], obs.meta["theta"]
+    wkt = sim.generate_wkernel(th, np.arange(-6, 7, 1.0))
+    g_host = np.zeros((n, n), np.complex128)
+    ctx.grid_wtowers(g_host, n, th, V(rg, u, v, w, vis), wkt, 128, 16, 10.0)
+    dev = torch.device("cuda", 0)
+    t = [torch.from_numpy(a).to(dev) for a in (u, v, w, vis)]
+    g_dev = torch.zeros((n, n), dtype=torch.complex128, device=dev)
+    ctx.grid_wtowers(g_dev, n, th, V(rg, *t), wkt, 128, 16, 10.0,
+                     wkern_data=torch.from_numpy(wkt.data).to(dev))
+    torch.cuda.synchronize()
+    assert rel_rms(g_dev.cpu().numpy(), g_host) < 1e-6
+
+
+def test_accumulate_and_overwrite(rg, ctx, sim, wproj_data):
+    obs, u, v, w, vis = wproj_data
+    n, th = obs.meta["grid_size"], obs.meta["theta"]
+    wk = sim.wkernel_for(w, th, 10.0)
+    once = np.zeros((n, n), np.complex128)
+    ctx.grid_wprojection(once, n, th, V(rg, u, v, w, vis), wk)
+    twice = once.copy()
+    ctx.grid_wprojection(twice, n, th, V(rg, u, v, w, vis), wk)  # accumulates
+    assert rel_rms(twice, 2 * once) < 1e-6
+    junk = np.full((n, n), 7.0 + 1j)
+    ctx.grid_wprojection(junk, n, th, V(rg, u, v, w, vis), wk, flags=rg.RG_GRID_OVERWRITE)
+    assert rel_rms(junk, once) < 1e-6
+
+
+def test_empty_input(rg, ctx, sim):
+    wkt = sim.generate_wkernel(0.1, np.arange(-6, 7, 1.0))
+    e = np.zeros(0)
+    g = np.full((256, 256), 1.0 + 0j)
+    ctx.grid_wtowers(g, 256, 0.1, V(rg, e, e, e, e.astype(np.complex128)), wkt, 128, 16, 10.0)
+    assert np.all(g == 1.0)
+    ctx.grid_wprojection(g, 256, 0.1, V(rg, e, e, e, e.astype(np.complex128)), wkt,
+                         flags=rg.RG_GRID_OVERWRITE)
+    assert np.all(g == 0.0)
+
+
+def test_single_visibility_ragged(rg, ctx, sim, oracle):
+    """One visibility, and counts that are not multiples of any batch size."""
+    th, n = 0.1, 256
+    wkt = sim.generate_wkernel(th, np.arange(-6, 7, 1.0))
+    rng = np.random.default_rng(4)
+    for count in (1, 2, 255, 257, 1025):
+        u = rng.uniform(-1000, 1000, count)
+        v = rng.uniform(-1000, 1000, count)
+        w = rng.uniform(-40, 40, count)
+        vis = rng.normal(size=count) + 1j * rng.normal(size=count)
+        g = np.zeros((n, n), np.complex128)
+        ctx.grid_wtowers(g, n, th, V(rg, u, v, w, vis), wkt, 128, 16, 10.0)
+        ref = oracle.grid_wtowers(n, th, u, v, w, vis, wkt, 128, 16, 10.0)
+        assert rel_rms(g, ref) < TOL
+
+
+def test_wtowers_linearity_full_size(rg, ctx, sim):
+    """Size-independent property at the benchmark size: G(a V1 + V2) = a G(V1) + G(V2)."""
+    obs = sim.wtowers_plain()
+    u, v, w, vis = obs.flat()
+    wkt = sim.generate_wkernel(0.1, np.arange(-5, 6, 1.0))
+    rng = np.random.default_rng(0)
+    v2 = rng.normal(size=len(u)) + 1j * rng.normal(size=len(u))
+    a = 0.37 - 1.1j
+
+    def grid(x):
+        g = np.zeros((2048, 2048), np.complex128)
+        ctx.grid_wtowers(g, 2048, 0.1, V(rg, u, v, w, x), wkt, 512, 16, 10.0)
+        return g
+
+    g1, g2, g12 = grid(vis), grid(v2), grid(a * vis + v2)
+    assert rel_rms(g12, a * g1 + g2) < 1e-5
+    assert ctx.last_stats()["gridded"] == len(u)
+
+
+def test_weight_hermitian_shift_image_exact(rg, ctx, oracle, wproj_data, golden):
+    obs, u, v, w, vis = wproj_data
+    n, th = obs.meta["grid_size"], obs.meta["theta"]
+    out = ctx.weight(n, th, V(rg, u, v, w, vis))
+    assert np.array_equal(out, oracle.weight(n, th, u, v, vis))
+    g = golden["grid_wprojection"]
+    assert np.array_equal(ctx.make_hermitian(g.copy()), golden["hermitian"])
+    assert np.array_equal(ctx.fft_shift(g.copy()), golden["shifted"])
+    img = ctx.image_from_grid(g.copy())
+    assert rel_rms(img, oracle.image_from_grid(g)) < 1e-13
