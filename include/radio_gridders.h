@@ -112,6 +112,25 @@ int rg_last_timings(rg_context *ctx, const char **names, float *ms, int n);
 rg_status rg_grid_wprojection(rg_context *ctx, double *uvgrid, int grid_size, double theta,
                               const rg_vis *vis, const rg_wkern *wkern, int flags);
 
+/* W-projection that allocates nothing.  No counterpart in the reference.
+ * For callers that cannot allocate device memory or let a library do it:
+ * code running while another framework owns the device memory pool and its
+ * budget, real-time pipelines that forbid allocation after start-up, embedders
+ * with a fixed memory plan.  No context, stream, event or allocation is
+ * created; the caller passes device pointers for every input and the output
+ * (host pointers are rejected) and the stream to run on (NULL = default).
+ * Intermediates live in one file-scope device array (about 13.5 MiB, held by
+ * every GPU that loads the library until exit), which limits grid_size to
+ * 1024 and the w-kernel table to 524288 taps; larger requests fail with
+ * RG_ERR_UNSUPPORTED.  Any number of visibilities.  The first call on each
+ * device resolves the array's address (cudaGetSymbolAddress); make that first
+ * call before any stream capture.  Calls share the array: calls that overlap
+ * on the GPU (other streams, other host threads) race.  Runs on the calling
+ * thread's current device and returns after the grid is written. */
+rg_status rg_grid_wprojection_noalloc(double *uvgrid, int grid_size, double theta,
+                                      const rg_vis *vis, const rg_wkern *wkern, int flags,
+                                      void *cuda_stream);
+
 /* W-towers.  Replaces grid_wtowers (src/reference/grid.h:123-126,
  * grid.c:295-555) and the GPU wrapper wtowers_CUDA_flat
  * (src/grid/grid_common.cuh:52-55, grid_cuda.cu:522-744) up to the final FFT:

@@ -39,6 +39,7 @@ EXPORTS = [
     "rg_context_create", "rg_context_destroy", "rg_context_set_stream", "rg_last_error",
     "rg_last_stats", "rg_context_set_profiling", "rg_last_timings", "rg_grid_wprojection", "rg_grid_wtowers", "rg_weight",
     "rg_make_hermitian", "rg_fft_shift", "rg_image_from_grid", "rg_fft2d", "rg_dft_image",
+    "rg_grid_wprojection_noalloc",
 ]
 
 
@@ -91,6 +92,7 @@ def lib():
         L.rg_image_from_grid.argtypes = [vp, vp, i, vp, vp]
         L.rg_fft2d.argtypes = [vp, vp, i, i, i, i, i]
         L.rg_dft_image.argtypes = [vp, vp, i, d, ct.POINTER(_Vis), i, d]
+        L.rg_grid_wprojection_noalloc.argtypes = [vp, i, d, ct.POINTER(_Vis), ct.POINTER(_WKern), i, vp]
         for name in EXPORTS:
             getattr(L, name)  # raises AttributeError if a declared symbol is missing
         _lib = L
