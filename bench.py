@@ -63,6 +63,15 @@ def workload(rank: int):
     return obs, wk
 
 
+def reduce_master(grid, world):
+    """Sum the ranks' FP64 master grids onto rank 0 (one collective).  The grid
+    is a complex128 torch tensor; it travels as its real view."""
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        dist.reduce(torch.view_as_real(grid), dst=0)
+
+
 def peaks():
     path = os.path.join(REPO, "MEASURED_PEAKS.json")
     try:
@@ -245,8 +254,7 @@ def run_b200(args, rank, world, local_rank):
     def step():
         ctx.grid_wtowers(grid, GRID, THETA, V, wk, SUBGRID, MARGIN, WINC,
                          flags=rg.RG_GRID_OVERWRITE, wkern_data=dwk)
-        if world > 1:
-            dist.reduce(grid, dst=0)
+        reduce_master(grid, world)
 
     for _ in range(max(args.warmup, 3)):
         step()

@@ -95,22 +95,22 @@ __global__ void __launch_bounds__(256) fft32_rows_kernel(float2 *__restrict__ da
 // ---------------------------------------------------------------------------
 // columns: a strip of C columns of one N x N array per CTA, 256 threads
 // ---------------------------------------------------------------------------
-template <int N1>
+template <int N1, int CW = (N1 >= 32 ? 8 : 16)>
 struct ColGeom {
     static constexpr int N = N1 * 32;
-    static constexpr int C = N1 >= 32 ? 8 : 16;           // strip width
-    static constexpr int CS = N1 * kPad + 1;               // per-column stride in T
+    static constexpr int C = CW;                            // strip width
+    static constexpr int CS = N1 * kPad + 1;                // per-column stride in T
     static constexpr int T_ELEMS = C * CS;
     static constexpr int LB = ilog2c(N1);
 };
 
 // Step 1 of a column transform: load from `src` (row stride `ld`, column c of
 // the strip at src[row*ld + c]), 32-point transforms, twiddle, into T.
-template <int N1, int SIGN>
+template <int N1, int SIGN, int CW = ColGeom<N1>::C>
 __device__ __forceinline__ void col_step1(const float2 *__restrict__ src, int ld, float2 *T,
                                           const float2 *W)
 {
-    using G = ColGeom<N1>;
+    using G = ColGeom<N1, CW>;
     for (int it = threadIdx.x; it < G::C * N1; it += blockDim.x) {
         const int c = it % G::C, n1 = it / G::C;
         float2 a[32];
@@ -153,35 +153,46 @@ __global__ void __launch_bounds__(256) fft32_cols_kernel(float2 *__restrict__ da
 }
 
 // ---------------------------------------------------------------------------
-// W-towers column stage.  CTA = (tower, strip).  For each active floor slot of
-// the tower: backward column transform of the row-transformed sub-grid, times
-// exp(-2 pi i wp ph(l, m)) with ph = winc (1 - sqrt(1 - l^2 - m^2)) (the
-// reference's wtransfer^(-wp), grid.c:304-319,473-496), accumulated in
-// registers.  Then the forward column transform of the sum, into subimg.
-// Phase products are formed and reduced modulo 1 in FP64; sin/cos of the
-// reduced phase in FP32.
+// W-towers column stage, in two kernels so uneven towers balance.
+//
+// tower_partial_kernel: CTA = (floor group, strip of C columns).  A group is up
+// to G consecutive active floors of one tower.  For each floor: backward column
+// transform of the row-transformed sub-grid, times exp(-2 pi i wp ph(l, m)) with
+// ph = winc (1 - sqrt(1 - l^2 - m^2)) — the reference's wtransfer^(-wp),
+// grid.c:304-319 and :473-496, which also covers the w = 0 transfer —
+// accumulated in registers; the strip sum is written to the group's partial
+// buffer.  Phase products are formed and reduced modulo 1 in FP64; sin/cos of
+// the reduced phase in FP32.
+//
+// tower_finish_kernel: CTA = (tower, strip).  Sums the tower's group partials in
+// group order (deterministic) and applies the forward column transform into the
+// tower's sub-image (grid.c:499, with the row half done by the row kernel).
 // ---------------------------------------------------------------------------
+constexpr int kPartialThreads = 128;
 template <int N1>
-__global__ void __launch_bounds__(256) tower_cols_kernel(
+using PartialGeom = ColGeom<N1, 8>;
+
+template <int N1>
+__global__ void __launch_bounds__(kPartialThreads) tower_partial_kernel(
     const float2 *__restrict__ slots, const int *__restrict__ bin_of_slot,
-    const int *__restrict__ tower_first, const int *__restrict__ tower_count, int nfloor,
-    int wp_min, const double *__restrict__ ph, float2 *__restrict__ subimg,
+    const int *__restrict__ group_begin, const int *__restrict__ group_end, int nfloor,
+    int wp_min, const double *__restrict__ ph, float2 *__restrict__ partial,
     const float2 *__restrict__ tw)
 {
-    using G = ColGeom<N1>;
+    using G = PartialGeom<N1>;
     constexpr int N = G::N, C = G::C;
-    constexpr int ITEMS = C * 32;                   // step-2 work items per strip
-    constexpr int PER = (ITEMS + 255) / 256;         // per thread (blockDim 256)
+    constexpr int ITEMS = C * 32;
+    constexpr int PER = (ITEMS + kPartialThreads - 1) / kPartialThreads;
     extern __shared__ float2 smem[];
     float2 *T = smem;
     float2 *W = smem + G::T_ELEMS;
-    float2 *U = W + N;  // [N][C] accumulated strip
+    double *P = reinterpret_cast<double *>(W + N);  // [N][C] Fresnel phase of the strip
     const int strips = N / C;
-    const int tower = blockIdx.x / strips, strip = blockIdx.x % strips;
-    const int count = tower_count[tower];
-    if (count == 0) return;
-    const int first = tower_first[tower];
+    const int group = blockIdx.x / strips, strip = blockIdx.x % strips;
+    const int begin = group_begin[group], end = group_end[group];
     for (int i = threadIdx.x; i < N; i += blockDim.x) W[i] = tw[i];
+    for (int e = threadIdx.x; e < N * C; e += blockDim.x)
+        P[e] = ph[(int64_t)(e / C) * N + strip * C + e % C];
 
     float2 acc[PER][N1];
 #pragma unroll
@@ -190,52 +201,75 @@ __global__ void __launch_bounds__(256) tower_cols_kernel(
         for (int j = 0; j < N1; j++) acc[q][j] = make_float2(0.f, 0.f);
     __syncthreads();
 
-    for (int f = 0; f < count; f++) {
-        const int slot = first + f;
-        const int wp = wp_min + bin_of_slot[slot] % nfloor;
-        const double mwp = -(double)wp;
+    for (int slot = begin; slot < end; slot++) {
+        const double mwp = -(double)(wp_min + bin_of_slot[slot] % nfloor);
         const float2 *base = slots + (int64_t)slot * N * N + strip * C;
-        col_step1<N1, +1>(base, N, T, W);
+        col_step1<N1, +1, C>(base, N, T, W);
         __syncthreads();
 #pragma unroll
         for (int q = 0; q < PER; q++) {
-            const int it = threadIdx.x + q * 256;
+            const int it = threadIdx.x + q * kPartialThreads;
             if (it < ITEMS) {
                 const int c = it % C, k2 = it / C;
                 float2 b[N1];
 #pragma unroll
                 for (int n1 = 0; n1 < N1; n1++) b[n1] = T[c * G::CS + n1 * kPad + k2];
                 reg_fft<N1, +1>(b);
-                const int col = strip * C + c;
 #pragma unroll
                 for (int j = 0; j < N1; j++) {
                     const int row = k2 + 32 * bitrevc(j, G::LB);
-                    double phase = mwp * __ldg(ph + (int64_t)row * N + col);
-                    phase -= rint(phase);
+                    double phase = mwp * P[row * C + c];
+                    phase -= rint(phase);  // |phase| <= 1/2 after the FP64 reduction
                     float sn, cs;
-                    sincospif(2.0f * (float)phase, &sn, &cs);
-                    const float2 v = cmulf(b[j], make_float2(cs, sn));
-                    acc[q][j] = caddf(acc[q][j], v);
+                    __sincosf(6.28318530717958647f * (float)phase, &sn, &cs);
+                    acc[q][j] = caddf(acc[q][j], cmulf(b[j], make_float2(cs, sn)));
                 }
             }
         }
         __syncthreads();
     }
-    // stage the accumulated strip, then forward column transform into subimg
+    float2 *out = partial + (int64_t)group * N * N + strip * C;
 #pragma unroll
     for (int q = 0; q < PER; q++) {
-        const int it = threadIdx.x + q * 256;
+        const int it = threadIdx.x + q * kPartialThreads;
         if (it < ITEMS) {
             const int c = it % C, k2 = it / C;
 #pragma unroll
-            for (int j = 0; j < N1; j++) U[(k2 + 32 * bitrevc(j, G::LB)) * C + c] = acc[q][j];
+            for (int j = 0; j < N1; j++) out[(int64_t)(k2 + 32 * bitrevc(j, G::LB)) * N + c] = acc[q][j];
         }
+    }
+}
+
+template <int N1>
+__global__ void __launch_bounds__(256) tower_finish_kernel(
+    const float2 *__restrict__ partial, const int *__restrict__ tower_group_first,
+    const int *__restrict__ tower_group_count, float2 *__restrict__ subimg,
+    const float2 *__restrict__ tw)
+{
+    using G = ColGeom<N1>;
+    constexpr int N = G::N, C = G::C;
+    extern __shared__ float2 smem[];
+    float2 *T = smem;
+    float2 *W = smem + G::T_ELEMS;
+    float2 *U = W + N;  // [N][C]
+    const int strips = N / C;
+    const int tower = blockIdx.x / strips, strip = blockIdx.x % strips;
+    const int gcount = tower_group_count[tower];
+    if (gcount == 0) return;
+    const int gfirst = tower_group_first[tower];
+    for (int i = threadIdx.x; i < N; i += blockDim.x) W[i] = tw[i];
+    for (int e = threadIdx.x; e < N * C; e += blockDim.x) {
+        const int row = e / C, c = e % C;
+        float2 sum = make_float2(0.f, 0.f);
+        for (int g = 0; g < gcount; g++)
+            sum = caddf(sum, partial[(int64_t)(gfirst + g) * N * N + (int64_t)row * N + strip * C + c]);
+        U[e] = sum;
     }
     __syncthreads();
     col_step1<N1, -1>(U, C, T, W);
     __syncthreads();
     float2 *out = subimg + (int64_t)tower * N * N + strip * C;
-    for (int it = threadIdx.x; it < ITEMS; it += blockDim.x) {
+    for (int it = threadIdx.x; it < C * 32; it += blockDim.x) {
         const int c = it % C, k2 = it / C;
         float2 b[N1];
 #pragma unroll
@@ -254,7 +288,13 @@ static size_t rows_smem() { return sizeof(float2) * (16 * N1 * kPad + N1 * 32); 
 template <int N1>
 static size_t cols_smem() { return sizeof(float2) * (ColGeom<N1>::T_ELEMS + N1 * 32); }
 template <int N1>
-static size_t tower_smem()
+static size_t partial_smem()
+{
+    return sizeof(float2) * (PartialGeom<N1>::T_ELEMS + N1 * 32) +
+           sizeof(double) * N1 * 32 * PartialGeom<N1>::C;
+}
+template <int N1>
+static size_t finish_smem()
 {
     return sizeof(float2) * (ColGeom<N1>::T_ELEMS + N1 * 32 + N1 * 32 * ColGeom<N1>::C);
 }
@@ -288,15 +328,23 @@ static void cols_impl(cudaStream_t s, float2 *data, int batch, int sign, const f
 }
 
 template <int N1>
-static void tower_impl(cudaStream_t s, float2 *slots, const int *bin_of_slot, const int *tower_first,
-                       const int *tower_count, int ntowers, int nfloor, int wp_min,
-                       const double *ph, float2 *subimg, const float2 *tw)
+static void tower_impl(cudaStream_t s, const float2 *slots, const int *bin_of_slot,
+                       const int *group_begin, const int *group_end, int ngroups,
+                       const int *tower_group_first, const int *tower_group_count, int ntowers,
+                       int nfloor, int wp_min, const double *ph, float2 *partial, float2 *subimg,
+                       const float2 *tw)
 {
-    const size_t sm = tower_smem<N1>();
-    cudaFuncSetAttribute(tower_cols_kernel<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    const unsigned blocks = (unsigned)ntowers * (N1 * 32 / ColGeom<N1>::C);
-    tower_cols_kernel<N1><<<blocks, 256, sm, s>>>(slots, bin_of_slot, tower_first, tower_count,
-                                                  nfloor, wp_min, ph, subimg, tw);
+    const int pstrips = N1 * 32 / PartialGeom<N1>::C;
+    const int strips = N1 * 32 / ColGeom<N1>::C;
+    const size_t sm1 = partial_smem<N1>();
+    cudaFuncSetAttribute(tower_partial_kernel<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
+    if (ngroups > 0)
+        tower_partial_kernel<N1><<<(unsigned)ngroups * pstrips, kPartialThreads, sm1, s>>>(
+            slots, bin_of_slot, group_begin, group_end, nfloor, wp_min, ph, partial, tw);
+    const size_t sm2 = finish_smem<N1>();
+    cudaFuncSetAttribute(tower_finish_kernel<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
+    tower_finish_kernel<N1><<<(unsigned)ntowers * strips, 256, sm2, s>>>(
+        partial, tower_group_first, tower_group_count, subimg, tw);
 }
 
 #define RG_DISPATCH_N1(n, CALL) \
@@ -323,17 +371,20 @@ void launch_fft32_cols(cudaStream_t s, float2 *data, int batch, int n, int sign,
 #undef CALL
 }
 
-void launch_tower_columns(cudaStream_t s, float2 *slots, const int *bin_of_slot,
-                          const int *tower_first, const int *tower_count, int ntowers, int nfloor,
-                          int wp_min, double winc, const double *ph, float2 *subimg, int subgrid,
-                          const float2 *tw)
+void launch_tower_columns(cudaStream_t s, const float2 *slots, const int *bin_of_slot,
+                          const int *group_begin, const int *group_end, int ngroups,
+                          const int *tower_group_first, const int *tower_group_count, int ntowers,
+                          int nfloor, int wp_min, const double *ph, float2 *partial, float2 *subimg,
+                          int subgrid, const float2 *tw)
 {
-    (void)winc;
-#define CALL(N1) tower_impl<N1>(s, slots, bin_of_slot, tower_first, tower_count, ntowers, nfloor, \
-                                wp_min, ph, subimg, tw)
+#define CALL(N1) tower_impl<N1>(s, slots, bin_of_slot, group_begin, group_end, ngroups,           \
+                                tower_group_first, tower_group_count, ntowers, nfloor, wp_min, ph, \
+                                partial, subimg, tw)
     RG_DISPATCH_N1(subgrid, CALL)
 #undef CALL
 }
+
+int fft32_strips(int n) { return n / 8; }  // strips of the partial (column) stage
 
 // ---------------------------------------------------------------------------
 // FP64 transforms (image formation)

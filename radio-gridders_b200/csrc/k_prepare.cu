@@ -7,8 +7,10 @@
 //   w-plane selection   src/reference/grid.c:168-170
 //   tower/floor cuts    src/reference/grid.c:357-367, 425-458, 244-254
 // Record layout (int4): x = bin (tower*nfloor + floor, -1 = not gridded),
-// y = (row0 << 16) | (col0 & 0xffff)  (footprint origin, int16 each, may be -1),
-// z = tap base index into the FP32 kernel table, w = unused.
+// y = row0 * side + col0, the linear index of the footprint origin (the
+// reference's grid_offset; may be slightly negative at a tower's low edge),
+// z = tap base index into the FP32 kernel table,
+// w = ((row0 mod 64) << 8) | (col0 mod 64), the residues the Romein threads need.
 #include <cfloat>
 
 #include "rg_internal.h"
@@ -173,8 +175,9 @@ __global__ void prepare_towers_kernel(const double *__restrict__ u, const double
         const int tower = found_cy * g.nchunk + found_cx;
         const int bin = tower * nfloor + (found_wp - wp_min);
         r.x = bin;
-        r.y = (row0 << 16) | (col0 & 0xffff);
+        r.y = row0 * g.subgrid + col0;
         r.z = (int)tap;
+        r.w = ((row0 & 63) << 8) | (col0 & 63);
         rec[i] = r;
         active[bin] = 1;
         gridded++;
@@ -243,8 +246,9 @@ __global__ void prepare_wproj_kernel(const double *__restrict__ u, const double 
             continue;
         }
         r.x = 0;
-        r.y = (row0 << 16) | (col0 & 0xffff);
+        r.y = row0 * grid_size + col0;
         r.z = (int)tap;
+        r.w = ((row0 & 63) << 8) | (col0 & 63);
         rec[i] = r;
     }
     if (local_err) atomicOr(err, local_err);
@@ -262,63 +266,105 @@ void launch_prepare_wproj(cudaStream_t s, const double *u, const double *v, cons
                                                 planes, wk_wmin, wk_wstep, rec, visf, err);
 }
 
+// Block-wide exclusive scan (blockDim a multiple of 32, <= 1024).  Returns the
+// exclusive prefix of x; *total receives the block sum.  warp_sums: 32 ints of
+// shared memory.  Must be called by every thread of the block.
+__device__ int block_exclusive_scan(int x, int *warp_sums, int *total)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int incl = x;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_sums[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        int y = lane < nw ? warp_sums[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, y, o);
+            if (lane >= o) y += t;
+        }
+        if (lane < nw) warp_sums[lane] = y;
+    }
+    __syncthreads();
+    const int excl = (wid > 0 ? warp_sums[wid - 1] : 0) + incl - x;
+    *total = warp_sums[nw - 1];
+    __syncthreads();
+    return excl;
+}
+
 // Single-CTA compaction of active (tower, floor) bins into slots, in bin order,
-// so each tower's slots are contiguous and ordered by floor.
+// so each tower's slots are contiguous and ordered by floor; then the floor
+// groups of the column stage (up to G consecutive slots of one tower, G chosen
+// so the stage has about target_items (group, strip) work items).
 __global__ void compact_bins_kernel(const int *__restrict__ active, int nbins, int nfloor,
                                     int *__restrict__ slot_of_bin, int *__restrict__ bin_of_slot,
-                                    int *__restrict__ n_active, int *__restrict__ tower_first,
-                                    int *__restrict__ tower_count, int ntowers)
+                                    int *__restrict__ counts, int *__restrict__ tower_first,
+                                    int *__restrict__ tower_count, int ntowers, int strips,
+                                    int target_items, int *__restrict__ group_begin,
+                                    int *__restrict__ group_end, int *__restrict__ tower_group_first,
+                                    int *__restrict__ tower_group_count)
 {
     __shared__ int warp_sums[32];
-    __shared__ int carry;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int carry = 0;
     for (int base = 0; base < nbins; base += blockDim.x) {
         const int b = base + threadIdx.x;
         const int a = (b < nbins && active[b]) ? 1 : 0;
-        int incl = a;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
-        }
-        if (lane == 31) warp_sums[wid] = incl;
-        __syncthreads();
-        if (wid == 0) {
-            int x = lane < nw ? warp_sums[lane] : 0;
-            for (int o = 1; o < 32; o <<= 1) {
-                const int t = __shfl_up_sync(0xffffffffu, x, o);
-                if (lane >= o) x += t;
-            }
-            if (lane < nw) warp_sums[lane] = x;
-        }
-        __syncthreads();
-        const int excl = carry + (wid > 0 ? warp_sums[wid - 1] : 0) + incl - a;
+        int total;
+        const int excl = carry + block_exclusive_scan(a, warp_sums, &total);
         if (b < nbins) slot_of_bin[b] = excl;  // exclusive prefix for now
         if (a) bin_of_slot[excl] = b;
-        __syncthreads();
-        if (threadIdx.x == 0) carry += warp_sums[nw - 1];
-        __syncthreads();
+        carry += total;
     }
-    const int total = carry;
+    const int n_active = carry;
+    __syncthreads();
     for (int t = threadIdx.x; t < ntowers; t += blockDim.x) {
         const int first = slot_of_bin[t * nfloor];
-        const int next = (t + 1 < ntowers) ? slot_of_bin[(t + 1) * nfloor] : total;
+        const int next = (t + 1 < ntowers) ? slot_of_bin[(t + 1) * nfloor] : n_active;
         tower_first[t] = first;
         tower_count[t] = next - first;
     }
     __syncthreads();
     for (int b = threadIdx.x; b < nbins; b += blockDim.x)
         if (!active[b]) slot_of_bin[b] = -1;
-    if (threadIdx.x == 0) *n_active = total;
+    long long want = ((long long)n_active * strips + target_items - 1) / (target_items > 0 ? target_items : 1);
+    int G = (int)(want < 4 ? 4 : (want > 64 ? 64 : want));
+    carry = 0;
+    for (int base = 0; base < ntowers; base += blockDim.x) {
+        const int t = base + threadIdx.x;
+        const int cnt = t < ntowers ? tower_count[t] : 0;
+        const int ng = (cnt + G - 1) / G;
+        int total;
+        const int gfirst = carry + block_exclusive_scan(ng, warp_sums, &total);
+        if (t < ntowers) {
+            tower_group_first[t] = gfirst;
+            tower_group_count[t] = ng;
+            const int sfirst = tower_first[t];
+            for (int j = 0; j < ng; j++) {
+                const int b0 = sfirst + j * G;
+                const int b1 = b0 + G < sfirst + cnt ? b0 + G : sfirst + cnt;
+                group_begin[gfirst + j] = b0;
+                group_end[gfirst + j] = b1;
+            }
+        }
+        carry += total;
+    }
+    if (threadIdx.x == 0) {
+        counts[0] = n_active;
+        counts[1] = carry;
+    }
 }
 
 void launch_compact_bins(cudaStream_t s, const int *active, int nbins, int nfloor, int *slot_of_bin,
-                         int *bin_of_slot, int *n_active, int *tower_first, int *tower_count,
-                         int ntowers)
+                         int *bin_of_slot, int *counts, int *tower_first, int *tower_count,
+                         int ntowers, int strips, int target_items, int *group_begin,
+                         int *group_end, int *tower_group_first, int *tower_group_count)
 {
-    compact_bins_kernel<<<1, 1024, 0, s>>>(active, nbins, nfloor, slot_of_bin, bin_of_slot,
-                                           n_active, tower_first, tower_count, ntowers);
+    compact_bins_kernel<<<1, 1024, 0, s>>>(active, nbins, nfloor, slot_of_bin, bin_of_slot, counts,
+                                           tower_first, tower_count, ntowers, strips, target_items,
+                                           group_begin, group_end, tower_group_first,
+                                           tower_group_count);
 }
 
 }  // namespace rg

@@ -11,10 +11,12 @@
 // registers.  Per tap: sum += vis * conj(tap), the reference's
 // grid += v * conj(wk) (src/reference/grid.c:177-182).
 //
-// The linear index (row0 + cv) * side + (col0 + cu) is the reference's
+// The linear index grid_offset + cv * side + cu is the reference's
 // grid_offset + y*size + x; points outside [0, side^2) are dropped (the
 // reference does not check, grid.c:177-182; its GPU gridder drops them,
-// src/grid/grid_cuda.cu:25-41).
+// src/grid/grid_cuda.cu:25-41).  The record carries grid_offset and the
+// footprint origin's residues modulo 64, so a thread's tap (cu, cv) is two
+// subtractions and masks.
 //
 // Visibilities are staged through shared memory in batches (coalesced 16-byte
 // record and 8-byte visibility loads); taps are read through the read-only
@@ -33,12 +35,11 @@ __global__ void __launch_bounds__(K *K) romein_kernel(
     __shared__ int4 srec[BATCH];
     __shared__ float2 svis[BATCH];
     const int myU = threadIdx.x % K, myV = threadIdx.x / K;
-    const int64_t limit = (int64_t)side * side;
+    const int limit = side * side;
 
     for (int64_t c0 = (int64_t)blockIdx.x * chunk; c0 < n; c0 += (int64_t)gridDim.x * chunk) {
         const int64_t c1 = c0 + chunk < n ? c0 + chunk : n;
-        int cur_bin = -1;
-        int64_t cur_idx = 0;
+        int cur_bin = -1, cur_idx = 0;
         float2 sum = make_float2(0.f, 0.f);
         for (int64_t b0 = c0; b0 < c1; b0 += BATCH) {
             const int cnt = (int)(c1 - b0 < BATCH ? c1 - b0 : BATCH);
@@ -48,28 +49,36 @@ __global__ void __launch_bounds__(K *K) romein_kernel(
                 svis[threadIdx.x] = visf[b0 + threadIdx.x];
             }
             __syncthreads();
+            // software pipeline: the tap of visibility j+1 is loaded before j is used
+            int4 r = srec[0];
+            int cu = (myU - (r.w & 0xff)) & (K - 1);
+            int cv = (myV - (r.w >> 8)) & (K - 1);
+            float2 t = r.x >= 0 ? __ldg(taps + r.z + cv * K + cu) : make_float2(0.f, 0.f);
             for (int j = 0; j < cnt; j++) {
-                const int4 r = srec[j];
-                if (r.x < 0) continue;
-                const int col0 = (int)(short)(r.y & 0xffff);
-                const int row0 = r.y >> 16;
-                const int cu = (myU - col0) & (K - 1);
-                const int cv = (myV - row0) & (K - 1);
-                const int64_t idx = (int64_t)(row0 + cv) * side + (col0 + cu);
-                if (r.x != cur_bin || idx != cur_idx) {
-                    if (cur_bin >= 0 && cur_idx >= 0 && cur_idx < limit)
-                        atomicAdd(grids + (int64_t)slot_of_bin[cur_bin] * grid_stride + cur_idx, sum);
-                    cur_bin = r.x;
-                    cur_idx = idx;
-                    sum = make_float2(0.f, 0.f);
+                const int4 rn = srec[j + 1 < cnt ? j + 1 : j];
+                const int cun = (myU - (rn.w & 0xff)) & (K - 1);
+                const int cvn = (myV - (rn.w >> 8)) & (K - 1);
+                const float2 tn = rn.x >= 0 ? __ldg(taps + rn.z + cvn * K + cun) : make_float2(0.f, 0.f);
+                if (r.x >= 0) {
+                    const int idx = r.y + cv * side + cu;
+                    if (r.x != cur_bin || idx != cur_idx) {
+                        if (cur_bin >= 0 && (unsigned)cur_idx < (unsigned)limit)
+                            atomicAdd(grids + (int64_t)slot_of_bin[cur_bin] * grid_stride + cur_idx, sum);
+                        cur_bin = r.x;
+                        cur_idx = idx;
+                        sum = make_float2(0.f, 0.f);
+                    }
+                    const float2 vz = svis[j];
+                    sum.x = fmaf(vz.x, t.x, fmaf(vz.y, t.y, sum.x));
+                    sum.y = fmaf(vz.y, t.x, fmaf(-vz.x, t.y, sum.y));
                 }
-                const float2 t = __ldg(taps + r.z + cv * K + cu);
-                const float2 vz = svis[j];
-                sum.x = fmaf(vz.x, t.x, fmaf(vz.y, t.y, sum.x));
-                sum.y = fmaf(vz.y, t.x, fmaf(-vz.x, t.y, sum.y));
+                r = rn;
+                cu = cun;
+                cv = cvn;
+                t = tn;
             }
         }
-        if (cur_bin >= 0 && cur_idx >= 0 && cur_idx < limit)
+        if (cur_bin >= 0 && (unsigned)cur_idx < (unsigned)limit)
             atomicAdd(grids + (int64_t)slot_of_bin[cur_bin] * grid_stride + cur_idx, sum);
     }
 }

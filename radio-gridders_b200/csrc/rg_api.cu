@@ -476,6 +476,7 @@ rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double
     const int nfloor = (int)nfloor64, nbins = (int)nbins64;
 
     void *active, *rec, *visf, *slot_of_bin, *bin_of_slot, *nact, *tfirst, *tcount;
+    void *gbegin, *gend, *tgfirst, *tgcount;
     RG_CHECK(scratch(ctx, "active", sizeof(int) * (size_t)nbins, &active));
     RG_CHECK(scratch(ctx, "rec", sizeof(int4) * (size_t)dv.n, &rec));
     RG_CHECK(scratch(ctx, "visf", sizeof(float2) * (size_t)dv.n, &visf));
@@ -484,6 +485,10 @@ rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double
     RG_CHECK(scratch(ctx, "n_active", 16, &nact));
     RG_CHECK(scratch(ctx, "tower_first", sizeof(int) * (size_t)ntowers, &tfirst));
     RG_CHECK(scratch(ctx, "tower_count", sizeof(int) * (size_t)ntowers, &tcount));
+    RG_CHECK(scratch(ctx, "group_begin", sizeof(int) * (size_t)nbins, &gbegin));
+    RG_CHECK(scratch(ctx, "group_end", sizeof(int) * (size_t)nbins, &gend));
+    RG_CHECK(scratch(ctx, "tower_group_first", sizeof(int) * (size_t)ntowers, &tgfirst));
+    RG_CHECK(scratch(ctx, "tower_group_count", sizeof(int) * (size_t)ntowers, &tgcount));
     RG_CUDA(cudaMemsetAsync(active, 0, sizeof(int) * (size_t)nbins, st));
 
     TowerGeom g;
@@ -506,15 +511,18 @@ rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double
         ctx->launches++;
     }
     end_stage(ctx);
+    const int strips = fft32_strips(S);
     begin_stage(ctx, "compact");
     launch_compact_bins(st, (const int *)active, nbins, nfloor, (int *)slot_of_bin, (int *)bin_of_slot,
-                        (int *)nact, (int *)tfirst, (int *)tcount, ntowers);
+                        (int *)nact, (int *)tfirst, (int *)tcount, ntowers, strips,
+                        8 * ctx->sm_count, (int *)gbegin, (int *)gend, (int *)tgfirst, (int *)tgcount);
     end_stage(ctx);
     ctx->launches++;
     RG_CHECK(check_launch("tower binning"));
-    int n_active = 0;
-    RG_CUDA(cudaMemcpyAsync(&n_active, nact, sizeof(int), cudaMemcpyDeviceToHost, st));
+    int counts_h[2] = {0, 0};
+    RG_CUDA(cudaMemcpyAsync(counts_h, nact, sizeof(counts_h), cudaMemcpyDeviceToHost, st));
     RG_CUDA(cudaStreamSynchronize(st));
+    const int n_active = counts_h[0], n_groups = counts_h[1];
 
     const int64_t sub_cells = (int64_t)S * S;
     void *slots = nullptr, *subimg = nullptr, *ph = nullptr;
@@ -544,15 +552,19 @@ rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double
         begin_stage(ctx, "fft_rows_backward");
         launch_fft32_rows(st, (float2 *)slots, (int64_t)n_active * S, S, +1, tw);
         end_stage(ctx);
+        void *partial;
+        RG_CHECK(scratch(ctx, "partial", sizeof(float2) * (size_t)(sub_cells * (n_groups > 0 ? n_groups : 1)),
+                         &partial));
         begin_stage(ctx, "tower_columns");
-        launch_tower_columns(st, (float2 *)slots, (const int *)bin_of_slot, (const int *)tfirst,
-                             (const int *)tcount, ntowers, nfloor, wp_min, wincrement,
-                             (const double *)ph, (float2 *)subimg, S, tw);
+        launch_tower_columns(st, (const float2 *)slots, (const int *)bin_of_slot, (const int *)gbegin,
+                             (const int *)gend, n_groups, (const int *)tgfirst, (const int *)tgcount,
+                             ntowers, nfloor, wp_min, (const double *)ph, (float2 *)partial,
+                             (float2 *)subimg, S, tw);
         end_stage(ctx);
         begin_stage(ctx, "fft_rows_forward");
         launch_fft32_rows(st, (float2 *)subimg, (int64_t)ntowers * S, S, -1, tw);
         end_stage(ctx);
-        ctx->launches += 4;
+        ctx->launches += 5;
         RG_CHECK(check_launch("tower gridding / transforms"));
     }
     begin_stage(ctx, "add_back");

@@ -137,9 +137,12 @@ void launch_prepare_wproj(cudaStream_t s, const double *u, const double *v, cons
                           const double2 *vis, int64_t n, int grid_size, double theta,
                           int ksize, int ov, int planes, double wk_wmin, double wk_wstep,
                           int4 *rec, float2 *visf, unsigned *err);
+// counts[0] = active slots, counts[1] = floor groups (target_items: aim for
+// about this many (group, strip) work items in the column stage)
 void launch_compact_bins(cudaStream_t s, const int *active, int nbins, int nfloor, int *slot_of_bin,
-                         int *bin_of_slot, int *n_active, int *tower_first, int *tower_count,
-                         int ntowers);
+                         int *bin_of_slot, int *counts, int *tower_first, int *tower_count,
+                         int ntowers, int strips, int target_items, int *group_begin,
+                         int *group_end, int *tower_group_first, int *tower_group_count);
 
 // k_romein.cu
 void launch_romein(cudaStream_t s, const int4 *rec, const float2 *visf, int64_t n,
@@ -148,10 +151,15 @@ void launch_romein(cudaStream_t s, const int4 *rec, const float2 *visf, int64_t 
 
 // k_towers.cu
 void launch_fresnel_table(cudaStream_t s, double *ph, int subgrid, double theta, double winc);
-void launch_tower_columns(cudaStream_t s, float2 *slots, const int *bin_of_slot,
-                          const int *tower_first, const int *tower_count, int ntowers,
-                          int nfloor, int wp_min, double winc, const double *ph,
-                          float2 *subimg, int subgrid, const float2 *tw);
+// Column stage in floor groups: group g covers active slots
+// [group_begin[g], group_end[g]) of one tower; partial holds one sub-grid per
+// group; tower t's groups are [tower_group_first[t], +tower_group_count[t]).
+void launch_tower_columns(cudaStream_t s, const float2 *slots, const int *bin_of_slot,
+                          const int *group_begin, const int *group_end, int ngroups,
+                          const int *tower_group_first, const int *tower_group_count, int ntowers,
+                          int nfloor, int wp_min, const double *ph, float2 *partial, float2 *subimg,
+                          int subgrid, const float2 *tw);
+int fft32_strips(int n);  // column strips per sub-grid in the column kernels
 void launch_add_back(cudaStream_t s, const float2 *subimg, const int *tower_count,
                      double2 *master, int grid_size, int subgrid, int margin, int chunk,
                      int nchunk, int overwrite);
