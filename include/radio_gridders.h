@@ -175,6 +175,36 @@ rg_status rg_fft2d(rg_context *ctx, void *data, int batch, int ny, int nx, int s
 rg_status rg_dft_image(rg_context *ctx, double *image_out, int grid_size, double theta,
                        const rg_vis *vis, int precision, double factor);
 
+/* ---- learned w-kernel ---------------------------------------------------- */
+
+/* A small MLP that returns the tap of the w-kernel for a continuous (w, du, dv)
+ * and tap (tx, ty), in place of the quantised oversampled table.  No
+ * counterpart in the reference (whose kernels come from crocodile table files,
+ * src/common/hdf5.c:1362-1509).  Network: 21 features -> 128 -> 128 -> 128
+ * (SiLU) -> complex tap / out_scale; BF16 tensor-core layers with FP32
+ * accumulation; trained by the library's own forward/backward kernels with
+ * Adam.  Samples are [5][n] float arrays (w, du, dv, tx, ty), taps complex
+ * float interleaved.  A network belongs to the context's device. */
+typedef struct rg_mlp rg_mlp;
+int rg_mlp_param_count(void);
+rg_status rg_mlp_create(rg_context *ctx, int ksize, double wmax, double out_scale, uint64_t seed,
+                        rg_mlp **mlp);
+rg_status rg_mlp_destroy(rg_mlp *mlp);
+rg_status rg_mlp_set_params(rg_context *ctx, rg_mlp *mlp, const float *params);
+rg_status rg_mlp_get_params(rg_context *ctx, rg_mlp *mlp, float *params);
+/* Loss and gradient of one batch without updating (checked against the CPU oracle). */
+rg_status rg_mlp_gradient(rg_context *ctx, rg_mlp *mlp, const float *samples, const float *targets,
+                          int n, float *grad_out, float *loss_out);
+/* `steps` Adam steps over consecutive batches of the training set. */
+rg_status rg_mlp_train(rg_context *ctx, rg_mlp *mlp, const float *samples, const float *targets,
+                       int64_t n, int batch, int steps, float lr, float *loss_out);
+rg_status rg_mlp_eval(rg_context *ctx, rg_mlp *mlp, const float *samples, int64_t n, float *taps_out);
+/* W-projection with taps evaluated by the network at each visibility's exact
+ * sub-cell offset and w (no oversampling quantisation).  Replaces the table
+ * lookup of grid_wprojection (src/reference/grid.c:157-202). */
+rg_status rg_grid_wprojection_learned(rg_context *ctx, rg_mlp *mlp, double *uvgrid, int grid_size,
+                                      double theta, const rg_vis *vis, int flags);
+
 #ifdef __cplusplus
 }
 #endif

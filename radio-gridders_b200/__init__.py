@@ -39,7 +39,9 @@ EXPORTS = [
     "rg_context_create", "rg_context_destroy", "rg_context_set_stream", "rg_last_error",
     "rg_last_stats", "rg_context_set_profiling", "rg_last_timings", "rg_grid_wprojection", "rg_grid_wtowers", "rg_weight",
     "rg_make_hermitian", "rg_fft_shift", "rg_image_from_grid", "rg_fft2d", "rg_dft_image",
-    "rg_grid_wprojection_noalloc",
+    "rg_grid_wprojection_noalloc", "rg_mlp_param_count", "rg_mlp_create", "rg_mlp_destroy",
+    "rg_mlp_set_params", "rg_mlp_get_params", "rg_mlp_gradient", "rg_mlp_train", "rg_mlp_eval",
+    "rg_grid_wprojection_learned",
 ]
 
 
@@ -93,6 +95,15 @@ def lib():
         L.rg_fft2d.argtypes = [vp, vp, i, i, i, i, i]
         L.rg_dft_image.argtypes = [vp, vp, i, d, ct.POINTER(_Vis), i, d]
         L.rg_grid_wprojection_noalloc.argtypes = [vp, i, d, ct.POINTER(_Vis), ct.POINTER(_WKern), i, vp]
+        L.rg_mlp_param_count.restype = i
+        L.rg_mlp_create.argtypes = [vp, i, d, d, ct.c_uint64, ct.POINTER(vp)]
+        L.rg_mlp_destroy.argtypes = [vp]
+        L.rg_mlp_set_params.argtypes = [vp, vp, vp]
+        L.rg_mlp_get_params.argtypes = [vp, vp, vp]
+        L.rg_mlp_gradient.argtypes = [vp, vp, vp, vp, i, vp, vp]
+        L.rg_mlp_train.argtypes = [vp, vp, vp, vp, i64, i, i, ct.c_float, vp]
+        L.rg_mlp_eval.argtypes = [vp, vp, vp, i64, vp]
+        L.rg_grid_wprojection_learned.argtypes = [vp, vp, vp, i, d, ct.POINTER(_Vis), i]
         for name in EXPORTS:
             getattr(L, name)  # raises AttributeError if a declared symbol is missing
         _lib = L
@@ -252,6 +263,78 @@ class Context:
         _check(lib().rg_dft_image(self._h, _ptr(image), int(grid_size), float(theta),
                                   ct.byref(vs), int(precision), float(factor)))
         return image
+
+
+class LearnedKernel:
+    """The learned w-kernel network (rg_mlp_*): tap(w, du, dv, tx, ty)."""
+
+    def __init__(self, ctx: "Context", ksize=16, wmax=2000.0, out_scale=0.05, seed=0):
+        self.ctx = ctx
+        self.ksize, self.wmax, self.out_scale = ksize, wmax, out_scale
+        self._h = ct.c_void_p()
+        _check(lib().rg_mlp_create(ctx.handle, ksize, float(wmax), float(out_scale), int(seed),
+                                   ct.byref(self._h)))
+
+    def close(self):
+        if self._h:
+            lib().rg_mlp_destroy(self._h)
+            self._h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    @staticmethod
+    def samples(w, du, dv, tx, ty):
+        return np.ascontiguousarray(np.stack([w, du, dv, tx, ty]).astype(np.float32))
+
+    @staticmethod
+    def targets(taps):
+        t = np.asarray(taps, np.complex128)
+        return np.ascontiguousarray(np.stack([t.real, t.imag], axis=-1).astype(np.float32))
+
+    def get_params(self):
+        out = np.empty(lib().rg_mlp_param_count(), np.float32)
+        _check(lib().rg_mlp_get_params(self.ctx.handle, self._h, _ptr(out)))
+        return out
+
+    def set_params(self, params):
+        p = np.ascontiguousarray(params, np.float32)
+        _check(lib().rg_mlp_set_params(self.ctx.handle, self._h, _ptr(p)))
+
+    def gradient(self, samples, targets):
+        n = samples.shape[1]
+        g = np.empty(lib().rg_mlp_param_count(), np.float32)
+        loss = np.zeros(1, np.float32)
+        _check(lib().rg_mlp_gradient(self.ctx.handle, self._h, _ptr(samples), _ptr(targets), int(n),
+                                     _ptr(g), _ptr(loss)))
+        return float(loss[0]), g
+
+    def train(self, samples, targets, batch=16384, steps=100, lr=1e-3):
+        n = samples.shape[1] if not hasattr(samples, "data_ptr") else samples.shape[1]
+        loss = np.zeros(1, np.float32)
+        _check(lib().rg_mlp_train(self.ctx.handle, self._h, _ptr(samples), _ptr(targets), int(n),
+                                  int(batch), int(steps), ct.c_float(lr), _ptr(loss)))
+        return float(loss[0])
+
+    def eval(self, samples):
+        n = samples.shape[1]
+        out = np.empty((n, 2), np.float32)
+        _check(lib().rg_mlp_eval(self.ctx.handle, self._h, _ptr(samples), int(n), _ptr(out)))
+        return out[:, 0].astype(np.complex128) + 1j * out[:, 1]
+
+
+def grid_wprojection_learned(ctx, mlp, uvgrid, grid_size, theta, vis, flags=RG_GRID_ACCUMULATE):
+    vs = vis.struct()
+    _check(lib().rg_grid_wprojection_learned(ctx.handle, mlp.handle, _ptr(uvgrid), int(grid_size),
+                                             float(theta), ct.byref(vs), int(flags)))
+    return uvgrid
 
 
 _default = None

@@ -50,6 +50,19 @@ struct Buffer {
     size_t bytes = 0;
 };
 
+// k_mlp.cu — learned w-kernel
+int mlp_param_count();
+int mlp_bf16_count();
+void launch_mlp_grad(cudaStream_t s, const float *P, const void *PB, const float *in, const float2 *target,
+                     int n, int ksize, float inv_wmax, float inv_scale, float *grad, float *loss);
+void launch_mlp_adam(cudaStream_t s, float *P, void *PB, float *grad, float *m, float *v, float lr, int step);
+void launch_mlp_to_bf16(cudaStream_t s, const float *P, void *PB);
+void launch_mlp_eval(cudaStream_t s, const float *P, const void *PB, const float *in, int n, int ksize,
+                     float inv_wmax, float scale, float2 *out, int sm_count);
+void launch_learned_wproj(cudaStream_t s, const double *u, const double *v, const double *w,
+                          const double2 *vis, int64_t n, int N, double theta, const float *P, const void *PB,
+                          int ksize, float inv_wmax, float scale, float2 *grid, int sm_count);
+
 }  // namespace rg
 
 struct rg_stage_event {
@@ -168,5 +181,18 @@ void launch_add_back(cudaStream_t s, const float2 *subimg, const int *tower_coun
 void launch_dft(cudaStream_t s, const double *u, const double *v, const double *w,
                 const double2 *vis, int64_t n, double *image, int grid_size, double theta,
                 int precision, double factor, int sm_count);
+
+// k_mlp.cu — learned w-kernel
+int mlp_param_count();
+int mlp_bf16_count();
+void launch_mlp_grad(cudaStream_t s, const float *P, const void *PB, const float *in, const float2 *target,
+                     int n, int ksize, float inv_wmax, float inv_scale, float *grad, float *loss);
+void launch_mlp_adam(cudaStream_t s, float *P, void *PB, float *grad, float *m, float *v, float lr, int step);
+void launch_mlp_to_bf16(cudaStream_t s, const float *P, void *PB);
+void launch_mlp_eval(cudaStream_t s, const float *P, const void *PB, const float *in, int n, int ksize,
+                     float inv_wmax, float scale, float2 *out, int sm_count);
+void launch_learned_wproj(cudaStream_t s, const double *u, const double *v, const double *w,
+                          const double2 *vis, int64_t n, int N, double theta, const float *P, const void *PB,
+                          int ksize, float inv_wmax, float scale, float2 *grid, int sm_count);
 
 }  // namespace rg

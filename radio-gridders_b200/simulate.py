@@ -390,10 +390,11 @@ def dft_study(seed: int = 2, n_vis: int = 200_000, theta: float = 0.05,
 
 
 def learned_wproj(seed: int = 3, n_vis: int = 1_000_000, theta: float = 0.1,
-                  lam: float = 20480.0, ksize: int = 16):
+                  lam: float = 20480.0, ksize: int = 16, w_limit: float = 2000.0):
     """Learned-kernel W-projection workload: the W-projection generator scaled to
     a 2048x2048 grid (theta 0.1, lambda 20480) with 1,000,000 visibilities
-    (351 baselines x 2850 dumps, truncated)."""
+    (351 baselines x 2850 dumps, truncated).  Recorded knob: w is scaled so
+    max |w| = w_limit (the learned kernel's training range)."""
     rng = np.random.default_rng(seed)
     enu = uniform_disc(rng, 27, 10_000.0)
     lat, dec = 10.0, -30.0
@@ -403,9 +404,13 @@ def learned_wproj(seed: int = 3, n_vis: int = 1_000_000, theta: float = 0.1,
     n_grid = int(theta * lam)
     scale = fit_scale(enu, lat, dec, ha, freqs, (n_grid / 2 - ksize / 2 - 2) / theta)
     src = random_sources(rng, 10, theta, "uniform")
-    obs = observe(enu * scale, lat, dec, ha, freqs, src)
+    xyz = enu_to_xyz(enu * scale, math.radians(lat))
+    a1, a2 = _pairs(len(enu))
+    uvw = baseline_uvw(xyz[a2] - xyz[a1], ha * math.pi / 12, math.radians(dec))
+    wmax = np.max(np.abs(uvw[:, :, 2])) * freqs[0] / C_LIGHT
+    obs = observe(enu * scale, lat, dec, ha, freqs, src, w_scale=w_limit / wmax)
     obs.meta = dict(name="learned_wproj", theta=theta, lam=lam, grid_size=n_grid,
-                    array_scale=scale, sources=src, seed=seed, n_vis=n_vis)
+                    array_scale=scale, w_scale=w_limit / wmax, sources=src, seed=seed, n_vis=n_vis)
     return obs
 
 
@@ -420,3 +425,39 @@ def wkernel_for(flat_w: np.ndarray, theta: float, w_step: float, size: int = 16,
     hi = math.ceil(max(float(np.max(flat_w)), 0.0) / w_step) + 1
     planes = np.arange(lo, hi + 1) * w_step
     return generate_wkernel(theta, planes, size, oversampling, c)
+
+
+def learned_training_set(n_triples: int, wmax: float, theta: float, size: int = 16,
+                         c: float | None = None, seed: int = 0, m_pix: int = 128,
+                         batch: int = 128):
+    """Training taps for the learned w-kernel: n_triples random (w, du, dv) with
+    w uniform in [-wmax, wmax] and du, dv uniform in [0, 1), each with all
+    size x size taps of the generator's continuous kernel
+        K_w(tx - size/2 - du, ty - size/2 - dv)   (kernel_taps).
+    Returns (w, du, dv, tx, ty) float arrays and complex128 targets, one entry
+    per tap (n_triples * size^2)."""
+    if c is None:
+        c = math.pi * (size - 2) / 2.0
+    rng = np.random.default_rng(seed)
+    w = rng.uniform(-wmax, wmax, n_triples)
+    du = rng.uniform(0.0, 1.0, n_triples)
+    dv = rng.uniform(0.0, 1.0, n_triples)
+    lm = screen_coords(theta, m_pix)
+    a = pswf0(c, 2.0 * lm / theta)
+    taper = a[None, :] * a[:, None]
+    one_minus_n = 1.0 - np.sqrt(1.0 - (lm[None, :] ** 2 + lm[:, None] ** 2))
+    taps = np.arange(size) - size // 2
+    out = np.empty((n_triples, size, size), np.complex128)
+    for b0 in range(0, n_triples, batch):
+        sl = slice(b0, min(b0 + batch, n_triples))
+        s = taper[None] * np.exp(2j * np.pi * w[sl, None, None] * one_minus_n[None])
+        px = taps[None, :] - du[sl, None]
+        qy = taps[None, :] - dv[sl, None]
+        ex = np.exp(-2j * np.pi * px[:, :, None] * lm[None, None, :] / theta)
+        ey = np.exp(-2j * np.pi * qy[:, :, None] * lm[None, None, :] / theta)
+        out[sl] = ey @ s @ np.transpose(ex, (0, 2, 1)) / (m_pix * m_pix)
+    ty, tx = np.meshgrid(np.arange(size), np.arange(size), indexing="ij")
+    rep = size * size
+    return (np.repeat(w, rep), np.repeat(du, rep), np.repeat(dv, rep),
+            np.tile(tx.ravel(), n_triples).astype(np.float64),
+            np.tile(ty.ravel(), n_triples).astype(np.float64), out.reshape(-1))
