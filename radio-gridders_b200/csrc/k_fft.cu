@@ -45,16 +45,25 @@ __device__ __forceinline__ float2 twiddle(const float2 *W, int k)
 // ---------------------------------------------------------------------------
 // rows: R rows of length N = N1*32 per CTA, 256 threads
 // ---------------------------------------------------------------------------
+// rows: the row count, or, when count_dev is given, min(rows, *count_dev * N)
+// (the number of active sub-grids lives on the device; the grid is sized for
+// the capacity and CTAs past the live rows return at once).
 template <int N1, int SIGN>
 __global__ void __launch_bounds__(256) fft32_rows_kernel(float2 *__restrict__ data, int64_t rows,
-                                                         const float2 *__restrict__ tw)
+                                                         const float2 *__restrict__ tw,
+                                                         const int *__restrict__ count_dev)
 {
     constexpr int N = N1 * 32, R = 16, LB = ilog2c(N1);
     extern __shared__ float2 smem[];
     float2 *T = smem;                 // [R][N1][kPad]
     float2 *W = smem + R * N1 * kPad;  // [N]
-    for (int i = threadIdx.x; i < N; i += blockDim.x) W[i] = tw[i];
     const int64_t row0 = (int64_t)blockIdx.x * R;
+    if (count_dev) {
+        const int64_t live = (int64_t)(*count_dev) * N;
+        if (live < rows) rows = live;
+    }
+    if (row0 >= rows) return;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) W[i] = tw[i];
     __syncthreads();
 
     for (int it = threadIdx.x; it < R * N1; it += blockDim.x) {
@@ -175,9 +184,9 @@ using PartialGeom = ColGeom<N1, 8>;
 template <int N1>
 __global__ void __launch_bounds__(kPartialThreads) tower_partial_kernel(
     const float2 *__restrict__ slots, const int *__restrict__ bin_of_slot,
-    const int *__restrict__ group_begin, const int *__restrict__ group_end, int nfloor,
-    int wp_min, const double *__restrict__ ph, float2 *__restrict__ partial,
-    const float2 *__restrict__ tw)
+    const int *__restrict__ group_begin, const int *__restrict__ group_end,
+    const int *__restrict__ range, const int *__restrict__ counts, int slot_cap,
+    const double *__restrict__ ph, float2 *__restrict__ partial, const float2 *__restrict__ tw)
 {
     using G = PartialGeom<N1>;
     constexpr int N = G::N, C = G::C;
@@ -189,7 +198,10 @@ __global__ void __launch_bounds__(kPartialThreads) tower_partial_kernel(
     double *P = reinterpret_cast<double *>(W + N);  // [N][C] Fresnel phase of the strip
     const int strips = N / C;
     const int group = blockIdx.x / strips, strip = blockIdx.x % strips;
-    const int begin = group_begin[group], end = group_end[group];
+    if (group >= counts[1]) return;  // groups live on the device; grid sized for capacity
+    const int wp_min = range[0], nfloor = range[1];
+    const int begin = group_begin[group];
+    const int end = group_end[group] < slot_cap ? group_end[group] : slot_cap;
     for (int i = threadIdx.x; i < N; i += blockDim.x) W[i] = tw[i];
     for (int e = threadIdx.x; e < N * C; e += blockDim.x)
         P[e] = ph[(int64_t)(e / C) * N + strip * C + e % C];
@@ -243,7 +255,7 @@ __global__ void __launch_bounds__(kPartialThreads) tower_partial_kernel(
 template <int N1>
 __global__ void __launch_bounds__(256) tower_finish_kernel(
     const float2 *__restrict__ partial, const int *__restrict__ tower_group_first,
-    const int *__restrict__ tower_group_count, float2 *__restrict__ subimg,
+    const int *__restrict__ tower_group_count, int group_cap, float2 *__restrict__ subimg,
     const float2 *__restrict__ tw)
 {
     using G = ColGeom<N1>;
@@ -254,9 +266,10 @@ __global__ void __launch_bounds__(256) tower_finish_kernel(
     float2 *U = W + N;  // [N][C]
     const int strips = N / C;
     const int tower = blockIdx.x / strips, strip = blockIdx.x % strips;
-    const int gcount = tower_group_count[tower];
-    if (gcount == 0) return;
     const int gfirst = tower_group_first[tower];
+    int gcount = tower_group_count[tower];
+    if (gfirst + gcount > group_cap) gcount = group_cap - gfirst;  // capacity overflow: rerun
+    if (gcount <= 0) return;
     for (int i = threadIdx.x; i < N; i += blockDim.x) W[i] = tw[i];
     for (int e = threadIdx.x; e < N * C; e += blockDim.x) {
         const int row = e / C, c = e % C;
@@ -300,16 +313,18 @@ static size_t finish_smem()
 }
 
 template <int N1>
-static void rows_impl(cudaStream_t s, float2 *data, int64_t rows, int sign, const float2 *tw)
+static void rows_impl(cudaStream_t s, float2 *data, int64_t rows, int sign, const float2 *tw,
+                      const int *count_dev)
 {
     const size_t sm = rows_smem<N1>();
     const unsigned blocks = (unsigned)((rows + 15) / 16);
+    if (blocks == 0) return;
     if (sign < 0) {
         cudaFuncSetAttribute(fft32_rows_kernel<N1, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        fft32_rows_kernel<N1, -1><<<blocks, 256, sm, s>>>(data, rows, tw);
+        fft32_rows_kernel<N1, -1><<<blocks, 256, sm, s>>>(data, rows, tw, count_dev);
     } else {
         cudaFuncSetAttribute(fft32_rows_kernel<N1, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        fft32_rows_kernel<N1, +1><<<blocks, 256, sm, s>>>(data, rows, tw);
+        fft32_rows_kernel<N1, +1><<<blocks, 256, sm, s>>>(data, rows, tw, count_dev);
     }
 }
 
@@ -329,22 +344,22 @@ static void cols_impl(cudaStream_t s, float2 *data, int batch, int sign, const f
 
 template <int N1>
 static void tower_impl(cudaStream_t s, const float2 *slots, const int *bin_of_slot,
-                       const int *group_begin, const int *group_end, int ngroups,
+                       const int *group_begin, const int *group_end, const int *range,
+                       const int *counts, int slot_cap, int group_cap,
                        const int *tower_group_first, const int *tower_group_count, int ntowers,
-                       int nfloor, int wp_min, const double *ph, float2 *partial, float2 *subimg,
-                       const float2 *tw)
+                       const double *ph, float2 *partial, float2 *subimg, const float2 *tw)
 {
     const int pstrips = N1 * 32 / PartialGeom<N1>::C;
     const int strips = N1 * 32 / ColGeom<N1>::C;
     const size_t sm1 = partial_smem<N1>();
     cudaFuncSetAttribute(tower_partial_kernel<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
-    if (ngroups > 0)
-        tower_partial_kernel<N1><<<(unsigned)ngroups * pstrips, kPartialThreads, sm1, s>>>(
-            slots, bin_of_slot, group_begin, group_end, nfloor, wp_min, ph, partial, tw);
+    if (group_cap > 0)
+        tower_partial_kernel<N1><<<(unsigned)group_cap * pstrips, kPartialThreads, sm1, s>>>(
+            slots, bin_of_slot, group_begin, group_end, range, counts, slot_cap, ph, partial, tw);
     const size_t sm2 = finish_smem<N1>();
     cudaFuncSetAttribute(tower_finish_kernel<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
     tower_finish_kernel<N1><<<(unsigned)ntowers * strips, 256, sm2, s>>>(
-        partial, tower_group_first, tower_group_count, subimg, tw);
+        partial, tower_group_first, tower_group_count, group_cap, subimg, tw);
 }
 
 #define RG_DISPATCH_N1(n, CALL) \
@@ -357,9 +372,10 @@ static void tower_impl(cudaStream_t s, const float2 *slots, const int *bin_of_sl
         default: break;          \
     }
 
-void launch_fft32_rows(cudaStream_t s, float2 *data, int64_t rows, int n, int sign, const float2 *tw)
+void launch_fft32_rows(cudaStream_t s, float2 *data, int64_t rows, int n, int sign, const float2 *tw,
+                       const int *count_dev)
 {
-#define CALL(N1) rows_impl<N1>(s, data, rows, sign, tw)
+#define CALL(N1) rows_impl<N1>(s, data, rows, sign, tw, count_dev)
     RG_DISPATCH_N1(n, CALL)
 #undef CALL
 }
@@ -372,14 +388,15 @@ void launch_fft32_cols(cudaStream_t s, float2 *data, int batch, int n, int sign,
 }
 
 void launch_tower_columns(cudaStream_t s, const float2 *slots, const int *bin_of_slot,
-                          const int *group_begin, const int *group_end, int ngroups,
+                          const int *group_begin, const int *group_end, const int *range,
+                          const int *counts, int slot_cap, int group_cap,
                           const int *tower_group_first, const int *tower_group_count, int ntowers,
-                          int nfloor, int wp_min, const double *ph, float2 *partial, float2 *subimg,
-                          int subgrid, const float2 *tw)
+                          const double *ph, float2 *partial, float2 *subimg, int subgrid,
+                          const float2 *tw)
 {
-#define CALL(N1) tower_impl<N1>(s, slots, bin_of_slot, group_begin, group_end, ngroups,           \
-                                tower_group_first, tower_group_count, ntowers, nfloor, wp_min, ph, \
-                                partial, subimg, tw)
+#define CALL(N1) tower_impl<N1>(s, slots, bin_of_slot, group_begin, group_end, range, counts, slot_cap, \
+                                group_cap, tower_group_first, tower_group_count, ntowers, ph, partial,  \
+                                subimg, tw)
     RG_DISPATCH_N1(subgrid, CALL)
 #undef CALL
 }

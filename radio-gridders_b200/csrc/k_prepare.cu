@@ -75,6 +75,26 @@ void launch_minmax_w(cudaStream_t s, const double *u, const double *v, const dou
     minmax_w_kernel<<<blocks, 256, 0, s>>>(u, v, w, n, (unsigned long long *)out2, err);
 }
 
+// Floors spanned by the w range (grid.c:357-367): wp = floor(w / winc + 0.5)
+// for the range's ends (which include 0).
+__global__ void w_floors_kernel(const double *__restrict__ wrange, double winc, int floors_cap,
+                                int *__restrict__ range, unsigned *err)
+{
+    const int wp_min = (int)floor(wrange[0] / winc + 0.5);
+    const int wp_max = (int)floor(wrange[1] / winc + 0.5);
+    const long long nfloor = (long long)wp_max - wp_min + 1;
+    range[0] = wp_min;
+    range[1] = (int)(nfloor < (1 << 30) ? nfloor : (1 << 30));
+    range[2] = nfloor <= floors_cap ? 1 : 0;
+    if (nfloor > floors_cap) atomicOr(err, DERR_CAPACITY);
+}
+
+void launch_w_floors(cudaStream_t s, const double *wrange, double winc, int floors_cap, int *range,
+                     unsigned *err)
+{
+    w_floors_kernel<<<1, 1, 0, s>>>(wrange, winc, floors_cap, range, err);
+}
+
 struct Bounds {
     double lo, hi, mid;
     int origin;
@@ -102,11 +122,13 @@ __device__ __forceinline__ void frac_axis(double coord, double mid, double theta
 
 __global__ void prepare_towers_kernel(const double *__restrict__ u, const double *__restrict__ v,
                                       const double *__restrict__ w, const double2 *__restrict__ vis,
-                                      int64_t n, TowerGeom g, int wp_min, int nfloor,
+                                      int64_t n, TowerGeom g, const int *__restrict__ range,
                                       int4 *__restrict__ rec, float2 *__restrict__ visf,
                                       int *__restrict__ active, unsigned *err,
                                       unsigned long long *counters)
 {
+    if (!range[2]) return;  // more floors than the bin capacity: the caller reruns
+    const int wp_min = range[0], nfloor = range[1];
     const double half_over_ov = 0.5 / (double)g.ov;
     const int wp_max = wp_min + nfloor - 1;
     const int taps_total = g.planes * g.ov * g.ov * g.ksize * g.ksize;
@@ -195,15 +217,15 @@ __global__ void prepare_towers_kernel(const double *__restrict__ u, const double
 }
 
 void launch_prepare_towers(cudaStream_t s, const double *u, const double *v, const double *w,
-                           const double2 *vis, int64_t n, TowerGeom g, int wp_min, int nfloor,
+                           const double2 *vis, int64_t n, TowerGeom g, const int *range,
                            int4 *rec, float2 *visf, int *active, unsigned *err,
                            unsigned long long *counters)
 {
     int blocks = (int)((n + 255) / 256);
     if (blocks > 148 * 16) blocks = 148 * 16;
     if (blocks < 1) blocks = 1;
-    prepare_towers_kernel<<<blocks, 256, 0, s>>>(u, v, w, vis, n, g, wp_min, nfloor, rec, visf,
-                                                 active, err, counters);
+    prepare_towers_kernel<<<blocks, 256, 0, s>>>(u, v, w, vis, n, g, range, rec, visf, active, err,
+                                                 counters);
 }
 
 __global__ void prepare_wproj_kernel(const double *__restrict__ u, const double *__restrict__ v,
@@ -298,7 +320,7 @@ __device__ int block_exclusive_scan(int x, int *warp_sums, int *total)
 // so each tower's slots are contiguous and ordered by floor; then the floor
 // groups of the column stage (up to G consecutive slots of one tower, G chosen
 // so the stage has about target_items (group, strip) work items).
-__global__ void compact_bins_kernel(const int *__restrict__ active, int nbins, int nfloor,
+__global__ void compact_bins_kernel(const int *__restrict__ active, const int *__restrict__ range,
                                     int *__restrict__ slot_of_bin, int *__restrict__ bin_of_slot,
                                     int *__restrict__ counts, int *__restrict__ tower_first,
                                     int *__restrict__ tower_count, int ntowers, int strips,
@@ -307,6 +329,8 @@ __global__ void compact_bins_kernel(const int *__restrict__ active, int nbins, i
                                     int *__restrict__ tower_group_count)
 {
     __shared__ int warp_sums[32];
+    const int nfloor = range[2] ? range[1] : 0;
+    const int nbins = ntowers * nfloor;
     int carry = 0;
     for (int base = 0; base < nbins; base += blockDim.x) {
         const int b = base + threadIdx.x;
@@ -320,8 +344,8 @@ __global__ void compact_bins_kernel(const int *__restrict__ active, int nbins, i
     const int n_active = carry;
     __syncthreads();
     for (int t = threadIdx.x; t < ntowers; t += blockDim.x) {
-        const int first = slot_of_bin[t * nfloor];
-        const int next = (t + 1 < ntowers) ? slot_of_bin[(t + 1) * nfloor] : n_active;
+        const int first = nfloor ? slot_of_bin[t * nfloor] : 0;
+        const int next = (t + 1 < ntowers && nfloor) ? slot_of_bin[(t + 1) * nfloor] : n_active;
         tower_first[t] = first;
         tower_count[t] = next - first;
     }
@@ -331,6 +355,7 @@ __global__ void compact_bins_kernel(const int *__restrict__ active, int nbins, i
     long long want = ((long long)n_active * strips + target_items - 1) / (target_items > 0 ? target_items : 1);
     int G = (int)(want < 4 ? 4 : (want > 64 ? 64 : want));
     carry = 0;
+    int with_data = 0;
     for (int base = 0; base < ntowers; base += blockDim.x) {
         const int t = base + threadIdx.x;
         const int cnt = t < ntowers ? tower_count[t] : 0;
@@ -338,6 +363,7 @@ __global__ void compact_bins_kernel(const int *__restrict__ active, int nbins, i
         int total;
         const int gfirst = carry + block_exclusive_scan(ng, warp_sums, &total);
         if (t < ntowers) {
+            with_data += cnt > 0;
             tower_group_first[t] = gfirst;
             tower_group_count[t] = ng;
             const int sfirst = tower_first[t];
@@ -350,18 +376,22 @@ __global__ void compact_bins_kernel(const int *__restrict__ active, int nbins, i
         }
         carry += total;
     }
+    int total_with_data;
+    const int unused = block_exclusive_scan(with_data, warp_sums, &total_with_data);
+    (void)unused;
     if (threadIdx.x == 0) {
         counts[0] = n_active;
         counts[1] = carry;
+        counts[2] = total_with_data;
     }
 }
 
-void launch_compact_bins(cudaStream_t s, const int *active, int nbins, int nfloor, int *slot_of_bin,
+void launch_compact_bins(cudaStream_t s, const int *active, const int *range, int *slot_of_bin,
                          int *bin_of_slot, int *counts, int *tower_first, int *tower_count,
                          int ntowers, int strips, int target_items, int *group_begin,
                          int *group_end, int *tower_group_first, int *tower_group_count)
 {
-    compact_bins_kernel<<<1, 1024, 0, s>>>(active, nbins, nfloor, slot_of_bin, bin_of_slot, counts,
+    compact_bins_kernel<<<1, 1024, 0, s>>>(active, range, slot_of_bin, bin_of_slot, counts,
                                            tower_first, tower_count, ntowers, strips, target_items,
                                            group_begin, group_end, tower_group_first,
                                            tower_group_count);

@@ -29,7 +29,7 @@ template <int K>
 __global__ void __launch_bounds__(K *K) romein_kernel(
     const int4 *__restrict__ rec, const float2 *__restrict__ visf, int64_t n,
     const float2 *__restrict__ taps, float2 *__restrict__ grids,
-    const int *__restrict__ slot_of_bin, int64_t grid_stride, int side, int64_t chunk)
+    const int *__restrict__ slot_of_bin, int64_t grid_stride, int side, int64_t chunk, int slot_cap)
 {
     constexpr int BATCH = K * K;
     __shared__ int4 srec[BATCH];
@@ -62,8 +62,10 @@ __global__ void __launch_bounds__(K *K) romein_kernel(
                 if (r.x >= 0) {
                     const int idx = r.y + cv * side + cu;
                     if (r.x != cur_bin || idx != cur_idx) {
-                        if (cur_bin >= 0 && (unsigned)cur_idx < (unsigned)limit)
-                            atomicAdd(grids + (int64_t)slot_of_bin[cur_bin] * grid_stride + cur_idx, sum);
+                        if (cur_bin >= 0 && (unsigned)cur_idx < (unsigned)limit) {
+                            const int slot = slot_of_bin[cur_bin];
+                            if (slot < slot_cap) atomicAdd(grids + (int64_t)slot * grid_stride + cur_idx, sum);
+                        }
                         cur_bin = r.x;
                         cur_idx = idx;
                         sum = make_float2(0.f, 0.f);
@@ -78,14 +80,16 @@ __global__ void __launch_bounds__(K *K) romein_kernel(
                 t = tn;
             }
         }
-        if (cur_bin >= 0 && (unsigned)cur_idx < (unsigned)limit)
-            atomicAdd(grids + (int64_t)slot_of_bin[cur_bin] * grid_stride + cur_idx, sum);
+        if (cur_bin >= 0 && (unsigned)cur_idx < (unsigned)limit) {
+            const int slot = slot_of_bin[cur_bin];
+            if (slot < slot_cap) atomicAdd(grids + (int64_t)slot * grid_stride + cur_idx, sum);
+        }
     }
 }
 
 void launch_romein(cudaStream_t s, const int4 *rec, const float2 *visf, int64_t n,
                    const float2 *taps, float2 *grids, const int *slot_of_bin, int64_t grid_stride,
-                   int grid_side, int ksize, int sm_count)
+                   int grid_side, int ksize, int sm_count, int slot_cap)
 {
     const int64_t chunk = 1024;
     int64_t blocks = (n + chunk - 1) / chunk;
@@ -95,19 +99,19 @@ void launch_romein(cudaStream_t s, const int4 *rec, const float2 *visf, int64_t 
     switch (ksize) {
         case 4:
             romein_kernel<4><<<(unsigned)blocks, 16, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin,
-                                                             grid_stride, grid_side, chunk);
+                                                             grid_stride, grid_side, chunk, slot_cap);
             break;
         case 8:
             romein_kernel<8><<<(unsigned)blocks, 64, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin,
-                                                             grid_stride, grid_side, chunk);
+                                                             grid_stride, grid_side, chunk, slot_cap);
             break;
         case 16:
             romein_kernel<16><<<(unsigned)blocks, 256, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin,
-                                                               grid_stride, grid_side, chunk);
+                                                               grid_stride, grid_side, chunk, slot_cap);
             break;
         case 32:
             romein_kernel<32><<<(unsigned)blocks, 1024, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin,
-                                                                grid_stride, grid_side, chunk);
+                                                                grid_stride, grid_side, chunk, slot_cap);
             break;
         default: break;
     }

@@ -31,16 +31,38 @@ void launch_fresnel_table(cudaStream_t s, double *ph, int subgrid, double theta,
     fresnel_table_kernel<<<blocks, 256, 0, s>>>(ph, subgrid, theta, winc);
 }
 
+// Zero the live sub-grids (counts[0] of them, at most slot_cap).
+__global__ void zero_slots_kernel(float4 *__restrict__ slots, const int *__restrict__ counts, int slot_cap,
+                                  int64_t slot_elems4)
+{
+    const int live = counts[0] < slot_cap ? counts[0] : slot_cap;
+    const int64_t total = (int64_t)live * slot_elems4;
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x)
+        slots[i] = z;
+}
+
+void launch_zero_slots(cudaStream_t s, float2 *slots, const int *counts, int slot_cap, int64_t slot_elems,
+                       int sm_count)
+{
+    zero_slots_kernel<<<sm_count * 8, 512, 0, s>>>((float4 *)slots, counts, slot_cap, slot_elems / 2);
+}
+
 // Owner-computes add-back (src/reference/grid.c:503-516): every master pixel
 // sums, in tower order (cy, then cx), the overlapping towers' forward-
 // transformed sub-images divided by S^2, in FP64.  Deterministic.
+// When a capacity overflowed (range[2] == 0 or a live count above its
+// capacity) nothing is written, so the caller can rerun on the same grid.
 __global__ void add_back_kernel(const float2 *__restrict__ subimg, const int *__restrict__ tower_count,
                                 double2 *__restrict__ master, int N, int S, int M, int chunk,
-                                int nchunk, int overwrite)
+                                int nchunk, int overwrite, const int *__restrict__ range,
+                                const int *__restrict__ counts, int slot_cap, int group_cap)
 {
     const int gx = blockIdx.x * blockDim.x + threadIdx.x;
     const int gy = blockIdx.y * blockDim.y + threadIdx.y;
     if (gx >= N || gy >= N) return;
+    if (range && (!range[2] || counts[0] > slot_cap || counts[1] > group_cap)) return;
     const int ax = gx + M / 2, ay = gy + M / 2;  // x + N/2 + M/2 with x = gx - N/2
     int cx_hi = ax / chunk, cy_hi = ay / chunk;
     int cx_lo = (ax - S) >= 0 ? (ax - S) / chunk + 1 : 0;
@@ -67,12 +89,13 @@ __global__ void add_back_kernel(const float2 *__restrict__ subimg, const int *__
 }
 
 void launch_add_back(cudaStream_t s, const float2 *subimg, const int *tower_count, double2 *master,
-                     int grid_size, int subgrid, int margin, int chunk, int nchunk, int overwrite)
+                     int grid_size, int subgrid, int margin, int chunk, int nchunk, int overwrite,
+                     const int *range, const int *counts, int slot_cap, int group_cap)
 {
     dim3 blk(32, 8);
     dim3 grd((grid_size + 31) / 32, (grid_size + 7) / 8);
     add_back_kernel<<<grd, blk, 0, s>>>(subimg, tower_count, master, grid_size, subgrid, margin,
-                                        chunk, nchunk, overwrite);
+                                        chunk, nchunk, overwrite, range, counts, slot_cap, group_cap);
 }
 
 }  // namespace rg

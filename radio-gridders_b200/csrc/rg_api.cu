@@ -415,6 +415,151 @@ rg_status rg_grid_wprojection(rg_context *ctx, double *uvgrid, int grid_size, do
     return RG_OK;
 }
 
+}  // extern "C"
+
+namespace rg {
+
+// One W-towers pass with fixed capacities: every launch is sized by the plan's
+// capacities and reads the live counts (w floors, active sub-grids, floor
+// groups) from device memory, so the host enqueues the whole pass without
+// waiting; one read-back at the end returns the error word, the counters and
+// the live counts.  *overflow is set when a capacity was too small (the caller
+// grows the plan and runs again).
+static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *taps, const rg_wkern *wkern,
+                              double *out_dev, int N, double theta, int S, int M, double winc, int flags,
+                              TowerPlan &pl, bool *overflow)
+{
+    cudaStream_t st = ctx->stream;
+    const int K = wkern->size;
+    const int chunk = S - M;
+    const int nchunk = N / chunk + 1;
+    const int ntowers = nchunk * nchunk;
+    const int64_t sub_cells = (int64_t)S * S;
+    const int nbins_cap = ntowers * pl.floors_cap;
+
+    Diag d;
+    RG_CHECK(diag_begin(ctx, &d));
+    int *range = (int *)((char *)d.err + 48);    // {wp_min, nfloor, ok}
+    int *counts = (int *)((char *)d.err + 32);   // {slots, groups, towers with data}
+
+    void *mm, *active, *rec, *visf, *slot_of_bin, *bin_of_slot, *tfirst, *tcount, *gbegin, *gend, *tgfirst,
+        *tgcount, *slots, *partial, *subimg, *ph;
+    RG_CHECK(scratch(ctx, "wminmax", 16, &mm));
+    RG_CHECK(scratch(ctx, "active", sizeof(int) * (size_t)nbins_cap, &active));
+    RG_CHECK(scratch(ctx, "rec", sizeof(int4) * (size_t)dv.n, &rec));
+    RG_CHECK(scratch(ctx, "visf", sizeof(float2) * (size_t)dv.n, &visf));
+    RG_CHECK(scratch(ctx, "slot_of_bin", sizeof(int) * (size_t)nbins_cap, &slot_of_bin));
+    RG_CHECK(scratch(ctx, "bin_of_slot", sizeof(int) * (size_t)nbins_cap, &bin_of_slot));
+    RG_CHECK(scratch(ctx, "tower_first", sizeof(int) * (size_t)ntowers, &tfirst));
+    RG_CHECK(scratch(ctx, "tower_count", sizeof(int) * (size_t)ntowers, &tcount));
+    RG_CHECK(scratch(ctx, "group_begin", sizeof(int) * (size_t)nbins_cap, &gbegin));
+    RG_CHECK(scratch(ctx, "group_end", sizeof(int) * (size_t)nbins_cap, &gend));
+    RG_CHECK(scratch(ctx, "tower_group_first", sizeof(int) * (size_t)ntowers, &tgfirst));
+    RG_CHECK(scratch(ctx, "tower_group_count", sizeof(int) * (size_t)ntowers, &tgcount));
+    RG_CHECK(scratch(ctx, "slots", sizeof(float2) * (size_t)(sub_cells * pl.slots_cap), &slots));
+    RG_CHECK(scratch(ctx, "partial", sizeof(float2) * (size_t)(sub_cells * pl.groups_cap), &partial));
+    RG_CHECK(scratch(ctx, "subimg", sizeof(float2) * (size_t)(sub_cells * ntowers), &subimg));
+    float2 *tw;
+    RG_CHECK(get_twiddles32(ctx, S, &tw));
+    {
+        char key[160];
+        std::snprintf(key, sizeof(key), "ph_%d_%.17g_%.17g", S, theta, winc);
+        bool fresh = ctx->scratch.find(key) == ctx->scratch.end();
+        RG_CHECK(scratch(ctx, key, sizeof(double) * (size_t)sub_cells, &ph));
+        if (fresh) {
+            launch_fresnel_table(st, (double *)ph, S, theta, winc);
+            ctx->launches++;
+        }
+    }
+    RG_CUDA(cudaMemsetAsync(active, 0, sizeof(int) * (size_t)nbins_cap, st));
+
+    TowerGeom g;
+    g.grid_size = N;
+    g.subgrid = S;
+    g.margin = M;
+    g.chunk = chunk;
+    g.nchunk = nchunk;
+    g.ksize = K;
+    g.ov = wkern->oversampling;
+    g.planes = wkern->plane_count;
+    g.theta = theta;
+    g.winc = winc;
+    g.wk_wmin = wkern->w_min;
+    g.wk_wstep = wkern->w_step;
+    const int strips = fft32_strips(S);
+
+    begin_stage(ctx, "w_range");
+    launch_minmax_w(st, dv.u, dv.v, dv.w, dv.n, (double *)mm, d.err);
+    launch_w_floors(st, (const double *)mm, winc, pl.floors_cap, range, d.err);
+    end_stage(ctx);
+    begin_stage(ctx, "prepare");
+    if (dv.n > 0)
+        launch_prepare_towers(st, dv.u, dv.v, dv.w, dv.vis, dv.n, g, range, (int4 *)rec, (float2 *)visf,
+                              (int *)active, d.err, d.counters);
+    end_stage(ctx);
+    begin_stage(ctx, "compact");
+    launch_compact_bins(st, (const int *)active, range, (int *)slot_of_bin, (int *)bin_of_slot, counts,
+                        (int *)tfirst, (int *)tcount, ntowers, strips, 8 * ctx->sm_count, (int *)gbegin,
+                        (int *)gend, (int *)tgfirst, (int *)tgcount);
+    end_stage(ctx);
+    begin_stage(ctx, "zero_subgrids");
+    launch_zero_slots(st, (float2 *)slots, counts, pl.slots_cap, sub_cells, ctx->sm_count);
+    end_stage(ctx);
+    begin_stage(ctx, "romein");
+    if (dv.n > 0)
+        launch_romein(st, (const int4 *)rec, (const float2 *)visf, dv.n, taps, (float2 *)slots,
+                      (const int *)slot_of_bin, sub_cells, S, K, ctx->sm_count, pl.slots_cap);
+    end_stage(ctx);
+    begin_stage(ctx, "fft_rows_backward");
+    launch_fft32_rows(st, (float2 *)slots, (int64_t)pl.slots_cap * S, S, +1, tw, counts);
+    end_stage(ctx);
+    begin_stage(ctx, "tower_columns");
+    launch_tower_columns(st, (const float2 *)slots, (const int *)bin_of_slot, (const int *)gbegin,
+                         (const int *)gend, range, counts, pl.slots_cap, pl.groups_cap, (const int *)tgfirst,
+                         (const int *)tgcount, ntowers, (const double *)ph, (float2 *)partial,
+                         (float2 *)subimg, S, tw);
+    end_stage(ctx);
+    begin_stage(ctx, "fft_rows_forward");
+    launch_fft32_rows(st, (float2 *)subimg, (int64_t)ntowers * S, S, -1, tw);
+    end_stage(ctx);
+    begin_stage(ctx, "add_back");
+    launch_add_back(st, (const float2 *)subimg, (const int *)tcount, (double2 *)out_dev, N, S, M, chunk, nchunk,
+                    (flags & RG_GRID_OVERWRITE) ? 1 : 0, range, counts, pl.slots_cap, pl.groups_cap);
+    end_stage(ctx);
+    ctx->launches += 12;
+    RG_CHECK(check_launch("W-towers pass"));
+
+    // single read-back: error word, counters, counts, range
+    unsigned char host[64];
+    RG_CUDA(cudaMemcpyAsync(host, d.err, 64, cudaMemcpyDeviceToHost, st));
+    RG_CUDA(cudaStreamSynchronize(st));
+    unsigned err;
+    unsigned long long ctr[2];
+    int cnt[3], rng[3];
+    std::memcpy(&err, host, 4);
+    std::memcpy(ctr, host + 16, 16);
+    std::memcpy(cnt, host + 32, 12);
+    std::memcpy(rng, host + 48, 12);
+    pl.seen_floors = rng[1];
+    pl.seen_slots = cnt[0];
+    pl.seen_groups = cnt[1];
+    *overflow = (err & DERR_CAPACITY) || !rng[2] || cnt[0] > pl.slots_cap || cnt[1] > pl.groups_cap;
+    if (*overflow) return RG_OK;
+    if (err & DERR_NONFINITE) return fail(RG_ERR_INVALID_ARGUMENT, "non-finite u, v or w in the visibilities");
+    if (err & DERR_PLANE_RANGE)
+        return fail(RG_ERR_INVALID_ARGUMENT, "a visibility's w (or sub-cell index) falls outside the w-kernel table");
+    ctx->stats[0] = (int64_t)ctr[0];
+    ctx->stats[1] = cnt[0];
+    ctx->stats[2] = cnt[2];
+    ctx->stats[3] = rng[1];
+    ctx->stats[4] = (int64_t)ctr[1];
+    return RG_OK;
+}
+
+}  // namespace rg
+
+extern "C" {
+
 rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double theta,
                           const rg_vis *vis, const rg_wkern *wkern, int subgrid_size,
                           int subgrid_margin, double wincrement, int flags)
@@ -437,157 +582,53 @@ rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double
     const int N = grid_size;
     const int64_t cells = (int64_t)N * N;
     const int chunk = S - M;
-    const int nchunk = N / chunk + 1;
-    const int ntowers = nchunk * nchunk;
-    cudaStream_t st = ctx->stream;
+    const int ntowers = (N / chunk + 1) * (N / chunk + 1);
 
     DevVis dv;
     begin_stage(ctx, "stage_in");
     RG_CHECK(stage_vis(ctx, vis, &dv));
     float2 *taps;
     RG_CHECK(stage_taps(ctx, wkern, &taps));
-    Diag d;
-    RG_CHECK(diag_begin(ctx, &d));
     OutView ov;
     RG_CHECK(out_view(ctx, uvgrid, sizeof(double2) * (size_t)cells, "out_grid",
                       !(flags & RG_GRID_OVERWRITE), &ov));
     end_stage(ctx);
 
-    // w range -> floors (grid.c:357-367)
-    void *mm;
-    RG_CHECK(scratch(ctx, "wminmax", 16, &mm));
-    begin_stage(ctx, "w_range");
-    launch_minmax_w(st, dv.u, dv.v, dv.w, dv.n, (double *)mm, d.err);
-    end_stage(ctx);
-    ctx->launches++;
-    RG_CHECK(check_launch("w range"));
-    double wr[2];
-    unsigned err0 = 0;
-    RG_CUDA(cudaMemcpyAsync(wr, mm, 16, cudaMemcpyDeviceToHost, st));
-    RG_CUDA(cudaMemcpyAsync(&err0, d.err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-    RG_CUDA(cudaStreamSynchronize(st));
-    if (err0 & DERR_NONFINITE) return fail(RG_ERR_INVALID_ARGUMENT, "non-finite u, v or w in the visibilities");
-    const int wp_min = (int)std::floor(wr[0] / wincrement + 0.5);
-    const int wp_max = (int)std::floor(wr[1] / wincrement + 0.5);
-    const int64_t nfloor64 = (int64_t)wp_max - wp_min + 1;
-    const int64_t nbins64 = nfloor64 * ntowers;
-    if (nfloor64 > (1 << 20) || nbins64 > (int64_t)1 << 28)
-        return fail(RG_ERR_UNSUPPORTED, "too many (tower, w-floor) bins; increase wincrement");
-    const int nfloor = (int)nfloor64, nbins = (int)nbins64;
-
-    void *active, *rec, *visf, *slot_of_bin, *bin_of_slot, *nact, *tfirst, *tcount;
-    void *gbegin, *gend, *tgfirst, *tgcount;
-    RG_CHECK(scratch(ctx, "active", sizeof(int) * (size_t)nbins, &active));
-    RG_CHECK(scratch(ctx, "rec", sizeof(int4) * (size_t)dv.n, &rec));
-    RG_CHECK(scratch(ctx, "visf", sizeof(float2) * (size_t)dv.n, &visf));
-    RG_CHECK(scratch(ctx, "slot_of_bin", sizeof(int) * (size_t)nbins, &slot_of_bin));
-    RG_CHECK(scratch(ctx, "bin_of_slot", sizeof(int) * (size_t)nbins, &bin_of_slot));
-    RG_CHECK(scratch(ctx, "n_active", 16, &nact));
-    RG_CHECK(scratch(ctx, "tower_first", sizeof(int) * (size_t)ntowers, &tfirst));
-    RG_CHECK(scratch(ctx, "tower_count", sizeof(int) * (size_t)ntowers, &tcount));
-    RG_CHECK(scratch(ctx, "group_begin", sizeof(int) * (size_t)nbins, &gbegin));
-    RG_CHECK(scratch(ctx, "group_end", sizeof(int) * (size_t)nbins, &gend));
-    RG_CHECK(scratch(ctx, "tower_group_first", sizeof(int) * (size_t)ntowers, &tgfirst));
-    RG_CHECK(scratch(ctx, "tower_group_count", sizeof(int) * (size_t)ntowers, &tgcount));
-    RG_CUDA(cudaMemsetAsync(active, 0, sizeof(int) * (size_t)nbins, st));
-
-    TowerGeom g;
-    g.grid_size = N;
-    g.subgrid = S;
-    g.margin = M;
-    g.chunk = chunk;
-    g.nchunk = nchunk;
-    g.ksize = K;
-    g.ov = wkern->oversampling;
-    g.planes = wkern->plane_count;
-    g.theta = theta;
-    g.winc = wincrement;
-    g.wk_wmin = wkern->w_min;
-    g.wk_wstep = wkern->w_step;
-    begin_stage(ctx, "prepare");
-    if (dv.n > 0) {
-        launch_prepare_towers(st, dv.u, dv.v, dv.w, dv.vis, dv.n, g, wp_min, nfloor, (int4 *)rec,
-                              (float2 *)visf, (int *)active, d.err, d.counters);
-        ctx->launches++;
+    char keybuf[200];
+    std::snprintf(keybuf, sizeof(keybuf), "%d_%d_%d_%.17g_%.17g_%lld", N, S, M, theta, wincrement,
+                  (long long)dv.n);
+    TowerPlan &pl = ctx->tower_plans[keybuf];
+    if (!pl.valid) {  // first call for this shape: generous capacities, learn the real sizes
+        pl.floors_cap = 256;
+        pl.slots_cap = ntowers * 16 + 64;
+        pl.groups_cap = pl.slots_cap;
+        pl.valid = true;
     }
-    end_stage(ctx);
-    const int strips = fft32_strips(S);
-    begin_stage(ctx, "compact");
-    launch_compact_bins(st, (const int *)active, nbins, nfloor, (int *)slot_of_bin, (int *)bin_of_slot,
-                        (int *)nact, (int *)tfirst, (int *)tcount, ntowers, strips,
-                        8 * ctx->sm_count, (int *)gbegin, (int *)gend, (int *)tgfirst, (int *)tgcount);
-    end_stage(ctx);
-    ctx->launches++;
-    RG_CHECK(check_launch("tower binning"));
-    int counts_h[2] = {0, 0};
-    RG_CUDA(cudaMemcpyAsync(counts_h, nact, sizeof(counts_h), cudaMemcpyDeviceToHost, st));
-    RG_CUDA(cudaStreamSynchronize(st));
-    const int n_active = counts_h[0], n_groups = counts_h[1];
-
-    const int64_t sub_cells = (int64_t)S * S;
-    void *slots = nullptr, *subimg = nullptr, *ph = nullptr;
-    float2 *tw;
-    RG_CHECK(get_twiddles32(ctx, S, &tw));
-    RG_CHECK(scratch(ctx, "subimg", sizeof(float2) * (size_t)(sub_cells * ntowers), &subimg));
-    // Fresnel phase table, cached per (S, theta, winc)
-    {
-        char key[160];
-        std::snprintf(key, sizeof(key), "ph_%d_%.17g_%.17g", S, theta, wincrement);
-        bool fresh = ctx->scratch.find(key) == ctx->scratch.end();
-        RG_CHECK(scratch(ctx, key, sizeof(double) * (size_t)sub_cells, &ph));
-        if (fresh) {
-            launch_fresnel_table(st, (double *)ph, S, theta, wincrement);
-            ctx->launches++;
-        }
+    // A pass whose capacities overflow writes nothing to the grid (the add-back
+    // checks the live counts), so it can simply be rerun with larger ones.
+    for (int attempt = 0; attempt < 4; attempt++) {
+        bool overflow = false;
+        RG_CHECK(wtowers_pass(ctx, dv, taps, wkern, (double *)ov.dev, N, theta, S, M, wincrement, flags, pl,
+                              &overflow));
+        if (!overflow) break;
+        if (attempt == 3) return fail(RG_ERR_UNSUPPORTED, "W-towers capacities could not be sized");
+        if (pl.seen_floors > (1 << 20) || (int64_t)pl.seen_floors * ntowers > ((int64_t)1 << 28))
+            return fail(RG_ERR_UNSUPPORTED, "too many (tower, w-floor) bins; increase wincrement");
+        pl.floors_cap = pl.seen_floors > pl.floors_cap ? pl.seen_floors + 8 : pl.floors_cap;
+        pl.slots_cap = pl.seen_slots > pl.slots_cap ? pl.seen_slots + pl.seen_slots / 8 + 8 : pl.slots_cap;
+        pl.groups_cap = pl.seen_groups > pl.groups_cap ? pl.seen_groups + pl.seen_groups / 8 + 8 : pl.groups_cap;
+        begin_call(ctx);
     }
-    if (n_active > 0) {
-        RG_CHECK(scratch(ctx, "slots", sizeof(float2) * (size_t)(sub_cells * n_active), &slots));
-        begin_stage(ctx, "zero_subgrids");
-        RG_CUDA(cudaMemsetAsync(slots, 0, sizeof(float2) * (size_t)(sub_cells * n_active), st));
-        end_stage(ctx);
-        begin_stage(ctx, "romein");
-        launch_romein(st, (const int4 *)rec, (const float2 *)visf, dv.n, taps, (float2 *)slots,
-                      (const int *)slot_of_bin, sub_cells, S, K, ctx->sm_count);
-        end_stage(ctx);
-        begin_stage(ctx, "fft_rows_backward");
-        launch_fft32_rows(st, (float2 *)slots, (int64_t)n_active * S, S, +1, tw);
-        end_stage(ctx);
-        void *partial;
-        RG_CHECK(scratch(ctx, "partial", sizeof(float2) * (size_t)(sub_cells * (n_groups > 0 ? n_groups : 1)),
-                         &partial));
-        begin_stage(ctx, "tower_columns");
-        launch_tower_columns(st, (const float2 *)slots, (const int *)bin_of_slot, (const int *)gbegin,
-                             (const int *)gend, n_groups, (const int *)tgfirst, (const int *)tgcount,
-                             ntowers, nfloor, wp_min, (const double *)ph, (float2 *)partial,
-                             (float2 *)subimg, S, tw);
-        end_stage(ctx);
-        begin_stage(ctx, "fft_rows_forward");
-        launch_fft32_rows(st, (float2 *)subimg, (int64_t)ntowers * S, S, -1, tw);
-        end_stage(ctx);
-        ctx->launches += 5;
-        RG_CHECK(check_launch("tower gridding / transforms"));
+    // shrink a first-call guess to the sizes seen (keeps memory proportional)
+    if (pl.slots_cap > pl.seen_slots + pl.seen_slots / 4 + 64) {
+        pl.slots_cap = pl.seen_slots + pl.seen_slots / 8 + 8;
+        pl.groups_cap = pl.seen_groups + pl.seen_groups / 8 + 8;
     }
-    begin_stage(ctx, "add_back");
-    launch_add_back(st, (const float2 *)subimg, (const int *)tcount, (double2 *)ov.dev, N, S, M, chunk,
-                    nchunk, (flags & RG_GRID_OVERWRITE) ? 1 : 0);
-    end_stage(ctx);
-    ctx->launches++;
-    RG_CHECK(check_launch("add-back"));
     begin_stage(ctx, "stage_out");
     RG_CHECK(finish_out(ctx, ov));
     end_stage(ctx);
-    unsigned long long counters[2] = {0, 0};
-    RG_CHECK(diag_end(ctx, d, counters));
+    RG_CUDA(cudaStreamSynchronize(ctx->stream));
     collect_timings(ctx);
-    std::vector<int> tc(ntowers);
-    RG_CUDA(cudaMemcpy(tc.data(), tcount, sizeof(int) * ntowers, cudaMemcpyDeviceToHost));
-    int with_data = 0;
-    for (int c : tc) with_data += c > 0;
-    ctx->stats[0] = (int64_t)counters[0];
-    ctx->stats[1] = n_active;
-    ctx->stats[2] = with_data;
-    ctx->stats[3] = nfloor;
-    ctx->stats[4] = (int64_t)counters[1];
     ctx->stats[5] = ctx->launches;
     return RG_OK;
 }

@@ -65,6 +65,12 @@ void launch_learned_wproj(cudaStream_t s, const double *u, const double *v, cons
 
 }  // namespace rg
 
+struct TowerPlan {
+    bool valid = false;
+    int floors_cap = 0, slots_cap = 0, groups_cap = 0;
+    int seen_floors = 0, seen_slots = 0, seen_groups = 0;
+};
+
 struct rg_stage_event {
     std::string name;
     cudaEvent_t start = nullptr, stop = nullptr;
@@ -76,6 +82,7 @@ struct rg_context {
     std::vector<rg_stage_event> events;  // pool, reused across calls
     int n_events = 0;                    // used by the current call
     std::vector<std::pair<std::string, float>> timings;  // last call
+    std::map<std::string, TowerPlan> tower_plans;         // capacities per W-towers shape
     int sm_count = 148;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
@@ -126,7 +133,7 @@ bool fft32_supported(int n);
 void fft32_init_twiddles(cudaStream_t s, float2 *tw, int n);  // tw: n entries
 // batched row transforms: rows = count of rows of length n (contiguous)
 void launch_fft32_rows(cudaStream_t s, float2 *data, int64_t rows, int n, int sign,
-                       const float2 *tw);
+                       const float2 *tw, const int *count_dev = nullptr);
 // column transforms of `batch` n x n arrays
 void launch_fft32_cols(cudaStream_t s, float2 *data, int batch, int n, int sign,
                        const float2 *tw);
@@ -142,40 +149,52 @@ struct TowerGeom {
 };
 void launch_minmax_w(cudaStream_t s, const double *u, const double *v, const double *w,
                      int64_t n, double *out4, unsigned *err);
+// range[0] = wp_min, range[1] = nfloor, range[2] = 1 if nfloor <= floors_cap
+// (grid.c:357-367 from the reduced w range)
+void launch_w_floors(cudaStream_t s, const double *wrange, double winc, int floors_cap, int *range,
+                     unsigned *err);
 void launch_prepare_towers(cudaStream_t s, const double *u, const double *v, const double *w,
-                           const double2 *vis, int64_t n, TowerGeom g, int wp_min, int nfloor,
+                           const double2 *vis, int64_t n, TowerGeom g, const int *range,
                            int4 *rec, float2 *visf, int *active, unsigned *err,
                            unsigned long long *counters);
+void launch_zero_slots(cudaStream_t s, float2 *slots, const int *counts, int slot_cap,
+                       int64_t slot_elems, int sm_count);
 void launch_prepare_wproj(cudaStream_t s, const double *u, const double *v, const double *w,
                           const double2 *vis, int64_t n, int grid_size, double theta,
                           int ksize, int ov, int planes, double wk_wmin, double wk_wstep,
                           int4 *rec, float2 *visf, unsigned *err);
 // counts[0] = active slots, counts[1] = floor groups (target_items: aim for
 // about this many (group, strip) work items in the column stage)
-void launch_compact_bins(cudaStream_t s, const int *active, int nbins, int nfloor, int *slot_of_bin,
+void launch_compact_bins(cudaStream_t s, const int *active, const int *range, int *slot_of_bin,
                          int *bin_of_slot, int *counts, int *tower_first, int *tower_count,
                          int ntowers, int strips, int target_items, int *group_begin,
                          int *group_end, int *tower_group_first, int *tower_group_count);
 
 // k_romein.cu
+// Sub-grids with slot index >= slot_cap are skipped (capacity overflow: the
+// caller detects it from the slot count and reruns).
 void launch_romein(cudaStream_t s, const int4 *rec, const float2 *visf, int64_t n,
                    const float2 *taps, float2 *grids, const int *slot_of_bin,
-                   int64_t grid_stride, int grid_side, int ksize, int sm_count);
+                   int64_t grid_stride, int grid_side, int ksize, int sm_count, int slot_cap = 1);
 
 // k_towers.cu
 void launch_fresnel_table(cudaStream_t s, double *ph, int subgrid, double theta, double winc);
 // Column stage in floor groups: group g covers active slots
 // [group_begin[g], group_end[g]) of one tower; partial holds one sub-grid per
 // group; tower t's groups are [tower_group_first[t], +tower_group_count[t]).
+// range = {wp_min, nfloor, ok} and counts = {slots, groups, towers} live on the
+// device; launches are sized by the capacities.
 void launch_tower_columns(cudaStream_t s, const float2 *slots, const int *bin_of_slot,
-                          const int *group_begin, const int *group_end, int ngroups,
+                          const int *group_begin, const int *group_end, const int *range,
+                          const int *counts, int slot_cap, int group_cap,
                           const int *tower_group_first, const int *tower_group_count, int ntowers,
-                          int nfloor, int wp_min, const double *ph, float2 *partial, float2 *subimg,
-                          int subgrid, const float2 *tw);
+                          const double *ph, float2 *partial, float2 *subimg, int subgrid,
+                          const float2 *tw);
 int fft32_strips(int n);  // column strips per sub-grid in the column kernels
 void launch_add_back(cudaStream_t s, const float2 *subimg, const int *tower_count,
                      double2 *master, int grid_size, int subgrid, int margin, int chunk,
-                     int nchunk, int overwrite);
+                     int nchunk, int overwrite, const int *range, const int *counts, int slot_cap,
+                     int group_cap);
 
 // k_dft.cu
 void launch_dft(cudaStream_t s, const double *u, const double *v, const double *w,
