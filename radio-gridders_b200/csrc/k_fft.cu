@@ -108,14 +108,16 @@ template <int N1, int CW = (N1 >= 32 ? 8 : 16)>
 struct ColGeom {
     static constexpr int N = N1 * 32;
     static constexpr int C = CW;                            // strip width
-    static constexpr int CS = N1 * kPad + 1;                // per-column stride in T
+    // per-column stride in T: N1*kPad + 16/C makes the 64-bit exchange accesses
+    // of a half-warp (C columns x 16/C rows) hit distinct banks
+    static constexpr int CS = N1 * kPad + 16 / CW;
     static constexpr int T_ELEMS = C * CS;
     static constexpr int LB = ilog2c(N1);
 };
 
 // Step 1 of a column transform: load from `src` (row stride `ld`, column c of
 // the strip at src[row*ld + c]), 32-point transforms, twiddle, into T.
-template <int N1, int SIGN, int CW = ColGeom<N1>::C>
+template <int N1, int SIGN, int CW = ColGeom<N1>::C, bool CLEAR = false>
 __device__ __forceinline__ void col_step1(const float2 *__restrict__ src, int ld, float2 *T,
                                           const float2 *W)
 {
@@ -125,6 +127,11 @@ __device__ __forceinline__ void col_step1(const float2 *__restrict__ src, int ld
         float2 a[32];
 #pragma unroll
         for (int n2 = 0; n2 < 32; n2++) a[n2] = src[(int64_t)(n1 + n2 * N1) * ld + c];
+        if (CLEAR) {  // leave the sub-grid zeroed for the next gridding pass
+            float2 *dst = const_cast<float2 *>(src);
+#pragma unroll
+            for (int n2 = 0; n2 < 32; n2++) dst[(int64_t)(n1 + n2 * N1) * ld + c] = make_float2(0.f, 0.f);
+        }
         reg_fft<32, SIGN>(a);
 #pragma unroll
         for (int j = 0; j < 32; j++) {
@@ -183,7 +190,7 @@ using PartialGeom = ColGeom<N1, 8>;
 
 template <int N1>
 __global__ void __launch_bounds__(kPartialThreads) tower_partial_kernel(
-    const float2 *__restrict__ slots, const int *__restrict__ bin_of_slot,
+    float2 *__restrict__ slots, const int *__restrict__ bin_of_slot,
     const int *__restrict__ group_begin, const int *__restrict__ group_end,
     const int *__restrict__ range, const int *__restrict__ counts, int slot_cap,
     const double *__restrict__ ph, float2 *__restrict__ partial, const float2 *__restrict__ tw)
@@ -216,7 +223,7 @@ __global__ void __launch_bounds__(kPartialThreads) tower_partial_kernel(
     for (int slot = begin; slot < end; slot++) {
         const double mwp = -(double)(wp_min + bin_of_slot[slot] % nfloor);
         const float2 *base = slots + (int64_t)slot * N * N + strip * C;
-        col_step1<N1, +1, C>(base, N, T, W);
+        col_step1<N1, +1, C, true>(base, N, T, W);
         __syncthreads();
 #pragma unroll
         for (int q = 0; q < PER; q++) {
@@ -343,7 +350,7 @@ static void cols_impl(cudaStream_t s, float2 *data, int batch, int sign, const f
 }
 
 template <int N1>
-static void tower_impl(cudaStream_t s, const float2 *slots, const int *bin_of_slot,
+static void tower_impl(cudaStream_t s, float2 *slots, const int *bin_of_slot,
                        const int *group_begin, const int *group_end, const int *range,
                        const int *counts, int slot_cap, int group_cap,
                        const int *tower_group_first, const int *tower_group_count, int ntowers,
@@ -387,7 +394,7 @@ void launch_fft32_cols(cudaStream_t s, float2 *data, int batch, int n, int sign,
 #undef CALL
 }
 
-void launch_tower_columns(cudaStream_t s, const float2 *slots, const int *bin_of_slot,
+void launch_tower_columns(cudaStream_t s, float2 *slots, const int *bin_of_slot,
                           const int *group_begin, const int *group_end, const int *range,
                           const int *counts, int slot_cap, int group_cap,
                           const int *tower_group_first, const int *tower_group_count, int ntowers,

@@ -25,64 +25,90 @@
 
 namespace rg {
 
-template <int K>
-__global__ void __launch_bounds__(K *K) romein_kernel(
+// P grid points per thread: thread (myU, myV0) owns the points of column
+// residue myU and row residues myV0 + j*K/P, j < P, so a visibility's record is
+// decoded once for P taps.
+template <int K, int P>
+__global__ void __launch_bounds__(K *K / P) romein_kernel(
     const int4 *__restrict__ rec, const float2 *__restrict__ visf, int64_t n,
     const float2 *__restrict__ taps, float2 *__restrict__ grids,
     const int *__restrict__ slot_of_bin, int64_t grid_stride, int side, int64_t chunk, int slot_cap)
 {
-    constexpr int BATCH = K * K;
+    constexpr int NT = K * K / P;     // threads
+    constexpr int BATCH = 256;        // visibilities staged per round
+    constexpr int RS = K / P;         // row stride between a thread's points
     __shared__ int4 srec[BATCH];
     __shared__ float2 svis[BATCH];
-    const int myU = threadIdx.x % K, myV = threadIdx.x / K;
+    const int myU = threadIdx.x % K, myV0 = threadIdx.x / K;
     const int limit = side * side;
 
     for (int64_t c0 = (int64_t)blockIdx.x * chunk; c0 < n; c0 += (int64_t)gridDim.x * chunk) {
         const int64_t c1 = c0 + chunk < n ? c0 + chunk : n;
-        int cur_bin = -1, cur_idx = 0;
-        float2 sum = make_float2(0.f, 0.f);
+        int cur_bin = -1;
+        int cur_idx[P];
+        float2 sum[P];
+#pragma unroll
+        for (int p = 0; p < P; p++) {
+            cur_idx[p] = 0;
+            sum[p] = make_float2(0.f, 0.f);
+        }
         for (int64_t b0 = c0; b0 < c1; b0 += BATCH) {
             const int cnt = (int)(c1 - b0 < BATCH ? c1 - b0 : BATCH);
             __syncthreads();
-            if ((int)threadIdx.x < cnt) {
-                srec[threadIdx.x] = rec[b0 + threadIdx.x];
-                svis[threadIdx.x] = visf[b0 + threadIdx.x];
+            for (int j = threadIdx.x; j < cnt; j += NT) {
+                srec[j] = rec[b0 + j];
+                svis[j] = visf[b0 + j];
             }
             __syncthreads();
-            // software pipeline: the tap of visibility j+1 is loaded before j is used
-            int4 r = srec[0];
-            int cu = (myU - (r.w & 0xff)) & (K - 1);
-            int cv = (myV - (r.w >> 8)) & (K - 1);
-            float2 t = r.x >= 0 ? __ldg(taps + r.z + cv * K + cu) : make_float2(0.f, 0.f);
             for (int j = 0; j < cnt; j++) {
-                const int4 rn = srec[j + 1 < cnt ? j + 1 : j];
-                const int cun = (myU - (rn.w & 0xff)) & (K - 1);
-                const int cvn = (myV - (rn.w >> 8)) & (K - 1);
-                const float2 tn = rn.x >= 0 ? __ldg(taps + rn.z + cvn * K + cun) : make_float2(0.f, 0.f);
-                if (r.x >= 0) {
-                    const int idx = r.y + cv * side + cu;
-                    if (r.x != cur_bin || idx != cur_idx) {
-                        if (cur_bin >= 0 && (unsigned)cur_idx < (unsigned)limit) {
-                            const int slot = slot_of_bin[cur_bin];
-                            if (slot < slot_cap) atomicAdd(grids + (int64_t)slot * grid_stride + cur_idx, sum);
-                        }
-                        cur_bin = r.x;
-                        cur_idx = idx;
-                        sum = make_float2(0.f, 0.f);
-                    }
-                    const float2 vz = svis[j];
-                    sum.x = fmaf(vz.x, t.x, fmaf(vz.y, t.y, sum.x));
-                    sum.y = fmaf(vz.y, t.x, fmaf(-vz.x, t.y, sum.y));
+                const int4 r = srec[j];
+                if (r.x < 0) continue;
+                const int cu = (myU - (r.w & 0xff)) & (K - 1);
+                const int r0 = r.w >> 8;
+                float2 t[P];
+                int idx[P];
+#pragma unroll
+                for (int p = 0; p < P; p++) {
+                    const int cv = (myV0 + p * RS - r0) & (K - 1);
+                    idx[p] = r.y + cv * side + cu;
+                    t[p] = __ldg(taps + r.z + cv * K + cu);
                 }
-                r = rn;
-                cu = cun;
-                cv = cvn;
-                t = tn;
+                const float2 vz = svis[j];
+                if (r.x != cur_bin) {
+#pragma unroll
+                    for (int p = 0; p < P; p++) {
+                        if (cur_bin >= 0 && (unsigned)cur_idx[p] < (unsigned)limit) {
+                            const int slot = slot_of_bin[cur_bin];
+                            if (slot < slot_cap)
+                                atomicAdd(grids + (int64_t)slot * grid_stride + cur_idx[p], sum[p]);
+                        }
+                        cur_idx[p] = idx[p];
+                        sum[p] = make_float2(0.f, 0.f);
+                    }
+                    cur_bin = r.x;
+                }
+#pragma unroll
+                for (int p = 0; p < P; p++) {
+                    if (idx[p] != cur_idx[p]) {
+                        if ((unsigned)cur_idx[p] < (unsigned)limit) {
+                            const int slot = slot_of_bin[cur_bin];
+                            if (slot < slot_cap)
+                                atomicAdd(grids + (int64_t)slot * grid_stride + cur_idx[p], sum[p]);
+                        }
+                        cur_idx[p] = idx[p];
+                        sum[p] = make_float2(0.f, 0.f);
+                    }
+                    sum[p].x = fmaf(vz.x, t[p].x, fmaf(vz.y, t[p].y, sum[p].x));
+                    sum[p].y = fmaf(vz.y, t[p].x, fmaf(-vz.x, t[p].y, sum[p].y));
+                }
             }
         }
-        if (cur_bin >= 0 && (unsigned)cur_idx < (unsigned)limit) {
+        if (cur_bin >= 0) {
             const int slot = slot_of_bin[cur_bin];
-            if (slot < slot_cap) atomicAdd(grids + (int64_t)slot * grid_stride + cur_idx, sum);
+#pragma unroll
+            for (int p = 0; p < P; p++)
+                if ((unsigned)cur_idx[p] < (unsigned)limit && slot < slot_cap)
+                    atomicAdd(grids + (int64_t)slot * grid_stride + cur_idx[p], sum[p]);
         }
     }
 }
@@ -93,25 +119,26 @@ void launch_romein(cudaStream_t s, const int4 *rec, const float2 *visf, int64_t 
 {
     const int64_t chunk = 1024;
     int64_t blocks = (n + chunk - 1) / chunk;
-    const int64_t cap = (int64_t)sm_count * 8;
+    const int64_t cap = (int64_t)sm_count * 16;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
+    const unsigned nb = (unsigned)blocks;
     switch (ksize) {
         case 4:
-            romein_kernel<4><<<(unsigned)blocks, 16, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin,
-                                                             grid_stride, grid_side, chunk, slot_cap);
+            romein_kernel<4, 1><<<nb, 16, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin, grid_stride, grid_side,
+                                                  chunk, slot_cap);
             break;
         case 8:
-            romein_kernel<8><<<(unsigned)blocks, 64, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin,
-                                                             grid_stride, grid_side, chunk, slot_cap);
+            romein_kernel<8, 2><<<nb, 32, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin, grid_stride, grid_side,
+                                                  chunk, slot_cap);
             break;
         case 16:
-            romein_kernel<16><<<(unsigned)blocks, 256, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin,
-                                                               grid_stride, grid_side, chunk, slot_cap);
+            romein_kernel<16, 4><<<nb, 64, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin, grid_stride,
+                                                   grid_side, chunk, slot_cap);
             break;
         case 32:
-            romein_kernel<32><<<(unsigned)blocks, 1024, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin,
-                                                                grid_stride, grid_side, chunk, slot_cap);
+            romein_kernel<32, 4><<<nb, 256, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin, grid_stride,
+                                                    grid_side, chunk, slot_cap);
             break;
         default: break;
     }

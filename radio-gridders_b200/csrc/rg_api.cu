@@ -472,6 +472,10 @@ static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *t
         }
     }
     RG_CUDA(cudaMemsetAsync(active, 0, sizeof(int) * (size_t)nbins_cap, st));
+    if (ctx->slots_owner != &pl) {  // the slot buffer was last used by another shape
+        pl.zeroed_slots = 0;
+        ctx->slots_owner = &pl;
+    }
 
     TowerGeom g;
     g.grid_size = N;
@@ -502,9 +506,14 @@ static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *t
                         (int *)tfirst, (int *)tcount, ntowers, strips, 8 * ctx->sm_count, (int *)gbegin,
                         (int *)gend, (int *)tgfirst, (int *)tgcount);
     end_stage(ctx);
-    begin_stage(ctx, "zero_subgrids");
-    launch_zero_slots(st, (float2 *)slots, counts, pl.slots_cap, sub_cells, ctx->sm_count);
-    end_stage(ctx);
+    // Sub-grids are left zeroed by the previous pass's column stage; only
+    // memory never cleared (new capacity, or after an overflowed pass) is zeroed.
+    if (pl.zeroed_slots < (size_t)pl.slots_cap) {
+        begin_stage(ctx, "zero_subgrids");
+        RG_CUDA(cudaMemsetAsync(slots, 0, sizeof(float2) * (size_t)(sub_cells * pl.slots_cap), st));
+        end_stage(ctx);
+        pl.zeroed_slots = (size_t)pl.slots_cap;
+    }
     begin_stage(ctx, "romein");
     if (dv.n > 0)
         launch_romein(st, (const int4 *)rec, (const float2 *)visf, dv.n, taps, (float2 *)slots,
@@ -514,7 +523,7 @@ static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *t
     launch_fft32_rows(st, (float2 *)slots, (int64_t)pl.slots_cap * S, S, +1, tw, counts);
     end_stage(ctx);
     begin_stage(ctx, "tower_columns");
-    launch_tower_columns(st, (const float2 *)slots, (const int *)bin_of_slot, (const int *)gbegin,
+    launch_tower_columns(st, (float2 *)slots, (const int *)bin_of_slot, (const int *)gbegin,
                          (const int *)gend, range, counts, pl.slots_cap, pl.groups_cap, (const int *)tgfirst,
                          (const int *)tgcount, ntowers, (const double *)ph, (float2 *)partial,
                          (float2 *)subimg, S, tw);
@@ -544,7 +553,10 @@ static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *t
     pl.seen_slots = cnt[0];
     pl.seen_groups = cnt[1];
     *overflow = (err & DERR_CAPACITY) || !rng[2] || cnt[0] > pl.slots_cap || cnt[1] > pl.groups_cap;
-    if (*overflow) return RG_OK;
+    if (*overflow) {
+        pl.zeroed_slots = 0;  // some sub-grids may not have been consumed (cleared)
+        return RG_OK;
+    }
     if (err & DERR_NONFINITE) return fail(RG_ERR_INVALID_ARGUMENT, "non-finite u, v or w in the visibilities");
     if (err & DERR_PLANE_RANGE)
         return fail(RG_ERR_INVALID_ARGUMENT, "a visibility's w (or sub-cell index) falls outside the w-kernel table");

@@ -69,6 +69,7 @@ struct TowerPlan {
     bool valid = false;
     int floors_cap = 0, slots_cap = 0, groups_cap = 0;
     int seen_floors = 0, seen_slots = 0, seen_groups = 0;
+    size_t zeroed_slots = 0;  // sub-grids known to be zero (cleared on consumption)
 };
 
 struct rg_stage_event {
@@ -83,6 +84,7 @@ struct rg_context {
     int n_events = 0;                    // used by the current call
     std::vector<std::pair<std::string, float>> timings;  // last call
     std::map<std::string, TowerPlan> tower_plans;         // capacities per W-towers shape
+    const TowerPlan *slots_owner = nullptr;               // plan whose pass last used "slots"
     int sm_count = 148;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
@@ -184,7 +186,10 @@ void launch_fresnel_table(cudaStream_t s, double *ph, int subgrid, double theta,
 // group; tower t's groups are [tower_group_first[t], +tower_group_count[t]).
 // range = {wp_min, nfloor, ok} and counts = {slots, groups, towers} live on the
 // device; launches are sized by the capacities.
-void launch_tower_columns(cudaStream_t s, const float2 *slots, const int *bin_of_slot,
+// The column stage reads every live sub-grid once and leaves it zeroed (the
+// reference clears its sub-grid after each floor, grid.c:473-481), so the
+// next gridding pass needs no separate clear.
+void launch_tower_columns(cudaStream_t s, float2 *slots, const int *bin_of_slot,
                           const int *group_begin, const int *group_end, const int *range,
                           const int *counts, int slot_cap, int group_cap,
                           const int *tower_group_first, const int *tower_group_count, int ntowers,
