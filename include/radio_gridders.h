@@ -175,6 +175,52 @@ rg_status rg_fft2d(rg_context *ctx, void *data, int batch, int ny, int nx, int s
 rg_status rg_dft_image(rg_context *ctx, double *image_out, int grid_size, double theta,
                        const rg_vis *vis, int precision, double factor);
 
+/* ---- crocodile HDF5 files ------------------------------------------------- */
+
+/* Flat visibilities read from a file; arrays owned by the struct, released
+ * with rg_free_vis_data. */
+typedef struct rg_vis_data {
+    double *u, *v, *w, *vis; /* vis: 2*n doubles */
+    int64_t n;
+    int64_t bl_count;
+} rg_vis_data;
+
+/* Replaces load_vis + flatten_visibilities_CUDA (src/reference/hdf5.c:173-318,
+ * src/common/hdf5.c:827-872): reads the hierarchical /vis/<a1>/<a2>/... or the
+ * legacy flat /vis layout, keeps baselines whose first uvw sample has length
+ * in [bl_min, bl_max) metres, and flattens to u, v, w in wavelengths in
+ * baseline/time/frequency order.  Project-written HDF5 reader (superblock
+ * 0/1, symbol-table groups, contiguous datasets); RG_ERR_IO otherwise. */
+rg_status rg_read_vis_hdf5(const char *path, double bl_min, double bl_max, rg_vis_data *out);
+void rg_free_vis_data(rg_vis_data *d);
+
+/* An oversampled w-kernel table read from a file (rg_wkern layout). */
+typedef struct rg_wkern_data {
+    double *data;
+    int plane_count, size, oversampling;
+    double w_min, w_step;
+} rg_wkern_data;
+
+/* Replaces load_wkern (src/reference/hdf5.c:321-413): group wkern/<theta %g>,
+ * one child per w plane, planes re-indexed nearest to w_min + i*w_step. */
+rg_status rg_read_wkern_hdf5(const char *path, double theta, rg_wkern_data *out);
+void rg_free_wkern_data(rg_wkern_data *d);
+
+/* Writers of the same layouts (hierarchical visibilities: time [bl][time],
+ * uvw [bl][time][3] metres, freq [bl][nf] Hz, vis [bl][time][nf] complex
+ * interleaved; one /vis/<ant1>/<ant2> group per baseline). */
+rg_status rg_write_vis_hdf5(const char *path, int n_bl, int n_time, int n_freq, const int *ant1,
+                            const int *ant2, const double *time, const double *freq,
+                            const double *uvw, const double *vis);
+rg_status rg_write_wkern_hdf5(const char *path, double theta, const rg_wkern *wk);
+/* Generic access used for other crocodile files (e.g. the separable kernels
+ * of src/common/hdf5.c:372-500): a float64 / int64 / {r, i} dataset by path
+ * (out may be NULL to query dims; up to 8 dims; a compound element adds a
+ * trailing axis of its member count), and a numeric attribute. */
+rg_status rg_hdf5_read_f64(const char *path, const char *dataset, double *out, int64_t capacity,
+                           int64_t *dims, int *ndims);
+rg_status rg_hdf5_attr_f64(const char *path, const char *object, const char *name, double *out);
+
 /* ---- learned w-kernel ---------------------------------------------------- */
 
 /* A small MLP that returns the tap of the w-kernel for a continuous (w, du, dv)

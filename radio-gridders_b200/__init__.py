@@ -41,7 +41,9 @@ EXPORTS = [
     "rg_make_hermitian", "rg_fft_shift", "rg_image_from_grid", "rg_fft2d", "rg_dft_image",
     "rg_grid_wprojection_noalloc", "rg_mlp_param_count", "rg_mlp_create", "rg_mlp_destroy",
     "rg_mlp_set_params", "rg_mlp_get_params", "rg_mlp_gradient", "rg_mlp_train", "rg_mlp_eval",
-    "rg_grid_wprojection_learned",
+    "rg_grid_wprojection_learned", "rg_read_vis_hdf5", "rg_free_vis_data", "rg_read_wkern_hdf5",
+    "rg_free_wkern_data", "rg_write_vis_hdf5", "rg_write_wkern_hdf5", "rg_hdf5_read_f64",
+    "rg_hdf5_attr_f64",
 ]
 
 
@@ -63,6 +65,17 @@ class _Vis(ct.Structure):
 
 class _WKern(ct.Structure):
     _fields_ = [("data", ct.c_void_p), ("plane_count", ct.c_int), ("size", ct.c_int),
+                ("oversampling", ct.c_int), ("w_min", ct.c_double), ("w_step", ct.c_double)]
+
+
+class _VisData(ct.Structure):
+    _fields_ = [("u", ct.POINTER(ct.c_double)), ("v", ct.POINTER(ct.c_double)),
+                ("w", ct.POINTER(ct.c_double)), ("vis", ct.POINTER(ct.c_double)),
+                ("n", ct.c_int64), ("bl_count", ct.c_int64)]
+
+
+class _WKernData(ct.Structure):
+    _fields_ = [("data", ct.POINTER(ct.c_double)), ("plane_count", ct.c_int), ("size", ct.c_int),
                 ("oversampling", ct.c_int), ("w_min", ct.c_double), ("w_step", ct.c_double)]
 
 
@@ -104,6 +117,16 @@ def lib():
         L.rg_mlp_train.argtypes = [vp, vp, vp, vp, i64, i, i, ct.c_float, vp]
         L.rg_mlp_eval.argtypes = [vp, vp, vp, i64, vp]
         L.rg_grid_wprojection_learned.argtypes = [vp, vp, vp, i, d, ct.POINTER(_Vis), i]
+        L.rg_read_vis_hdf5.argtypes = [ct.c_char_p, d, d, ct.POINTER(_VisData)]
+        L.rg_free_vis_data.argtypes = [ct.POINTER(_VisData)]
+        L.rg_free_vis_data.restype = None
+        L.rg_read_wkern_hdf5.argtypes = [ct.c_char_p, d, ct.POINTER(_WKernData)]
+        L.rg_free_wkern_data.argtypes = [ct.POINTER(_WKernData)]
+        L.rg_free_wkern_data.restype = None
+        L.rg_write_vis_hdf5.argtypes = [ct.c_char_p, i, i, i, vp, vp, vp, vp, vp, vp]
+        L.rg_write_wkern_hdf5.argtypes = [ct.c_char_p, d, ct.POINTER(_WKern)]
+        L.rg_hdf5_read_f64.argtypes = [ct.c_char_p, ct.c_char_p, vp, i64, ct.POINTER(i64), ct.POINTER(i)]
+        L.rg_hdf5_attr_f64.argtypes = [ct.c_char_p, ct.c_char_p, ct.c_char_p, ct.POINTER(d)]
         for name in EXPORTS:
             getattr(L, name)  # raises AttributeError if a declared symbol is missing
         _lib = L
@@ -376,3 +399,85 @@ def image_from_grid(uvgrid, taper_1d=None):
 
 def dft_image(grid_size, theta, vis, precision=RG_DFT_FP64_REDUCED, factor=2.0):
     return default_context().dft_image(grid_size, theta, vis, precision, factor)
+
+
+# Crocodile HDF5 files (host only: no device is touched) ----------------------
+
+class FileWKernel:
+    """An oversampled w-kernel table read from a file: data complex128
+    [planes, ov, ov, size, size], planes at w_min + i*w_step."""
+
+    def __init__(self, data, w_min, w_step):
+        self.data, self.w_min, self.w_step = data, w_min, w_step
+
+    @property
+    def w_max(self):
+        return self.w_min + (self.data.shape[0] - 1) * self.w_step
+
+
+def read_vis_hdf5(path, bl_min=0.0, bl_max=float("inf")):
+    """Flat visibilities of a crocodile visibility file (load_vis +
+    flatten_visibilities_CUDA, src/reference/hdf5.c:173-318,
+    src/common/hdf5.c:827-872).  Returns (Visibilities, baseline count)."""
+    L, d = lib(), _VisData()
+    _check(L.rg_read_vis_hdf5(os.fsencode(path), float(bl_min), float(min(bl_max, 1.7976931348623157e308)),
+                              ct.byref(d)))
+    try:
+        n = int(d.n)
+        take = (lambda p, k: np.ctypeslib.as_array(p, shape=(k,)).copy()) if n else (lambda p, k: np.zeros(k))
+        vis = Visibilities(take(d.u, n), take(d.v, n), take(d.w, n), take(d.vis, 2 * n).view(np.complex128))
+        return vis, int(d.bl_count)
+    finally:
+        L.rg_free_vis_data(ct.byref(d))
+
+
+def read_wkern_hdf5(path, theta):
+    """The w-kernel table of a crocodile kernel file (load_wkern,
+    src/reference/hdf5.c:321-413)."""
+    L, d = lib(), _WKernData()
+    _check(L.rg_read_wkern_hdf5(os.fsencode(path), float(theta), ct.byref(d)))
+    try:
+        shape = (d.plane_count, d.oversampling, d.oversampling, d.size, d.size)
+        flat = np.ctypeslib.as_array(d.data, shape=(2 * int(np.prod(shape)),)).copy()
+        return FileWKernel(flat.view(np.complex128).reshape(shape), float(d.w_min), float(d.w_step))
+    finally:
+        L.rg_free_wkern_data(ct.byref(d))
+
+
+def write_vis_hdf5(path, ant1, ant2, time, freq, uvw, vis):
+    """Hierarchical visibility file: uvw [bl, time, 3] metres, freq [bl, nf] Hz,
+    vis [bl, time, nf] complex, time [bl, time]."""
+    uvw = np.ascontiguousarray(uvw, np.float64)
+    n_bl, n_time = uvw.shape[:2]
+    freq = np.ascontiguousarray(freq, np.float64).reshape(n_bl, -1)
+    vis = np.ascontiguousarray(vis, np.complex128).reshape(n_bl, n_time, freq.shape[1])
+    a1 = np.ascontiguousarray(ant1, np.int32)
+    a2 = np.ascontiguousarray(ant2, np.int32)
+    t = np.ascontiguousarray(time, np.float64).reshape(n_bl, n_time)
+    _check(lib().rg_write_vis_hdf5(os.fsencode(path), n_bl, n_time, freq.shape[1], _ptr(a1), _ptr(a2),
+                                   _ptr(t), _ptr(freq), _ptr(uvw), _ptr(vis)))
+
+
+def write_wkern_hdf5(path, theta, wkern):
+    st, keep = _wkern_struct(wkern)
+    _check(lib().rg_write_wkern_hdf5(os.fsencode(path), float(theta), ct.byref(st)))
+    del keep
+
+
+def hdf5_read(path, dataset):
+    """A float64 / int64 / {r, i} dataset of any crocodile file as float64
+    (complex compounds come back with a trailing axis of 2)."""
+    L = lib()
+    dims, nd = (ct.c_int64 * 8)(), ct.c_int(8)
+    _check(L.rg_hdf5_read_f64(os.fsencode(path), dataset.encode(), None, 0, dims, ct.byref(nd)))
+    shape = tuple(dims[k] for k in range(nd.value))
+    out = np.empty(int(np.prod(shape)) if shape else 1, np.float64)
+    _check(L.rg_hdf5_read_f64(os.fsencode(path), dataset.encode(), _ptr(out), out.size, dims, ct.byref(nd)))
+    shape = tuple(dims[k] for k in range(nd.value))
+    return out.reshape(shape)
+
+
+def hdf5_attr(path, obj, name):
+    v = ct.c_double()
+    _check(lib().rg_hdf5_attr_f64(os.fsencode(path), obj.encode(), name.encode(), ct.byref(v)))
+    return v.value
