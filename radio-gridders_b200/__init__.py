@@ -411,8 +411,20 @@ class FileWKernel:
         self.data, self.w_min, self.w_step = data, w_min, w_step
 
     @property
+    def plane_count(self):
+        return int(self.data.shape[0])
+
+    @property
+    def oversampling(self):
+        return int(self.data.shape[1])
+
+    @property
+    def size(self):
+        return int(self.data.shape[3])
+
+    @property
     def w_max(self):
-        return self.w_min + (self.data.shape[0] - 1) * self.w_step
+        return self.w_min + (self.plane_count - 1) * self.w_step
 
 
 def read_vis_hdf5(path, bl_min=0.0, bl_max=float("inf")):

@@ -56,10 +56,14 @@ def test_grid_out(oracle, files, mode):
     assert rel_rms(_load(f"{d}/{mode}.img", n), img_ref) < 1e-5
 
 
-def test_dft_out(oracle, files):
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("reduced", 2e-5)])
+def test_dft_out(oracle, files, precision, tol):
+    """At 64 pixels a 32-pixel tile spans |u| dl ~ 64 turns, so the
+    FP64-reduced mode's FP32 increments leave ~3e-6; all-FP64 is exact."""
     d, obs, (u, v, w, vis), _ = files
     th, lam = obs.meta["theta"], 640.0
     n = int(np.floor(lam * th + 0.5))
-    run("dft.out", f"-vis={d}/vis.h5", f"-theta={th}", f"-lambda={lam}", f"-image={d}/dft.img", "-hermitian")
+    run("dft.out", f"-vis={d}/vis.h5", f"-theta={th}", f"-lambda={lam}", f"-image={d}/dft.img", "-hermitian",
+        f"-precision={precision}")
     ref = oracle.dft_image(n, th, u, v, w, vis, factor=2.0)
-    assert rel_rms(_load(f"{d}/dft.img", n), ref) < 1e-6  # FP64-reduced phase mode
+    assert rel_rms(_load(f"{d}/dft.img", n), ref) < tol
