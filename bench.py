@@ -2,10 +2,12 @@
 """W-towers gridding throughput on B200 (visibilities per second).
 
 One step = one rg_grid_wtowers call over one observation resident in HBM:
-w-range reduction, per-visibility tower/floor binning and coordinates, Romein
-gridding of every active (tower, w-floor) sub-grid, backward row transforms,
-the fused column-transform / Fresnel-step / w=0-transfer / forward-column
-stage, forward row transforms and the FP64 add-back into the master grid — the
+w-range reduction, per-visibility tower/floor binning, coordinates and
+column-strip marks, Romein gridding of every active (tower, w-floor)
+sub-grid, backward column transforms of the marked strips, the fused
+row-transform / Fresnel-step / w=0-transfer stage with the forward row
+transform, forward column transforms and the FP64 add-back into the master
+grid — the
 loop of the reference's grid_wtowers (src/reference/grid.c:295-555) and
 wtowers_CUDA_flat (src/grid/grid_cuda.cu:522-744) up to the final FFT.
 
@@ -140,29 +142,33 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def algorithmic_bytes(stats, nvis, ntowers_data):
-    """Bytes per step of the reference dataflow (one HBM pass per stage):
-    20 B per visibility (3 x f32 uvw + c64), 48 S^2 per active (tower, floor),
-    24 S^2 per tower with data, 32 N^2 for the FP64 master read + write."""
-    s2 = SUBGRID * SUBGRID
-    return (20 * nvis + 48 * s2 * stats["active_subgrids"] + 24 * s2 * ntowers_data
-            + 32 * GRID * GRID)
+STAGES = ("prepare", "romein", "fft_cols_backward", "tower_rows", "tower_finish", "fft_cols_forward",
+          "add_back")
 
 
 def stage_bytes(stage, stats, nvis):
-    """Algorithmic bytes of one launch of each stage (for the roofline)."""
+    """Algorithmic HBM bytes of one launch of each stage (for the roofline).
+    Sub-grids are touched only in their marked column strips (8 columns x S
+    rows x 8 B each): gridding writes them once, the column transform reads
+    and writes them, the row stage reads and clears them."""
     s2 = SUBGRID * SUBGRID
-    na, nt = stats["active_subgrids"], stats["towers_with_data"]
+    strip = 8 * 8 * SUBGRID * stats["marked_strips"]
+    nt, ng = stats["towers_with_data"], stats["floor_groups"]
     ntow = (GRID // (SUBGRID - MARGIN) + 1) ** 2
     return {
-        "zero_subgrids": 8 * s2 * na,                       # write
-        "romein": 24 * nvis + 8 * s2 * na,                  # records + vis in, sub-grids out
-        "fft_rows_backward": 16 * s2 * na,                  # read + write every sub-grid
-        "tower_columns": 8 * s2 * na + 8 * s2 * nt,         # read sub-grids, write sub-images
-        "fft_rows_forward": 16 * s2 * ntow,                 # read + write every sub-image
-        "add_back": 8 * s2 * nt + 16 * GRID * GRID,         # read sub-images, write master
         "prepare": 40 * nvis + 24 * nvis,                   # f64 uvw + c128 in, record + c64 out
+        "romein": 24 * nvis + strip,                        # records + vis in, marked strips out
+        "fft_cols_backward": 2 * strip,                     # marked strips in place
+        "tower_rows": 2 * strip + 8 * s2 * ng,              # strips in + cleared, partials out
+        "tower_finish": 8 * s2 * ng + 8 * s2 * nt,          # partials in, sub-images out
+        "fft_cols_forward": 16 * s2 * ntow,                 # every tower sub-image in place
+        "add_back": 8 * s2 * nt + 16 * GRID * GRID,         # read sub-images, write master
     }.get(stage)
+
+
+def algorithmic_bytes(stats, nvis):
+    """Bytes per step of the sparse dataflow: the sum over its stages."""
+    return sum(stage_bytes(k, stats, nvis) for k in STAGES)
 
 
 def cpu_baseline(obs, wk, reps=1):
@@ -339,7 +345,7 @@ def run_b200(args, rank, world, local_rank):
     if os.path.exists(tpath):
         with open(tpath) as f:
             traffic = json.load(f).get(dom)
-    path_bytes = algorithmic_bytes(stats, nvis, stats["towers_with_data"])
+    path_bytes = algorithmic_bytes(stats, nvis)
     line = {
         "impl": "b200", "metric": METRIC, "value": value, "unit": "vis/s", "n_gpus": world,
         "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step,

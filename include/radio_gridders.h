@@ -93,7 +93,10 @@ const char *rg_last_error(void);
  * visibilities gridded, 1 active (tower, floor) sub-grids, 2 towers with data,
  * 3 w-floors spanned, 4 visibilities dropped for lying outside every tower
  * (cf. the per-baseline check at src/reference/grid.c:519-530), 5 kernel
- * launches issued by the call.  Returns the count written (<= n). */
+ * launches issued by the call; W-towers only: 6 sub-grid column strips of 8
+ * columns holding data (the strips the transforms touch), 7 floor groups of
+ * the row stage.
+ * Returns the count written (<= n). */
 int rg_last_stats(rg_context *ctx, int64_t *out, int n);
 
 /* Per-stage timing (the reference's cudaEvent timing around gridding,

@@ -223,7 +223,8 @@ class Context:
     def last_stats(self):
         out = (ct.c_int64 * 8)()
         n = lib().rg_last_stats(self._h, out, 8)
-        keys = ["gridded", "active_subgrids", "towers_with_data", "floors", "dropped", "launches"]
+        keys = ["gridded", "active_subgrids", "towers_with_data", "floors", "dropped", "launches",
+                "marked_strips", "floor_groups"]
         return {k: int(out[j]) for j, k in enumerate(keys[:n])}
 
     # ---- gridders (src/reference/grid.h:121-126) -------------------------

@@ -169,75 +169,230 @@ __global__ void __launch_bounds__(256) fft32_cols_kernel(float2 *__restrict__ da
 }
 
 // ---------------------------------------------------------------------------
-// W-towers column stage, in two kernels so uneven towers balance.
+// Sparse W-towers transforms.
 //
-// tower_partial_kernel: CTA = (floor group, strip of C columns).  A group is up
-// to G consecutive active floors of one tower.  For each floor: backward column
-// transform of the row-transformed sub-grid, times exp(-2 pi i wp ph(l, m)) with
-// ph = winc (1 - sqrt(1 - l^2 - m^2)) — the reference's wtransfer^(-wp),
-// grid.c:304-319 and :473-496, which also covers the w = 0 transfer —
-// accumulated in registers; the strip sum is written to the group's partial
-// buffer.  Phase products are formed and reduced modulo 1 in FP64; sin/cos of
-// the reduced phase in FP32.
-//
-// tower_finish_kernel: CTA = (tower, strip).  Sums the tower's group partials in
-// group order (deterministic) and applies the forward column transform into the
-// tower's sub-image (grid.c:499, with the row half done by the row kernel).
+// A sub-grid is non-zero only in the column strips its bin's visibilities
+// marked (kStripCols columns each; typically a quarter of them), so the 2-D
+// backward transform runs columns first: sparse_cols_kernel transforms only the
+// marked strips, in place.  A row of the result is then non-zero only in those
+// strips, which is all the row stage reads (and clears).
 // ---------------------------------------------------------------------------
-constexpr int kPartialThreads = 128;
-template <int N1>
-using PartialGeom = ColGeom<N1, 8>;
+int mask_words(int subgrid) { return (subgrid / kStripCols + 31) / 32; }
 
-template <int N1>
-__global__ void __launch_bounds__(kPartialThreads) tower_partial_kernel(
-    float2 *__restrict__ slots, const int *__restrict__ bin_of_slot,
-    const int *__restrict__ group_begin, const int *__restrict__ group_end,
-    const int *__restrict__ range, const int *__restrict__ counts, int slot_cap,
-    const double *__restrict__ ph, float2 *__restrict__ partial, const float2 *__restrict__ tw)
+// One warp per mask word: lane s of warp (slot, word) tests strip 32*word + s.
+__global__ void slot_masks_kernel(const unsigned char *__restrict__ marks, const int *__restrict__ bin_of_slot,
+                                  const int *counts, int slot_cap, int strips, int words,
+                                  unsigned *__restrict__ masks)
 {
-    using G = PartialGeom<N1>;
-    constexpr int N = G::N, C = G::C;
-    constexpr int ITEMS = C * 32;
-    constexpr int PER = (ITEMS + kPartialThreads - 1) / kPartialThreads;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t wi = i / 32;  // (slot, word)
+    const int slot = (int)(wi / words), s = (int)(wi % words) * 32 + (int)(i % 32);
+    const int live = counts[0] < slot_cap ? counts[0] : slot_cap;
+    bool f = false;
+    if (slot < live && s < strips) f = marks[(int64_t)bin_of_slot[slot] * strips + s] != 0;
+    const unsigned b = __ballot_sync(0xffffffffu, f);
+    if ((threadIdx.x & 31) == 0 && slot < slot_cap) {
+        masks[wi] = b;
+        if (b) atomicAdd((int *)counts + 3, __popc(b));  // marked strips, for the statistics
+    }
+}
+
+void launch_slot_masks(cudaStream_t s, const unsigned char *marks, const int *bin_of_slot, const int *counts,
+                       int slot_cap, int subgrid, unsigned *masks)
+{
+    const int words = mask_words(subgrid);
+    const int64_t threads = (int64_t)slot_cap * words * 32;
+    if (threads <= 0) return;
+    slot_masks_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(marks, bin_of_slot, counts, slot_cap,
+                                                                      subgrid / kStripCols, words, masks);
+}
+
+constexpr int kSparseColThreads = 128;
+template <int N1>
+using StripGeom = ColGeom<N1, kStripCols>;
+
+// Persistent: the (slot, strip) pairs of the live slots are dealt round-robin
+// to the CTAs; each CTA gathers its marked pairs into a shared list, then
+// transforms them one after another.
+template <int N1>
+__global__ void __launch_bounds__(kSparseColThreads) sparse_cols_kernel(
+    float2 *__restrict__ slots, const unsigned *__restrict__ masks, const int *__restrict__ counts, int slot_cap,
+    const float2 *__restrict__ tw)
+{
+    using G = StripGeom<N1>;
+    constexpr int N = G::N, C = G::C, STRIPS = N / C, WORDS = (STRIPS + 31) / 32;
+    constexpr int NW = kSparseColThreads / 32;
     extern __shared__ float2 smem[];
     float2 *T = smem;
     float2 *W = smem + G::T_ELEMS;
-    double *P = reinterpret_cast<double *>(W + N);  // [N][C] Fresnel phase of the strip
-    const int strips = N / C;
-    const int group = blockIdx.x / strips, strip = blockIdx.x % strips;
+    __shared__ int list[kSparseColThreads];
+    __shared__ int warp_base[NW + 1];
+    for (int i = threadIdx.x; i < N; i += blockDim.x) W[i] = tw[i];
+    const int live = counts[0] < slot_cap ? counts[0] : slot_cap;
+    const int64_t total = (int64_t)live * STRIPS;
+    const int64_t stride = (int64_t)gridDim.x * kSparseColThreads;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int64_t base = 0; base < total; base += stride) {
+        const int64_t i = base + (int64_t)threadIdx.x * gridDim.x + blockIdx.x;
+        bool f = false;
+        if (i < total) {
+            const int slot = (int)(i / STRIPS), st = (int)(i % STRIPS);
+            f = (masks[(int64_t)slot * WORDS + st / 32] >> (st & 31)) & 1u;
+        }
+        const unsigned b = __ballot_sync(0xffffffffu, f);
+        __syncthreads();  // the previous round's list is consumed
+        if (lane == 0) warp_base[warp + 1] = __popc(b);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            warp_base[0] = 0;
+            for (int k = 1; k <= NW; k++) warp_base[k] += warp_base[k - 1];
+        }
+        __syncthreads();
+        if (f) list[warp_base[warp] + __popc(b & ((1u << lane) - 1u))] = (int)(i - base);
+        __syncthreads();
+        const int n = warp_base[NW];
+        for (int k = 0; k < n; k++) {
+            const int64_t item = base + list[k];
+            const int64_t slot = item / STRIPS;
+            const int st = (int)(item % STRIPS);
+            float2 *col = slots + slot * N * N + st * C;
+            col_step1<N1, +1, C>(col, N, T, W);
+            __syncthreads();
+            for (int it = threadIdx.x; it < C * 32; it += blockDim.x) {
+                const int c = it % C, k2 = it / C;
+                float2 v[N1];
+#pragma unroll
+                for (int n1 = 0; n1 < N1; n1++) v[n1] = T[c * G::CS + n1 * kPad + k2];
+                reg_fft<N1, +1>(v);
+#pragma unroll
+                for (int j = 0; j < N1; j++) col[(int64_t)(k2 + 32 * bitrevc(j, G::LB)) * N + c] = v[j];
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Row stage, in two kernels so uneven towers balance.
+//
+// tower_rows_kernel: CTA = (floor group, strip of R rows).  For each floor of
+// the group: backward row transform of the column-transformed sub-grid (only
+// the slot's marked strips are read, then zeroed), times exp(-2 pi i wp
+// ph(l, m)) with ph = winc (1 - sqrt(1 - l^2 - m^2)) — the reference's
+// wtransfer^(-wp), grid.c:304-319 and :473-496, which also covers the w = 0
+// transfer — accumulated in registers; the strip sum goes to the group's
+// partial buffer.  Phase products are formed and reduced modulo 1 in FP64;
+// sin/cos of the reduced phase in FP32.
+//
+// tower_rows_finish_kernel: CTA = (tower, strip of R rows).  Sums the tower's
+// group partials in group order (deterministic) and applies the forward row
+// transform into the tower's sub-image (the row half of grid.c:499).
+// ---------------------------------------------------------------------------
+constexpr int kRowThreads = 128;
+template <int N1>
+struct RowGeom {
+    static constexpr int N = N1 * 32;
+    static constexpr int R = N1 >= 32 ? 4 : 8;  // rows per CTA
+    static constexpr int LB = ilog2c(N1);
+    static constexpr int STRIPS = N / kStripCols;
+    static constexpr int WORDS = (STRIPS + 31) / 32;
+    static constexpr int ITEMS1 = R * N1;  // step-1 items (n1, row)
+    static constexpr int ITEMS2 = R * 32;  // step-2 items (k2, row)
+    static constexpr int PER = (ITEMS2 + kRowThreads - 1) / kRowThreads;
+    static constexpr int T_ELEMS = R * N1 * kPad;
+};
+
+int tower_row_strips(int subgrid) { return subgrid / (subgrid >= 1024 ? 4 : 8); }
+
+// a = *p when on, else a is left as it is.  A predicated load: the register is
+// written only by the load, so no select waits on the load's result and all of
+// a thread's loads stay in flight together.  The memory clobber keeps later
+// stores (the clearing) after it.
+__device__ __forceinline__ void ld_if(float2 &a, const float2 *p, bool on)
+{
+    asm volatile(
+        "{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %3, 0;\n\t@q ld.global.v2.f32 {%0, %1}, [%2];\n\t}"
+        : "+f"(a.x), "+f"(a.y)
+        : "l"(p), "r"((unsigned)on)
+        : "memory");
+}
+
+template <int N1>
+__global__ void __launch_bounds__(kRowThreads) tower_rows_kernel(
+    float2 *__restrict__ slots, const unsigned *__restrict__ masks, const int *__restrict__ bin_of_slot,
+    const int *__restrict__ group_begin, const int *__restrict__ group_end, const int *__restrict__ range,
+    const int *__restrict__ counts, int slot_cap, const double *__restrict__ ph, float2 *__restrict__ partial,
+    const float2 *__restrict__ tw)
+{
+    using G = RowGeom<N1>;
+    constexpr int N = G::N, R = G::R;
+    extern __shared__ float2 smem[];
+    float2 *T = smem;                                // [R][N1][kPad]
+    float2 *W = smem + G::T_ELEMS;                   // [N]
+    double *P = reinterpret_cast<double *>(W + N);   // [R][N] Fresnel phase of the strip
+    __shared__ unsigned smask[G::WORDS];
+    const int rstrips = N / R;
+    const int group = blockIdx.x / rstrips, row0 = (blockIdx.x % rstrips) * R;
     if (group >= counts[1]) return;  // groups live on the device; grid sized for capacity
     const int wp_min = range[0], nfloor = range[1];
     const int begin = group_begin[group];
     const int end = group_end[group] < slot_cap ? group_end[group] : slot_cap;
     for (int i = threadIdx.x; i < N; i += blockDim.x) W[i] = tw[i];
-    for (int e = threadIdx.x; e < N * C; e += blockDim.x)
-        P[e] = ph[(int64_t)(e / C) * N + strip * C + e % C];
+    for (int e = threadIdx.x; e < R * N; e += blockDim.x) P[e] = ph[(int64_t)row0 * N + e];
 
-    float2 acc[PER][N1];
+    float2 acc[G::PER][N1];
 #pragma unroll
-    for (int q = 0; q < PER; q++)
+    for (int q = 0; q < G::PER; q++)
 #pragma unroll
         for (int j = 0; j < N1; j++) acc[q][j] = make_float2(0.f, 0.f);
-    __syncthreads();
 
     for (int slot = begin; slot < end; slot++) {
         const double mwp = -(double)(wp_min + bin_of_slot[slot] % nfloor);
-        const float2 *base = slots + (int64_t)slot * N * N + strip * C;
-        col_step1<N1, +1, C, true>(base, N, T, W);
+        if (threadIdx.x < G::WORDS) smask[threadIdx.x] = masks[(int64_t)slot * G::WORDS + threadIdx.x];
+        __syncthreads();  // masks visible; the previous floor's step 2 is done with T
+        // the slot's strip mask in two 64-bit registers (at most 128 strips)
+        const unsigned long long m_lo = smask[0] | (G::WORDS > 1 ? (unsigned long long)smask[1] << 32 : 0ull);
+        const unsigned long long m_hi =
+            G::WORDS > 2 ? (smask[2] | (G::WORDS > 3 ? (unsigned long long)smask[3] << 32 : 0ull)) : 0ull;
+        for (int it = threadIdx.x; it < G::ITEMS1; it += blockDim.x) {
+            const int n1 = it % N1, r = it / N1;
+            float2 *src = slots + ((int64_t)slot * N + row0 + r) * N + n1;
+            float2 a[32];
+            // all 32 loads issue before any clearing store
+#pragma unroll
+            for (int n2 = 0; n2 < 32; n2++) {
+                const int strip = (n1 + n2 * N1) / kStripCols;
+                const bool on = ((strip < 64 ? m_lo >> strip : m_hi >> (strip - 64)) & 1ull) != 0;
+                a[n2] = make_float2(0.f, 0.f);
+                ld_if(a[n2], src + n2 * N1, on);
+            }
+#pragma unroll
+            for (int n2 = 0; n2 < 32; n2++) {
+                const int strip = (n1 + n2 * N1) / kStripCols;
+                const bool on = ((strip < 64 ? m_lo >> strip : m_hi >> (strip - 64)) & 1ull) != 0;
+                if (on) src[n2 * N1] = make_float2(0.f, 0.f);  // leave the sub-grid zeroed
+            }
+            reg_fft<32, +1>(a);
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+                const int k2 = bitrevc(j, 5);
+                T[(r * N1 + n1) * kPad + k2] = cmulf(a[j], twiddle<+1>(W, n1 * k2));
+            }
+        }
         __syncthreads();
 #pragma unroll
-        for (int q = 0; q < PER; q++) {
-            const int it = threadIdx.x + q * kPartialThreads;
-            if (it < ITEMS) {
-                const int c = it % C, k2 = it / C;
+        for (int q = 0; q < G::PER; q++) {
+            const int it = threadIdx.x + q * kRowThreads;
+            if (it < G::ITEMS2) {
+                const int k2 = it % 32, r = it / 32;
                 float2 b[N1];
 #pragma unroll
-                for (int n1 = 0; n1 < N1; n1++) b[n1] = T[c * G::CS + n1 * kPad + k2];
+                for (int n1 = 0; n1 < N1; n1++) b[n1] = T[(r * N1 + n1) * kPad + k2];
                 reg_fft<N1, +1>(b);
 #pragma unroll
                 for (int j = 0; j < N1; j++) {
-                    const int row = k2 + 32 * bitrevc(j, G::LB);
-                    double phase = mwp * P[row * C + c];
+                    const int col = k2 + 32 * bitrevc(j, G::LB);
+                    double phase = mwp * P[r * N + col];
                     phase -= rint(phase);  // |phase| <= 1/2 after the FP64 reduction
                     float sn, cs;
                     __sincosf(6.28318530717958647f * (float)phase, &sn, &cs);
@@ -245,58 +400,65 @@ __global__ void __launch_bounds__(kPartialThreads) tower_partial_kernel(
                 }
             }
         }
-        __syncthreads();
     }
-    float2 *out = partial + (int64_t)group * N * N + strip * C;
+    float2 *out = partial + ((int64_t)group * N + row0) * N;
 #pragma unroll
-    for (int q = 0; q < PER; q++) {
-        const int it = threadIdx.x + q * kPartialThreads;
-        if (it < ITEMS) {
-            const int c = it % C, k2 = it / C;
+    for (int q = 0; q < G::PER; q++) {
+        const int it = threadIdx.x + q * kRowThreads;
+        if (it < G::ITEMS2) {
+            const int k2 = it % 32, r = it / 32;
 #pragma unroll
-            for (int j = 0; j < N1; j++) out[(int64_t)(k2 + 32 * bitrevc(j, G::LB)) * N + c] = acc[q][j];
+            for (int j = 0; j < N1; j++) out[(int64_t)r * N + k2 + 32 * bitrevc(j, G::LB)] = acc[q][j];
         }
     }
 }
 
 template <int N1>
-__global__ void __launch_bounds__(256) tower_finish_kernel(
+__global__ void __launch_bounds__(kRowThreads) tower_rows_finish_kernel(
     const float2 *__restrict__ partial, const int *__restrict__ tower_group_first,
     const int *__restrict__ tower_group_count, int group_cap, float2 *__restrict__ subimg,
     const float2 *__restrict__ tw)
 {
-    using G = ColGeom<N1>;
-    constexpr int N = G::N, C = G::C;
+    using G = RowGeom<N1>;
+    constexpr int N = G::N, R = G::R;
     extern __shared__ float2 smem[];
     float2 *T = smem;
     float2 *W = smem + G::T_ELEMS;
-    float2 *U = W + N;  // [N][C]
-    const int strips = N / C;
-    const int tower = blockIdx.x / strips, strip = blockIdx.x % strips;
+    const int rstrips = N / R;
+    const int tower = blockIdx.x / rstrips, row0 = (blockIdx.x % rstrips) * R;
     const int gfirst = tower_group_first[tower];
     int gcount = tower_group_count[tower];
     if (gfirst + gcount > group_cap) gcount = group_cap - gfirst;  // capacity overflow: rerun
     if (gcount <= 0) return;
     for (int i = threadIdx.x; i < N; i += blockDim.x) W[i] = tw[i];
-    for (int e = threadIdx.x; e < N * C; e += blockDim.x) {
-        const int row = e / C, c = e % C;
-        float2 sum = make_float2(0.f, 0.f);
-        for (int g = 0; g < gcount; g++)
-            sum = caddf(sum, partial[(int64_t)(gfirst + g) * N * N + (int64_t)row * N + strip * C + c]);
-        U[e] = sum;
+    __syncthreads();
+    for (int it = threadIdx.x; it < G::ITEMS1; it += blockDim.x) {
+        const int n1 = it % N1, r = it / N1;
+        float2 a[32];
+#pragma unroll
+        for (int n2 = 0; n2 < 32; n2++) a[n2] = make_float2(0.f, 0.f);
+        for (int g = 0; g < gcount; g++) {
+            const float2 *src = partial + ((int64_t)(gfirst + g) * N + row0 + r) * N + n1;
+#pragma unroll
+            for (int n2 = 0; n2 < 32; n2++) a[n2] = caddf(a[n2], src[n2 * N1]);
+        }
+        reg_fft<32, -1>(a);
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+            const int k2 = bitrevc(j, 5);
+            T[(r * N1 + n1) * kPad + k2] = cmulf(a[j], twiddle<-1>(W, n1 * k2));
+        }
     }
     __syncthreads();
-    col_step1<N1, -1>(U, C, T, W);
-    __syncthreads();
-    float2 *out = subimg + (int64_t)tower * N * N + strip * C;
-    for (int it = threadIdx.x; it < C * 32; it += blockDim.x) {
-        const int c = it % C, k2 = it / C;
+    float2 *out = subimg + ((int64_t)tower * N + row0) * N;
+    for (int it = threadIdx.x; it < G::ITEMS2; it += blockDim.x) {
+        const int k2 = it % 32, r = it / 32;
         float2 b[N1];
 #pragma unroll
-        for (int n1 = 0; n1 < N1; n1++) b[n1] = T[c * G::CS + n1 * kPad + k2];
+        for (int n1 = 0; n1 < N1; n1++) b[n1] = T[(r * N1 + n1) * kPad + k2];
         reg_fft<N1, -1>(b);
 #pragma unroll
-        for (int j = 0; j < N1; j++) out[(int64_t)(k2 + 32 * bitrevc(j, G::LB)) * N + c] = b[j];
+        for (int j = 0; j < N1; j++) out[(int64_t)r * N + k2 + 32 * bitrevc(j, G::LB)] = b[j];
     }
 }
 
@@ -308,16 +470,14 @@ static size_t rows_smem() { return sizeof(float2) * (16 * N1 * kPad + N1 * 32); 
 template <int N1>
 static size_t cols_smem() { return sizeof(float2) * (ColGeom<N1>::T_ELEMS + N1 * 32); }
 template <int N1>
-static size_t partial_smem()
+static size_t sparse_cols_smem() { return sizeof(float2) * (StripGeom<N1>::T_ELEMS + N1 * 32); }
+template <int N1>
+static size_t tower_rows_smem()
 {
-    return sizeof(float2) * (PartialGeom<N1>::T_ELEMS + N1 * 32) +
-           sizeof(double) * N1 * 32 * PartialGeom<N1>::C;
+    return sizeof(float2) * (RowGeom<N1>::T_ELEMS + N1 * 32) + sizeof(double) * RowGeom<N1>::R * N1 * 32;
 }
 template <int N1>
-static size_t finish_smem()
-{
-    return sizeof(float2) * (ColGeom<N1>::T_ELEMS + N1 * 32 + N1 * 32 * ColGeom<N1>::C);
-}
+static size_t tower_finish_smem() { return sizeof(float2) * (RowGeom<N1>::T_ELEMS + N1 * 32); }
 
 template <int N1>
 static void rows_impl(cudaStream_t s, float2 *data, int64_t rows, int sign, const float2 *tw,
@@ -350,22 +510,40 @@ static void cols_impl(cudaStream_t s, float2 *data, int batch, int sign, const f
 }
 
 template <int N1>
-static void tower_impl(cudaStream_t s, float2 *slots, const int *bin_of_slot,
-                       const int *group_begin, const int *group_end, const int *range,
-                       const int *counts, int slot_cap, int group_cap,
-                       const int *tower_group_first, const int *tower_group_count, int ntowers,
-                       const double *ph, float2 *partial, float2 *subimg, const float2 *tw)
+static void sparse_cols_impl(cudaStream_t s, float2 *slots, const unsigned *masks, const int *counts, int slot_cap,
+                             const float2 *tw, int sm_count)
 {
-    const int pstrips = N1 * 32 / PartialGeom<N1>::C;
-    const int strips = N1 * 32 / ColGeom<N1>::C;
-    const size_t sm1 = partial_smem<N1>();
-    cudaFuncSetAttribute(tower_partial_kernel<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
+    const size_t sm = sparse_cols_smem<N1>();
+    cudaFuncSetAttribute(sparse_cols_kernel<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sparse_cols_kernel<N1>, kSparseColThreads, sm);
+    if (per_sm < 1) per_sm = 1;
+    sparse_cols_kernel<N1><<<(unsigned)(per_sm * sm_count), kSparseColThreads, sm, s>>>(slots, masks, counts,
+                                                                                        slot_cap, tw);
+}
+
+template <int N1>
+static void tower_rows_impl(cudaStream_t s, float2 *slots, const unsigned *masks, const int *bin_of_slot,
+                            const int *group_begin, const int *group_end, const int *range, const int *counts,
+                            int slot_cap, int group_cap, const double *ph, float2 *partial, const float2 *tw)
+{
+    const int rstrips = RowGeom<N1>::N / RowGeom<N1>::R;
+    const size_t sm1 = tower_rows_smem<N1>();
+    cudaFuncSetAttribute(tower_rows_kernel<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
     if (group_cap > 0)
-        tower_partial_kernel<N1><<<(unsigned)group_cap * pstrips, kPartialThreads, sm1, s>>>(
-            slots, bin_of_slot, group_begin, group_end, range, counts, slot_cap, ph, partial, tw);
-    const size_t sm2 = finish_smem<N1>();
-    cudaFuncSetAttribute(tower_finish_kernel<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
-    tower_finish_kernel<N1><<<(unsigned)ntowers * strips, 256, sm2, s>>>(
+        tower_rows_kernel<N1><<<(unsigned)group_cap * rstrips, kRowThreads, sm1, s>>>(
+            slots, masks, bin_of_slot, group_begin, group_end, range, counts, slot_cap, ph, partial, tw);
+}
+
+template <int N1>
+static void tower_finish_impl(cudaStream_t s, int group_cap, const int *tower_group_first,
+                              const int *tower_group_count, int ntowers, const float2 *partial, float2 *subimg,
+                              const float2 *tw)
+{
+    const int rstrips = RowGeom<N1>::N / RowGeom<N1>::R;
+    const size_t sm2 = tower_finish_smem<N1>();
+    cudaFuncSetAttribute(tower_rows_finish_kernel<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
+    tower_rows_finish_kernel<N1><<<(unsigned)ntowers * rstrips, kRowThreads, sm2, s>>>(
         partial, tower_group_first, tower_group_count, group_cap, subimg, tw);
 }
 
@@ -394,21 +572,33 @@ void launch_fft32_cols(cudaStream_t s, float2 *data, int batch, int n, int sign,
 #undef CALL
 }
 
-void launch_tower_columns(cudaStream_t s, float2 *slots, const int *bin_of_slot,
-                          const int *group_begin, const int *group_end, const int *range,
-                          const int *counts, int slot_cap, int group_cap,
-                          const int *tower_group_first, const int *tower_group_count, int ntowers,
-                          const double *ph, float2 *partial, float2 *subimg, int subgrid,
-                          const float2 *tw)
+void launch_sparse_cols(cudaStream_t s, float2 *slots, const unsigned *masks, const int *counts, int slot_cap,
+                        int subgrid, const float2 *tw, int sm_count)
 {
-#define CALL(N1) tower_impl<N1>(s, slots, bin_of_slot, group_begin, group_end, range, counts, slot_cap, \
-                                group_cap, tower_group_first, tower_group_count, ntowers, ph, partial,  \
-                                subimg, tw)
+#define CALL(N1) sparse_cols_impl<N1>(s, slots, masks, counts, slot_cap, tw, sm_count)
     RG_DISPATCH_N1(subgrid, CALL)
 #undef CALL
 }
 
-int fft32_strips(int n) { return n / 8; }  // strips of the partial (column) stage
+void launch_tower_rows(cudaStream_t s, float2 *slots, const unsigned *masks, const int *bin_of_slot,
+                       const int *group_begin, const int *group_end, const int *range, const int *counts,
+                       int slot_cap, int group_cap, const double *ph, float2 *partial, int subgrid,
+                       const float2 *tw)
+{
+#define CALL(N1) tower_rows_impl<N1>(s, slots, masks, bin_of_slot, group_begin, group_end, range, counts, \
+                                     slot_cap, group_cap, ph, partial, tw)
+    RG_DISPATCH_N1(subgrid, CALL)
+#undef CALL
+}
+
+void launch_tower_finish(cudaStream_t s, int group_cap, const int *tower_group_first, const int *tower_group_count,
+                         int ntowers, const float2 *partial, float2 *subimg, int subgrid, const float2 *tw)
+{
+#define CALL(N1) tower_finish_impl<N1>(s, group_cap, tower_group_first, tower_group_count, ntowers, partial, \
+                                       subimg, tw)
+    RG_DISPATCH_N1(subgrid, CALL)
+#undef CALL
+}
 
 // ---------------------------------------------------------------------------
 // FP64 transforms (image formation)

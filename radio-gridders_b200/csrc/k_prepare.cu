@@ -124,8 +124,8 @@ __global__ void prepare_towers_kernel(const double *__restrict__ u, const double
                                       const double *__restrict__ w, const double2 *__restrict__ vis,
                                       int64_t n, TowerGeom g, const int *__restrict__ range,
                                       int4 *__restrict__ rec, float2 *__restrict__ visf,
-                                      int *__restrict__ active, unsigned *err,
-                                      unsigned long long *counters)
+                                      int *__restrict__ active, unsigned char *__restrict__ marks,
+                                      unsigned *err, unsigned long long *counters)
 {
     if (!range[2]) return;  // more floors than the bin capacity: the caller reruns
     const int wp_min = range[0], nfloor = range[1];
@@ -202,6 +202,12 @@ __global__ void prepare_towers_kernel(const double *__restrict__ u, const double
         r.w = ((row0 & 63) << 8) | (col0 & 63);
         rec[i] = r;
         active[bin] = 1;
+        // column strips (kStripCols wide) the footprint's taps land in; the
+        // linear sub-grid index wraps a column past either edge into the
+        // neighbouring row, i.e. to column (col mod S)
+        unsigned char *mk = marks + (int64_t)bin * (g.subgrid / kStripCols);
+        for (int c = col0; c < col0 + g.ksize; c += kStripCols) mk[(c & (g.subgrid - 1)) / kStripCols] = 1;
+        mk[((col0 + g.ksize - 1) & (g.subgrid - 1)) / kStripCols] = 1;
         gridded++;
     }
     if (local_err) atomicOr(err, local_err);
@@ -218,13 +224,13 @@ __global__ void prepare_towers_kernel(const double *__restrict__ u, const double
 
 void launch_prepare_towers(cudaStream_t s, const double *u, const double *v, const double *w,
                            const double2 *vis, int64_t n, TowerGeom g, const int *range,
-                           int4 *rec, float2 *visf, int *active, unsigned *err,
+                           int4 *rec, float2 *visf, int *active, unsigned char *marks, unsigned *err,
                            unsigned long long *counters)
 {
     int blocks = (int)((n + 255) / 256);
     if (blocks > 148 * 16) blocks = 148 * 16;
     if (blocks < 1) blocks = 1;
-    prepare_towers_kernel<<<blocks, 256, 0, s>>>(u, v, w, vis, n, g, range, rec, visf, active, err,
+    prepare_towers_kernel<<<blocks, 256, 0, s>>>(u, v, w, vis, n, g, range, rec, visf, active, marks, err,
                                                  counters);
 }
 
@@ -383,6 +389,7 @@ __global__ void compact_bins_kernel(const int *__restrict__ active, const int *_
         counts[0] = n_active;
         counts[1] = carry;
         counts[2] = total_with_data;
+        counts[3] = 0;  // marked column strips, counted by the mask kernel
     }
 }
 

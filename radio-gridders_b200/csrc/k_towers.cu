@@ -31,24 +31,6 @@ void launch_fresnel_table(cudaStream_t s, double *ph, int subgrid, double theta,
     fresnel_table_kernel<<<blocks, 256, 0, s>>>(ph, subgrid, theta, winc);
 }
 
-// Zero the live sub-grids (counts[0] of them, at most slot_cap).
-__global__ void zero_slots_kernel(float4 *__restrict__ slots, const int *__restrict__ counts, int slot_cap,
-                                  int64_t slot_elems4)
-{
-    const int live = counts[0] < slot_cap ? counts[0] : slot_cap;
-    const int64_t total = (int64_t)live * slot_elems4;
-    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
-         i += (int64_t)gridDim.x * blockDim.x)
-        slots[i] = z;
-}
-
-void launch_zero_slots(cudaStream_t s, float2 *slots, const int *counts, int slot_cap, int64_t slot_elems,
-                       int sm_count)
-{
-    zero_slots_kernel<<<sm_count * 8, 512, 0, s>>>((float4 *)slots, counts, slot_cap, slot_elems / 2);
-}
-
 // Owner-computes add-back (src/reference/grid.c:503-516): every master pixel
 // sums, in tower order (cy, then cx), the overlapping towers' forward-
 // transformed sub-images divided by S^2, in FP64.  Deterministic.

@@ -218,6 +218,7 @@ void begin_call(rg_context *ctx)
     ctx->n_events = 0;
     ctx->timings.clear();
     ctx->launches = 0;
+    for (int64_t &v : ctx->stats) v = 0;
 }
 
 void begin_stage(rg_context *ctx, const char *name)
@@ -440,12 +441,15 @@ static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *t
     Diag d;
     RG_CHECK(diag_begin(ctx, &d));
     int *range = (int *)((char *)d.err + 48);    // {wp_min, nfloor, ok}
-    int *counts = (int *)((char *)d.err + 32);   // {slots, groups, towers with data}
+    int *counts = (int *)((char *)d.err + 32);   // {slots, groups, towers with data, marked strips}
 
-    void *mm, *active, *rec, *visf, *slot_of_bin, *bin_of_slot, *tfirst, *tcount, *gbegin, *gend, *tgfirst,
-        *tgcount, *slots, *partial, *subimg, *ph;
+    void *mm, *active, *marks, *masks, *rec, *visf, *slot_of_bin, *bin_of_slot, *tfirst, *tcount, *gbegin, *gend,
+        *tgfirst, *tgcount, *slots, *partial, *subimg, *ph;
+    const int strips = S / kStripCols;
     RG_CHECK(scratch(ctx, "wminmax", 16, &mm));
     RG_CHECK(scratch(ctx, "active", sizeof(int) * (size_t)nbins_cap, &active));
+    RG_CHECK(scratch(ctx, "strip_marks", (size_t)nbins_cap * strips, &marks));
+    RG_CHECK(scratch(ctx, "slot_masks", sizeof(unsigned) * (size_t)pl.slots_cap * mask_words(S), &masks));
     RG_CHECK(scratch(ctx, "rec", sizeof(int4) * (size_t)dv.n, &rec));
     RG_CHECK(scratch(ctx, "visf", sizeof(float2) * (size_t)dv.n, &visf));
     RG_CHECK(scratch(ctx, "slot_of_bin", sizeof(int) * (size_t)nbins_cap, &slot_of_bin));
@@ -472,6 +476,7 @@ static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *t
         }
     }
     RG_CUDA(cudaMemsetAsync(active, 0, sizeof(int) * (size_t)nbins_cap, st));
+    RG_CUDA(cudaMemsetAsync(marks, 0, (size_t)nbins_cap * strips, st));
     if (ctx->slots_owner != &pl) {  // the slot buffer was last used by another shape
         pl.zeroed_slots = 0;
         ctx->slots_owner = &pl;
@@ -490,7 +495,6 @@ static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *t
     g.winc = winc;
     g.wk_wmin = wkern->w_min;
     g.wk_wstep = wkern->w_step;
-    const int strips = fft32_strips(S);
 
     begin_stage(ctx, "w_range");
     launch_minmax_w(st, dv.u, dv.v, dv.w, dv.n, (double *)mm, d.err);
@@ -499,11 +503,11 @@ static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *t
     begin_stage(ctx, "prepare");
     if (dv.n > 0)
         launch_prepare_towers(st, dv.u, dv.v, dv.w, dv.vis, dv.n, g, range, (int4 *)rec, (float2 *)visf,
-                              (int *)active, d.err, d.counters);
+                              (int *)active, (unsigned char *)marks, d.err, d.counters);
     end_stage(ctx);
     begin_stage(ctx, "compact");
     launch_compact_bins(st, (const int *)active, range, (int *)slot_of_bin, (int *)bin_of_slot, counts,
-                        (int *)tfirst, (int *)tcount, ntowers, strips, 8 * ctx->sm_count, (int *)gbegin,
+                        (int *)tfirst, (int *)tcount, ntowers, tower_row_strips(S), 8 * ctx->sm_count, (int *)gbegin,
                         (int *)gend, (int *)tgfirst, (int *)tgcount);
     end_stage(ctx);
     // Sub-grids are left zeroed by the previous pass's column stage; only
@@ -519,23 +523,28 @@ static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *t
         launch_romein(st, (const int4 *)rec, (const float2 *)visf, dv.n, taps, (float2 *)slots,
                       (const int *)slot_of_bin, sub_cells, S, K, ctx->sm_count, pl.slots_cap);
     end_stage(ctx);
-    begin_stage(ctx, "fft_rows_backward");
-    launch_fft32_rows(st, (float2 *)slots, (int64_t)pl.slots_cap * S, S, +1, tw, counts);
+    begin_stage(ctx, "fft_cols_backward");
+    launch_slot_masks(st, (const unsigned char *)marks, (const int *)bin_of_slot, counts, pl.slots_cap, S,
+                      (unsigned *)masks);
+    launch_sparse_cols(st, (float2 *)slots, (const unsigned *)masks, counts, pl.slots_cap, S, tw, ctx->sm_count);
     end_stage(ctx);
-    begin_stage(ctx, "tower_columns");
-    launch_tower_columns(st, (float2 *)slots, (const int *)bin_of_slot, (const int *)gbegin,
-                         (const int *)gend, range, counts, pl.slots_cap, pl.groups_cap, (const int *)tgfirst,
-                         (const int *)tgcount, ntowers, (const double *)ph, (float2 *)partial,
-                         (float2 *)subimg, S, tw);
+    begin_stage(ctx, "tower_rows");
+    launch_tower_rows(st, (float2 *)slots, (const unsigned *)masks, (const int *)bin_of_slot, (const int *)gbegin,
+                      (const int *)gend, range, counts, pl.slots_cap, pl.groups_cap, (const double *)ph,
+                      (float2 *)partial, S, tw);
     end_stage(ctx);
-    begin_stage(ctx, "fft_rows_forward");
-    launch_fft32_rows(st, (float2 *)subimg, (int64_t)ntowers * S, S, -1, tw);
+    begin_stage(ctx, "tower_finish");
+    launch_tower_finish(st, pl.groups_cap, (const int *)tgfirst, (const int *)tgcount, ntowers,
+                        (const float2 *)partial, (float2 *)subimg, S, tw);
+    end_stage(ctx);
+    begin_stage(ctx, "fft_cols_forward");
+    launch_fft32_cols(st, (float2 *)subimg, ntowers, S, -1, tw);
     end_stage(ctx);
     begin_stage(ctx, "add_back");
     launch_add_back(st, (const float2 *)subimg, (const int *)tcount, (double2 *)out_dev, N, S, M, chunk, nchunk,
                     (flags & RG_GRID_OVERWRITE) ? 1 : 0, range, counts, pl.slots_cap, pl.groups_cap);
     end_stage(ctx);
-    ctx->launches += 12;
+    ctx->launches += 11;  // minmax, floors, prepare, compact, romein, masks, cols, rows, finish, cols, add-back
     RG_CHECK(check_launch("W-towers pass"));
 
     // single read-back: error word, counters, counts, range
@@ -544,10 +553,10 @@ static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *t
     RG_CUDA(cudaStreamSynchronize(st));
     unsigned err;
     unsigned long long ctr[2];
-    int cnt[3], rng[3];
+    int cnt[4], rng[3];
     std::memcpy(&err, host, 4);
     std::memcpy(ctr, host + 16, 16);
-    std::memcpy(cnt, host + 32, 12);
+    std::memcpy(cnt, host + 32, 16);
     std::memcpy(rng, host + 48, 12);
     pl.seen_floors = rng[1];
     pl.seen_slots = cnt[0];
@@ -565,6 +574,8 @@ static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *t
     ctx->stats[2] = cnt[2];
     ctx->stats[3] = rng[1];
     ctx->stats[4] = (int64_t)ctr[1];
+    ctx->stats[6] = cnt[3];
+    ctx->stats[7] = cnt[1];
     return RG_OK;
 }
 

@@ -155,12 +155,15 @@ void launch_minmax_w(cudaStream_t s, const double *u, const double *v, const dou
 // (grid.c:357-367 from the reduced w range)
 void launch_w_floors(cudaStream_t s, const double *wrange, double winc, int floors_cap, int *range,
                      unsigned *err);
+// Column strips: sub-grid columns in groups of kStripCols; a (bin, strip) mark
+// byte is set when any visibility of the bin has a tap in the strip.  Only
+// marked strips are ever non-zero, so the column transforms and the row stage
+// touch only them.
+constexpr int kStripCols = 8;
 void launch_prepare_towers(cudaStream_t s, const double *u, const double *v, const double *w,
                            const double2 *vis, int64_t n, TowerGeom g, const int *range,
-                           int4 *rec, float2 *visf, int *active, unsigned *err,
+                           int4 *rec, float2 *visf, int *active, unsigned char *marks, unsigned *err,
                            unsigned long long *counters);
-void launch_zero_slots(cudaStream_t s, float2 *slots, const int *counts, int slot_cap,
-                       int64_t slot_elems, int sm_count);
 void launch_prepare_wproj(cudaStream_t s, const double *u, const double *v, const double *w,
                           const double2 *vis, int64_t n, int grid_size, double theta,
                           int ksize, int ov, int planes, double wk_wmin, double wk_wstep,
@@ -181,21 +184,35 @@ void launch_romein(cudaStream_t s, const int4 *rec, const float2 *visf, int64_t 
 
 // k_towers.cu
 void launch_fresnel_table(cudaStream_t s, double *ph, int subgrid, double theta, double winc);
-// Column stage in floor groups: group g covers active slots
-// [group_begin[g], group_end[g]) of one tower; partial holds one sub-grid per
-// group; tower t's groups are [tower_group_first[t], +tower_group_count[t]).
-// range = {wp_min, nfloor, ok} and counts = {slots, groups, towers} live on the
-// device; launches are sized by the capacities.
-// The column stage reads every live sub-grid once and leaves it zeroed (the
-// reference clears its sub-grid after each floor, grid.c:473-481), so the
-// next gridding pass needs no separate clear.
-void launch_tower_columns(cudaStream_t s, float2 *slots, const int *bin_of_slot,
-                          const int *group_begin, const int *group_end, const int *range,
-                          const int *counts, int slot_cap, int group_cap,
-                          const int *tower_group_first, const int *tower_group_count, int ntowers,
-                          const double *ph, float2 *partial, float2 *subimg, int subgrid,
-                          const float2 *tw);
-int fft32_strips(int n);  // column strips per sub-grid in the column kernels
+// Sparse sub-grid transforms and the W-towers row stage.  Group g covers
+// active slots [group_begin[g], group_end[g]) of one tower; partial holds one
+// sub-grid per group; tower t's groups are [tower_group_first[t],
+// +tower_group_count[t]).  range = {wp_min, nfloor, ok} and counts = {slots,
+// groups, towers} live on the device; launches are sized by the capacities.
+//
+// slot_masks: bit s of word masks[slot*mask_words(S) + s/32] = strip s of the
+// slot's bin is marked.
+int mask_words(int subgrid);
+void launch_slot_masks(cudaStream_t s, const unsigned char *marks, const int *bin_of_slot,
+                       const int *counts, int slot_cap, int subgrid, unsigned *masks);
+// Backward column transform, in place, of the marked strips of the live slots.
+void launch_sparse_cols(cudaStream_t s, float2 *slots, const unsigned *masks, const int *counts,
+                        int slot_cap, int subgrid, const float2 *tw, int sm_count);
+// Row stage: per group and strip of rows, for each floor the backward row
+// transform (reading only marked strips and leaving them zeroed: the reference
+// clears its sub-grid after each floor, grid.c:473-481), times the floor's
+// Fresnel factor, accumulated into the group's partial sub-grid.
+void launch_tower_rows(cudaStream_t s, float2 *slots, const unsigned *masks, const int *bin_of_slot,
+                       const int *group_begin, const int *group_end, const int *range,
+                       const int *counts, int slot_cap, int group_cap, const double *ph,
+                       float2 *partial, int subgrid, const float2 *tw);
+// Per tower: the sum of its groups' partials (in group order) and the forward
+// row transform into subimg.  The forward column transform of subimg follows
+// (launch_fft32_cols).
+void launch_tower_finish(cudaStream_t s, int group_cap, const int *tower_group_first,
+                         const int *tower_group_count, int ntowers, const float2 *partial,
+                         float2 *subimg, int subgrid, const float2 *tw);
+int tower_row_strips(int subgrid);  // row strips per sub-grid in the row stage
 void launch_add_back(cudaStream_t s, const float2 *subimg, const int *tower_count,
                      double2 *master, int grid_size, int subgrid, int margin, int chunk,
                      int nchunk, int overwrite, const int *range, const int *counts, int slot_cap,
