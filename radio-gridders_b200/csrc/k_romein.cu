@@ -27,9 +27,11 @@ namespace rg {
 
 // P grid points per thread: thread (myU, myV0) owns the points of column
 // residue myU and row residues myV0 + j*K/P, j < P, so a visibility's record is
-// decoded once for P taps.
+// decoded once for P taps.  A visibility whose sub-grid, linear origin and
+// origin residues equal the previous one's (about half of them along a track)
+// skips the per-point change tests: all of the thread's points are unchanged.
 template <int K, int P>
-__global__ void __launch_bounds__(K *K / P) romein_kernel(
+__global__ void __launch_bounds__(K *K / P, 1536 / (K * K / P)) romein_kernel(
     const int4 *__restrict__ rec, const float2 *__restrict__ visf, int64_t n,
     const float2 *__restrict__ taps, float2 *__restrict__ grids,
     const int *__restrict__ slot_of_bin, int64_t grid_stride, int side, int64_t chunk, int slot_cap)
@@ -44,7 +46,8 @@ __global__ void __launch_bounds__(K *K / P) romein_kernel(
 
     for (int64_t c0 = (int64_t)blockIdx.x * chunk; c0 < n; c0 += (int64_t)gridDim.x * chunk) {
         const int64_t c1 = c0 + chunk < n ? c0 + chunk : n;
-        int cur_bin = -1;
+        int cur_bin = -1, cur_goff = 0, cur_res = 0;
+        float2 *cur_grid = nullptr;  // the current bin's sub-grid (null: past the slot capacity)
         int cur_idx[P];
         float2 sum[P];
 #pragma unroll
@@ -66,35 +69,42 @@ __global__ void __launch_bounds__(K *K / P) romein_kernel(
                 const int cu = (myU - (r.w & 0xff)) & (K - 1);
                 const int r0 = r.w >> 8;
                 float2 t[P];
-                int idx[P];
+                int cv[P];
 #pragma unroll
                 for (int p = 0; p < P; p++) {
-                    const int cv = (myV0 + p * RS - r0) & (K - 1);
-                    idx[p] = r.y + cv * side + cu;
-                    t[p] = __ldg(taps + r.z + cv * K + cu);
+                    cv[p] = (myV0 + p * RS - r0) & (K - 1);
+                    t[p] = __ldg(taps + r.z + cv[p] * K + cu);
                 }
                 const float2 vz = svis[j];
+                if (r.x == cur_bin && r.y == cur_goff && r.w == cur_res) {
+                    // same sub-grid and footprint origin: every point unchanged
+#pragma unroll
+                    for (int p = 0; p < P; p++) {
+                        sum[p].x = fmaf(vz.x, t[p].x, fmaf(vz.y, t[p].y, sum[p].x));
+                        sum[p].y = fmaf(vz.y, t[p].x, fmaf(-vz.x, t[p].y, sum[p].y));
+                    }
+                    continue;
+                }
+                cur_goff = r.y;
+                cur_res = r.w;
+                int idx[P];
+#pragma unroll
+                for (int p = 0; p < P; p++) idx[p] = r.y + cv[p] * side + cu;
                 if (r.x != cur_bin) {
 #pragma unroll
                     for (int p = 0; p < P; p++) {
-                        if (cur_bin >= 0 && (unsigned)cur_idx[p] < (unsigned)limit) {
-                            const int slot = slot_of_bin[cur_bin];
-                            if (slot < slot_cap)
-                                atomicAdd(grids + (int64_t)slot * grid_stride + cur_idx[p], sum[p]);
-                        }
+                        if (cur_grid && (unsigned)cur_idx[p] < (unsigned)limit) atomicAdd(cur_grid + cur_idx[p], sum[p]);
                         cur_idx[p] = idx[p];
                         sum[p] = make_float2(0.f, 0.f);
                     }
                     cur_bin = r.x;
+                    const int slot = slot_of_bin[cur_bin];
+                    cur_grid = slot < slot_cap ? grids + (int64_t)slot * grid_stride : nullptr;
                 }
 #pragma unroll
                 for (int p = 0; p < P; p++) {
                     if (idx[p] != cur_idx[p]) {
-                        if ((unsigned)cur_idx[p] < (unsigned)limit) {
-                            const int slot = slot_of_bin[cur_bin];
-                            if (slot < slot_cap)
-                                atomicAdd(grids + (int64_t)slot * grid_stride + cur_idx[p], sum[p]);
-                        }
+                        if (cur_grid && (unsigned)cur_idx[p] < (unsigned)limit) atomicAdd(cur_grid + cur_idx[p], sum[p]);
                         cur_idx[p] = idx[p];
                         sum[p] = make_float2(0.f, 0.f);
                     }
@@ -103,43 +113,43 @@ __global__ void __launch_bounds__(K *K / P) romein_kernel(
                 }
             }
         }
-        if (cur_bin >= 0) {
-            const int slot = slot_of_bin[cur_bin];
+        if (cur_grid) {
 #pragma unroll
             for (int p = 0; p < P; p++)
-                if ((unsigned)cur_idx[p] < (unsigned)limit && slot < slot_cap)
-                    atomicAdd(grids + (int64_t)slot * grid_stride + cur_idx[p], sum[p]);
+                if ((unsigned)cur_idx[p] < (unsigned)limit) atomicAdd(cur_grid + cur_idx[p], sum[p]);
         }
     }
+}
+
+template <int K, int P>
+static void romein_launch(cudaStream_t s, const int4 *rec, const float2 *visf, int64_t n, const float2 *taps,
+                          float2 *grids, const int *slot_of_bin, int64_t grid_stride, int grid_side, int sm_count,
+                          int slot_cap)
+{
+    // Every CTA resident at once, each with an equal contiguous run of
+    // visibilities: occupancy, not the chunk size, decides the grid.
+    constexpr int NT = K * K / P;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, romein_kernel<K, P>, NT, 0);
+    if (per_sm < 1) per_sm = 1;
+    int64_t blocks = (int64_t)sm_count * per_sm;
+    int64_t chunk = (n + blocks - 1) / blocks;
+    if (chunk < 32) chunk = 32;
+    blocks = (n + chunk - 1) / chunk;
+    if (blocks < 1) blocks = 1;
+    romein_kernel<K, P><<<(unsigned)blocks, NT, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin, grid_stride,
+                                                         grid_side, chunk, slot_cap);
 }
 
 void launch_romein(cudaStream_t s, const int4 *rec, const float2 *visf, int64_t n,
                    const float2 *taps, float2 *grids, const int *slot_of_bin, int64_t grid_stride,
                    int grid_side, int ksize, int sm_count, int slot_cap)
 {
-    const int64_t chunk = 1024;
-    int64_t blocks = (n + chunk - 1) / chunk;
-    const int64_t cap = (int64_t)sm_count * 16;
-    if (blocks > cap) blocks = cap;
-    if (blocks < 1) blocks = 1;
-    const unsigned nb = (unsigned)blocks;
     switch (ksize) {
-        case 4:
-            romein_kernel<4, 1><<<nb, 16, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin, grid_stride, grid_side,
-                                                  chunk, slot_cap);
-            break;
-        case 8:
-            romein_kernel<8, 2><<<nb, 32, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin, grid_stride, grid_side,
-                                                  chunk, slot_cap);
-            break;
-        case 16:
-            romein_kernel<16, 4><<<nb, 64, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin, grid_stride,
-                                                   grid_side, chunk, slot_cap);
-            break;
-        case 32:
-            romein_kernel<32, 4><<<nb, 256, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin, grid_stride,
-                                                    grid_side, chunk, slot_cap);
-            break;
+        case 4: romein_launch<4, 1>(s, rec, visf, n, taps, grids, slot_of_bin, grid_stride, grid_side, sm_count, slot_cap); break;
+        case 8: romein_launch<8, 2>(s, rec, visf, n, taps, grids, slot_of_bin, grid_stride, grid_side, sm_count, slot_cap); break;
+        case 16: romein_launch<16, 4>(s, rec, visf, n, taps, grids, slot_of_bin, grid_stride, grid_side, sm_count, slot_cap); break;
+        case 32: romein_launch<32, 4>(s, rec, visf, n, taps, grids, slot_of_bin, grid_stride, grid_side, sm_count, slot_cap); break;
         default: break;
     }
 }
