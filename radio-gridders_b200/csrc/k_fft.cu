@@ -34,6 +34,15 @@ void fft32_init_twiddles(cudaStream_t s, float2 *tw, int n)
     cudaStreamSynchronize(s);
 }
 
+// The four-step twiddles W_N^(n1 k2) in shared memory, laid out [k2][n1]: the
+// lanes of a warp (consecutive n1 for one k2) read consecutive entries, free of
+// bank conflicts.  tw is the length-N table exp(-2 pi i k / N).
+template <int N1>
+__device__ __forceinline__ void load_twiddles(float2 *W, const float2 *__restrict__ tw)
+{
+    for (int i = threadIdx.x; i < N1 * 32; i += blockDim.x) W[i] = tw[(i % N1) * (i / N1)];
+}
+
 template <int SIGN>
 __device__ __forceinline__ float2 twiddle(const float2 *W, int k)
 {
@@ -63,7 +72,7 @@ __global__ void __launch_bounds__(256) fft32_rows_kernel(float2 *__restrict__ da
         if (live < rows) rows = live;
     }
     if (row0 >= rows) return;
-    for (int i = threadIdx.x; i < N; i += blockDim.x) W[i] = tw[i];
+    load_twiddles<N1>(W, tw);
     __syncthreads();
 
     for (int it = threadIdx.x; it < R * N1; it += blockDim.x) {
@@ -82,7 +91,7 @@ __global__ void __launch_bounds__(256) fft32_rows_kernel(float2 *__restrict__ da
 #pragma unroll
         for (int j = 0; j < 32; j++) {
             const int k2 = bitrevc(j, 5);
-            T[(r * N1 + n1) * kPad + k2] = cmulf(a[j], twiddle<SIGN>(W, n1 * k2));
+            T[(r * N1 + n1) * kPad + k2] = cmulf(a[j], twiddle<SIGN>(W, k2 * N1 + n1));
         }
     }
     __syncthreads();
@@ -136,7 +145,7 @@ __device__ __forceinline__ void col_step1(const float2 *__restrict__ src, int ld
 #pragma unroll
         for (int j = 0; j < 32; j++) {
             const int k2 = bitrevc(j, 5);
-            T[c * G::CS + n1 * kPad + k2] = cmulf(a[j], twiddle<SIGN>(W, n1 * k2));
+            T[c * G::CS + n1 * kPad + k2] = cmulf(a[j], twiddle<SIGN>(W, k2 * N1 + n1));
         }
     }
 }
@@ -150,7 +159,7 @@ __global__ void __launch_bounds__(256) fft32_cols_kernel(float2 *__restrict__ da
     extern __shared__ float2 smem[];
     float2 *T = smem;
     float2 *W = smem + G::T_ELEMS;
-    for (int i = threadIdx.x; i < N; i += blockDim.x) W[i] = tw[i];
+    load_twiddles<N1>(W, tw);
     const int strip = blockIdx.x % (N / G::C);
     const int64_t arr = blockIdx.x / (N / G::C);
     float2 *base = data + arr * N * N + strip * G::C;
@@ -227,7 +236,7 @@ __global__ void __launch_bounds__(kSparseColThreads) sparse_cols_kernel(
     float2 *W = smem + G::T_ELEMS;
     __shared__ int list[kSparseColThreads];
     __shared__ int warp_base[NW + 1];
-    for (int i = threadIdx.x; i < N; i += blockDim.x) W[i] = tw[i];
+    load_twiddles<N1>(W, tw);
     const int live = counts[0] < slot_cap ? counts[0] : slot_cap;
     const int64_t total = (int64_t)live * STRIPS;
     const int64_t stride = (int64_t)gridDim.x * kSparseColThreads;
@@ -304,6 +313,40 @@ struct RowGeom {
 
 int tower_row_strips(int subgrid) { return subgrid / (subgrid >= 1024 ? 4 : 8); }
 
+// Bit n2 (n2 < 32) of the result = strip (n1 + n2*N1)/kStripCols of the
+// 128-bit strip mask (lo, hi) is marked: the element n1 + n2*N1 of a row that
+// the step-1 item n1 loads.  Strided bit gathers by mask-and-fold.
+__device__ __forceinline__ unsigned long long keep_every2(unsigned long long x)
+{
+    x &= 0x5555555555555555ull;
+    x = (x | (x >> 1)) & 0x3333333333333333ull;
+    x = (x | (x >> 2)) & 0x0F0F0F0F0F0F0F0Full;
+    x = (x | (x >> 4)) & 0x00FF00FF00FF00FFull;
+    x = (x | (x >> 8)) & 0x0000FFFF0000FFFFull;
+    return (x | (x >> 16)) & 0x00000000FFFFFFFFull;
+}
+__device__ __forceinline__ unsigned long long keep_every4(unsigned long long x)
+{
+    x &= 0x1111111111111111ull;
+    x = (x | (x >> 3)) & 0x0303030303030303ull;
+    x = (x | (x >> 6)) & 0x000F000F000F000Full;
+    x = (x | (x >> 12)) & 0x000000FF000000FFull;
+    return (x | (x >> 24)) & 0xFFFFull;
+}
+template <int N1>
+__device__ __forceinline__ unsigned element_bits(unsigned long long lo, unsigned long long hi, int n1)
+{
+    static_assert(kStripCols == 8, "strip gathers assume 8-column strips");
+    if (N1 == 8) return (unsigned)lo;                              // strip = n2
+    if (N1 == 16) return (unsigned)keep_every2(lo >> (n1 >> 3));   // strip = 2 n2 + n1/8
+    if (N1 == 32)                                                  // strip = 4 n2 + n1/8
+        return (unsigned)(keep_every4(lo >> (n1 >> 3)) | keep_every4(hi >> (n1 >> 3)) << 16);
+    unsigned b = 0;  // N1 < 8: several n2 share a strip
+#pragma unroll
+    for (int n2 = 0; n2 < 32; n2++) b |= (unsigned)((lo >> ((n1 + n2 * N1) / kStripCols)) & 1ull) << n2;
+    return b;
+}
+
 // a = *p when on, else a is left as it is.  A predicated load: the register is
 // written only by the load, so no select waits on the load's result and all of
 // a thread's loads stay in flight together.  The memory clobber keeps later
@@ -337,7 +380,7 @@ __global__ void __launch_bounds__(kRowThreads) tower_rows_kernel(
     const int wp_min = range[0], nfloor = range[1];
     const int begin = group_begin[group];
     const int end = group_end[group] < slot_cap ? group_end[group] : slot_cap;
-    for (int i = threadIdx.x; i < N; i += blockDim.x) W[i] = tw[i];
+    load_twiddles<N1>(W, tw);
     for (int e = threadIdx.x; e < R * N; e += blockDim.x) P[e] = ph[(int64_t)row0 * N + e];
 
     float2 acc[G::PER][N1];
@@ -357,26 +400,22 @@ __global__ void __launch_bounds__(kRowThreads) tower_rows_kernel(
         for (int it = threadIdx.x; it < G::ITEMS1; it += blockDim.x) {
             const int n1 = it % N1, r = it / N1;
             float2 *src = slots + ((int64_t)slot * N + row0 + r) * N + n1;
+            const unsigned on = element_bits<N1>(m_lo, m_hi, n1);
             float2 a[32];
             // all 32 loads issue before any clearing store
 #pragma unroll
             for (int n2 = 0; n2 < 32; n2++) {
-                const int strip = (n1 + n2 * N1) / kStripCols;
-                const bool on = ((strip < 64 ? m_lo >> strip : m_hi >> (strip - 64)) & 1ull) != 0;
                 a[n2] = make_float2(0.f, 0.f);
-                ld_if(a[n2], src + n2 * N1, on);
+                ld_if(a[n2], src + n2 * N1, (on >> n2) & 1u);
             }
 #pragma unroll
-            for (int n2 = 0; n2 < 32; n2++) {
-                const int strip = (n1 + n2 * N1) / kStripCols;
-                const bool on = ((strip < 64 ? m_lo >> strip : m_hi >> (strip - 64)) & 1ull) != 0;
-                if (on) src[n2 * N1] = make_float2(0.f, 0.f);  // leave the sub-grid zeroed
-            }
+            for (int n2 = 0; n2 < 32; n2++)
+                if ((on >> n2) & 1u) src[n2 * N1] = make_float2(0.f, 0.f);  // leave the sub-grid zeroed
             reg_fft<32, +1>(a);
 #pragma unroll
             for (int j = 0; j < 32; j++) {
                 const int k2 = bitrevc(j, 5);
-                T[(r * N1 + n1) * kPad + k2] = cmulf(a[j], twiddle<+1>(W, n1 * k2));
+                T[(r * N1 + n1) * kPad + k2] = cmulf(a[j], twiddle<+1>(W, k2 * N1 + n1));
             }
         }
         __syncthreads();
@@ -430,7 +469,7 @@ __global__ void __launch_bounds__(kRowThreads) tower_rows_finish_kernel(
     int gcount = tower_group_count[tower];
     if (gfirst + gcount > group_cap) gcount = group_cap - gfirst;  // capacity overflow: rerun
     if (gcount <= 0) return;
-    for (int i = threadIdx.x; i < N; i += blockDim.x) W[i] = tw[i];
+    load_twiddles<N1>(W, tw);
     __syncthreads();
     for (int it = threadIdx.x; it < G::ITEMS1; it += blockDim.x) {
         const int n1 = it % N1, r = it / N1;
@@ -446,7 +485,7 @@ __global__ void __launch_bounds__(kRowThreads) tower_rows_finish_kernel(
 #pragma unroll
         for (int j = 0; j < 32; j++) {
             const int k2 = bitrevc(j, 5);
-            T[(r * N1 + n1) * kPad + k2] = cmulf(a[j], twiddle<-1>(W, n1 * k2));
+            T[(r * N1 + n1) * kPad + k2] = cmulf(a[j], twiddle<-1>(W, k2 * N1 + n1));
         }
     }
     __syncthreads();

@@ -157,3 +157,16 @@ def test_weight_hermitian_shift_image_exact(rg, ctx, oracle, wproj_data, golden)
     assert np.array_equal(ctx.fft_shift(g.copy()), golden["shifted"])
     img = ctx.image_from_grid(g.copy())
     assert rel_rms(img, oracle.image_from_grid(g)) < 1e-13
+
+
+def test_wtowers_subgrid_1024(rg, ctx, sim, oracle):
+    """The largest sub-grid (1024: 128 column strips, two mask words per half)
+    on a 1024-cell grid, against the oracle."""
+    obs = sim.wtowers_plain(seed=6, n_st=40, n_dump=8, n_chan=2, lam=10240.0)
+    n, th = obs.meta["grid_size"], obs.meta["theta"]
+    u, v, w, vis = obs.flat()
+    wkt = sim.generate_wkernel(th, np.arange(-6, 7, 1.0))
+    g = np.zeros((n, n), np.complex128)
+    ctx.grid_wtowers(g, n, th, V(rg, u, v, w, vis), wkt, 1024, 32, 10.0)
+    ref = oracle.grid_wtowers(n, th, u, v, w, vis, wkt, 1024, 32, 10.0)
+    assert rel_rms(g, ref) < TOL
