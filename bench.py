@@ -269,8 +269,7 @@ def run_b200(args, rank, world, local_rank):
     torch.cuda.synchronize()
     stats = ctx.last_stats()
 
-    # timed region
-    ctx.set_profiling(True)
+    # timed region (no per-stage events inside it)
     clocks = Clocks(local_rank)
     clocks.start()
     if world > 1:
@@ -286,13 +285,20 @@ def run_b200(args, rank, world, local_rank):
         s1.record(stream)
         s1.synchronize()
         step_ms.append(s0.elapsed_time(s1))
-        for name, ms in ctx.last_timings():
-            stage_ms.setdefault(name, []).append(ms)
         launches += ctx.last_stats()["launches"]
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
+
+    # per-stage breakdown: the same steps again with CUDA events around each stage
+    ctx.set_profiling(True)
+    for _ in range(args.steps):
+        flush.fill_(1)
+        step()
+        torch.cuda.synchronize()
+        for name, ms in ctx.last_timings():
+            stage_ms.setdefault(name, []).append(ms)
     ctx.set_profiling(False)
 
     total = torch.tensor([sum(step_ms)], dtype=torch.float64, device=dev)
@@ -344,7 +350,8 @@ def run_b200(args, rank, world, local_rank):
     tpath = os.path.join(REPO, "profiles", "wtowers_traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get(dom)
+            entry = json.load(f).get(dom)
+        traffic = entry["dram_bytes"] if isinstance(entry, dict) else entry
     path_bytes = algorithmic_bytes(stats, nvis)
     line = {
         "impl": "b200", "metric": METRIC, "value": value, "unit": "vis/s", "n_gpus": world,
@@ -367,6 +374,8 @@ def run_b200(args, rank, world, local_rank):
         "path_roofline": {"algorithmic_bytes_per_step": path_bytes,
                           "achieved_gbs": path_bytes / (ms_per_step * 1e-3) / 1e9,
                           "frac": path_bytes / (ms_per_step * 1e-3) / 1e9 / peak},
+        "step_ms_min_median_max": [round(min(step_ms), 4), round(statistics.median(step_ms), 4),
+                                   round(max(step_ms), 4)],
         "stage_ms": {k: round(statistics.mean(v), 4) for k, v in stage_ms.items()},
         "e2e": {"value": e2e_value, "unit": "vis/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_t.item()},

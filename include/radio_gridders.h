@@ -254,6 +254,16 @@ rg_status rg_mlp_eval(rg_context *ctx, rg_mlp *mlp, const float *samples, int64_
 rg_status rg_grid_wprojection_learned(rg_context *ctx, rg_mlp *mlp, double *uvgrid, int grid_size,
                                       double theta, const rg_vis *vis, int flags);
 
+/* W-towers with the learned kernel: the rg_grid_wtowers pass (tower and floor
+ * binning, sub-grid transforms, Fresnel steps, FP64 add-back) with every
+ * visibility's taps evaluated by the network at its continuous residual
+ * w - w_mid and sub-cell offsets (footprint origin floor(x) - K/2) instead of
+ * the oversampled table.  The network's w range must cover wincrement / 2.
+ * No counterpart in the reference. */
+rg_status rg_grid_wtowers_learned(rg_context *ctx, rg_mlp *mlp, double *uvgrid, int grid_size, double theta,
+                                  const rg_vis *vis, int subgrid_size, int subgrid_margin, double wincrement,
+                                  int flags);
+
 #ifdef __cplusplus
 }
 #endif

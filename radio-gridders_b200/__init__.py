@@ -41,7 +41,7 @@ EXPORTS = [
     "rg_make_hermitian", "rg_fft_shift", "rg_image_from_grid", "rg_fft2d", "rg_dft_image",
     "rg_grid_wprojection_noalloc", "rg_mlp_param_count", "rg_mlp_create", "rg_mlp_destroy",
     "rg_mlp_set_params", "rg_mlp_get_params", "rg_mlp_gradient", "rg_mlp_train", "rg_mlp_eval",
-    "rg_grid_wprojection_learned", "rg_read_vis_hdf5", "rg_free_vis_data", "rg_read_wkern_hdf5",
+    "rg_grid_wprojection_learned", "rg_grid_wtowers_learned", "rg_read_vis_hdf5", "rg_free_vis_data", "rg_read_wkern_hdf5",
     "rg_free_wkern_data", "rg_write_vis_hdf5", "rg_write_wkern_hdf5", "rg_hdf5_read_f64",
     "rg_hdf5_attr_f64",
 ]
@@ -117,6 +117,7 @@ def lib():
         L.rg_mlp_train.argtypes = [vp, vp, vp, vp, i64, i, i, ct.c_float, vp]
         L.rg_mlp_eval.argtypes = [vp, vp, vp, i64, vp]
         L.rg_grid_wprojection_learned.argtypes = [vp, vp, vp, i, d, ct.POINTER(_Vis), i]
+        L.rg_grid_wtowers_learned.argtypes = [vp, vp, vp, i, d, ct.POINTER(_Vis), i, i, d, i]
         L.rg_read_vis_hdf5.argtypes = [ct.c_char_p, d, d, ct.POINTER(_VisData)]
         L.rg_free_vis_data.argtypes = [ct.POINTER(_VisData)]
         L.rg_free_vis_data.restype = None
@@ -358,6 +359,16 @@ def grid_wprojection_learned(ctx, mlp, uvgrid, grid_size, theta, vis, flags=RG_G
     vs = vis.struct()
     _check(lib().rg_grid_wprojection_learned(ctx.handle, mlp.handle, _ptr(uvgrid), int(grid_size),
                                              float(theta), ct.byref(vs), int(flags)))
+    return uvgrid
+
+
+def grid_wtowers_learned(ctx, mlp, uvgrid, grid_size, theta, vis, subgrid_size, subgrid_margin, wincrement,
+                         flags=RG_GRID_ACCUMULATE):
+    """W-towers with the learned kernel (rg_grid_wtowers_learned)."""
+    vs = vis.struct()
+    _check(lib().rg_grid_wtowers_learned(ctx.handle, mlp.handle, _ptr(uvgrid), int(grid_size), float(theta),
+                                         ct.byref(vs), int(subgrid_size), int(subgrid_margin), float(wincrement),
+                                         int(flags)))
     return uvgrid
 
 

@@ -471,6 +471,38 @@ __global__ void __launch_bounds__(256) mlp_eval_kernel(const float *__restrict__
 // ty); grid[idx] += vis * conj(tap) with the reference's linear index rule
 // (dropped outside [0, N^2)).  K = 16: two 128-row passes per visibility.
 // ---------------------------------------------------------------------------
+// One visibility: taps from the network in passes of IR rows, each scattered
+// as grid[goff + ty*ld + tx] += vis * conj(tap) where the index lies in
+// [0, limit).  All threads of the CTA take part (barriers inside).
+__device__ __forceinline__ void learned_scatter(InferSmem &S, const float *__restrict__ P,
+                                                const bf16 *__restrict__ PB, float wf, float du, float dv,
+                                                float vr, float vi, float2 *grid, int64_t goff, int64_t ld,
+                                                int64_t limit, int ksize, float inv_wmax, float scale)
+{
+    const int taps = ksize * ksize;
+    for (int t0 = 0; t0 < taps; t0 += IR) {
+        if (threadIdx.x < IR) {
+            const int t = t0 + threadIdx.x;
+            if (t < taps)
+                tap_features(wf, du, dv, (float)(t % ksize), (float)(t / ksize), ksize, inv_wmax,
+                             S.F + threadIdx.x * LDF);
+            else
+                for (int k = 0; k < MFIN; k++) S.F[threadIdx.x * LDF + k] = __float2bfloat16(0.f);
+        }
+        __syncthreads();
+        mlp_forward_rows(S, P, PB);
+        if (threadIdx.x < IR) {
+            const int t = t0 + threadIdx.x;
+            const float2 k = S.Y[threadIdx.x];
+            const float kr = k.x * scale, ki = k.y * scale;
+            const int64_t idx = goff + (int64_t)(t / ksize) * ld + (t % ksize);
+            if (t < taps && idx >= 0 && idx < limit)
+                atomicAdd(grid + idx, make_float2(vr * kr + vi * ki, vi * kr - vr * ki));
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void __launch_bounds__(256) learned_wproj_kernel(
     const double *__restrict__ u, const double *__restrict__ v, const double *__restrict__ w,
     const double2 *__restrict__ vis, int64_t nvis, int N, double theta, const float *__restrict__ P,
@@ -478,37 +510,39 @@ __global__ void __launch_bounds__(256) learned_wproj_kernel(
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     InferSmem &S = *reinterpret_cast<InferSmem *>(smem_raw);
-    const int taps = ksize * ksize;
-    const int64_t limit = (int64_t)N * N;
     for (int64_t i = blockIdx.x; i < nvis; i += gridDim.x) {
         const double x = theta * u[i], y = theta * v[i];
         const double cx = floor(x), cy = floor(y);
-        const float du = (float)(x - cx), dv = (float)(y - cy);
-        const float wf = (float)w[i];
         const double2 vz = vis[i];
-        const float vr = (float)vz.x, vi = (float)vz.y;
         const int64_t goff = ((int64_t)cy - ksize / 2 + N / 2) * N + ((int64_t)cx - ksize / 2 + N / 2);
-        for (int t0 = 0; t0 < taps; t0 += IR) {
-            if (threadIdx.x < IR) {
-                const int t = t0 + threadIdx.x;
-                if (t < taps)
-                    tap_features(wf, du, dv, (float)(t % ksize), (float)(t / ksize), ksize, inv_wmax,
-                                 S.F + threadIdx.x * LDF);
-                else
-                    for (int k = 0; k < MFIN; k++) S.F[threadIdx.x * LDF + k] = __float2bfloat16(0.f);
-            }
-            __syncthreads();
-            mlp_forward_rows(S, P, PB);
-            if (threadIdx.x < IR) {
-                const int t = t0 + threadIdx.x;
-                const float2 k = S.Y[threadIdx.x];
-                const float kr = k.x * scale, ki = k.y * scale;
-                const int64_t idx = goff + (int64_t)(t / ksize) * N + (t % ksize);
-                if (t < taps && idx >= 0 && idx < limit)
-                    atomicAdd(grid + idx, make_float2(vr * kr + vi * ki, vi * kr - vr * ki));
-            }
-            __syncthreads();
-        }
+        learned_scatter(S, P, PB, (float)w[i], (float)(x - cx), (float)(y - cy), (float)vz.x, (float)vz.y, grid,
+                        goff, N, (int64_t)N * N, ksize, inv_wmax, scale);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// W-towers with learned taps: the records of the tower binning (sub-grid slot
+// via slot_of_bin, footprint origin in the sub-grid) and the continuous
+// offsets feat = {w - w_mid, du, dv}; same scatter as above into the slot's
+// S x S sub-grid.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) learned_towers_kernel(
+    const int4 *__restrict__ rec, const float2 *__restrict__ visf, const float4 *__restrict__ feat, int64_t nvis,
+    const int *__restrict__ slot_of_bin, int slot_cap, float2 *__restrict__ slots, int sub,
+    const float *__restrict__ P, const bf16 *__restrict__ PB, int ksize, float inv_wmax, float scale)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    InferSmem &S = *reinterpret_cast<InferSmem *>(smem_raw);
+    const int64_t cells = (int64_t)sub * sub;
+    for (int64_t i = blockIdx.x; i < nvis; i += gridDim.x) {
+        const int4 r = rec[i];
+        if (r.x < 0) continue;  // uniform across the CTA
+        const int slot = slot_of_bin[r.x];
+        if (slot >= slot_cap) continue;
+        const float4 f = feat[i];
+        const float2 vz = visf[i];
+        learned_scatter(S, P, PB, f.x, f.y, f.z, vz.x, vz.y, slots + (int64_t)slot * cells, r.y, sub, cells, ksize,
+                        inv_wmax, scale);
     }
 }
 
@@ -545,6 +579,18 @@ void launch_mlp_eval(cudaStream_t s, const float *P, const void *PB, const float
     if (blocks > sm_count * 4) blocks = sm_count * 4;
     if (blocks < 1) blocks = 1;
     mlp_eval_kernel<<<blocks, 256, sm, s>>>(P, (const bf16 *)PB, in, n, ksize, inv_wmax, scale, out);
+}
+
+void launch_learned_towers(cudaStream_t s, const int4 *rec, const float2 *visf, const float4 *feat, int64_t n,
+                           const int *slot_of_bin, int slot_cap, float2 *slots, int subgrid, const float *P,
+                           const void *PB, int ksize, float inv_wmax, float scale, int sm_count)
+{
+    const size_t sm = sizeof(InferSmem);
+    cudaFuncSetAttribute(learned_towers_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    int64_t blocks = n < (int64_t)sm_count * 4 ? n : (int64_t)sm_count * 4;
+    if (blocks < 1) blocks = 1;
+    learned_towers_kernel<<<(unsigned)blocks, 256, sm, s>>>(rec, visf, feat, n, slot_of_bin, slot_cap, slots, subgrid,
+                                                            P, (const bf16 *)PB, ksize, inv_wmax, scale);
 }
 
 void launch_learned_wproj(cudaStream_t s, const double *u, const double *v, const double *w,

@@ -125,7 +125,7 @@ __global__ void prepare_towers_kernel(const double *__restrict__ u, const double
                                       int64_t n, TowerGeom g, const int *__restrict__ range,
                                       int4 *__restrict__ rec, float2 *__restrict__ visf,
                                       int *__restrict__ active, unsigned char *__restrict__ marks,
-                                      unsigned *err, unsigned long long *counters)
+                                      unsigned *err, unsigned long long *counters, float4 *__restrict__ feat)
 {
     if (!range[2]) return;  // more floors than the bin capacity: the caller reruns
     const int wp_min = range[0], nfloor = range[1];
@@ -179,18 +179,27 @@ __global__ void prepare_towers_kernel(const double *__restrict__ u, const double
             continue;
         }
         int cell_x, frac_x, cell_y, frac_y;
-        frac_axis(uu, bx.mid, g.theta, g.ov, half_over_ov, cell_x, frac_x);
-        frac_axis(vv, by.mid, g.theta, g.ov, half_over_ov, cell_y, frac_y);
         const double wmid = __dmul_rn((double)found_wp, g.winc);
         const double wr = __dsub_rn(ww, wmid);
-        const int plane = (int)floor(__dadd_rn(__ddiv_rn(__dsub_rn(wr, g.wk_wmin), g.wk_wstep), 0.5));
-        const int ks2 = g.ksize * g.ksize;
-        const long long tap = (long long)plane * g.ov * g.ov * ks2 +
-                              (long long)ks2 * (frac_y * g.ov + frac_x);
-        if (plane < 0 || plane >= g.planes || tap < 0 || tap + ks2 > taps_total) {
-            local_err |= DERR_PLANE_RANGE;
-            rec[i] = r;
-            continue;
+        long long tap = 0;
+        if (feat) {  // learned taps: continuous offsets, no table
+            const double x = __dmul_rn(g.theta, __dsub_rn(uu, bx.mid));
+            const double y = __dmul_rn(g.theta, __dsub_rn(vv, by.mid));
+            const double fx = floor(x), fy = floor(y);
+            cell_x = (int)fx;
+            cell_y = (int)fy;
+            feat[i] = make_float4((float)wr, (float)(x - fx), (float)(y - fy), 0.f);
+        } else {
+            frac_axis(uu, bx.mid, g.theta, g.ov, half_over_ov, cell_x, frac_x);
+            frac_axis(vv, by.mid, g.theta, g.ov, half_over_ov, cell_y, frac_y);
+            const int plane = (int)floor(__dadd_rn(__ddiv_rn(__dsub_rn(wr, g.wk_wmin), g.wk_wstep), 0.5));
+            const int ks2 = g.ksize * g.ksize;
+            tap = (long long)plane * g.ov * g.ov * ks2 + (long long)ks2 * (frac_y * g.ov + frac_x);
+            if (plane < 0 || plane >= g.planes || tap < 0 || tap + ks2 > taps_total) {
+                local_err |= DERR_PLANE_RANGE;
+                rec[i] = r;
+                continue;
+            }
         }
         const int col0 = cell_x + g.subgrid / 2 - g.ksize / 2;
         const int row0 = cell_y + g.subgrid / 2 - g.ksize / 2;
@@ -225,13 +234,13 @@ __global__ void prepare_towers_kernel(const double *__restrict__ u, const double
 void launch_prepare_towers(cudaStream_t s, const double *u, const double *v, const double *w,
                            const double2 *vis, int64_t n, TowerGeom g, const int *range,
                            int4 *rec, float2 *visf, int *active, unsigned char *marks, unsigned *err,
-                           unsigned long long *counters)
+                           unsigned long long *counters, float4 *feat)
 {
     int blocks = (int)((n + 255) / 256);
     if (blocks > 148 * 16) blocks = 148 * 16;
     if (blocks < 1) blocks = 1;
     prepare_towers_kernel<<<blocks, 256, 0, s>>>(u, v, w, vis, n, g, range, rec, visf, active, marks, err,
-                                                 counters);
+                                                 counters, feat);
 }
 
 __global__ void prepare_wproj_kernel(const double *__restrict__ u, const double *__restrict__ v,

@@ -427,11 +427,11 @@ namespace rg {
 // the live counts.  *overflow is set when a capacity was too small (the caller
 // grows the plan and runs again).
 static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *taps, const rg_wkern *wkern,
-                              double *out_dev, int N, double theta, int S, int M, double winc, int flags,
-                              TowerPlan &pl, bool *overflow)
+                              const LearnedTaps *lt, double *out_dev, int N, double theta, int S, int M,
+                              double winc, int flags, TowerPlan &pl, bool *overflow)
 {
     cudaStream_t st = ctx->stream;
-    const int K = wkern->size;
+    const int K = lt ? lt->ksize : wkern->size;
     const int chunk = S - M;
     const int nchunk = N / chunk + 1;
     const int ntowers = nchunk * nchunk;
@@ -452,6 +452,8 @@ static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *t
     RG_CHECK(scratch(ctx, "slot_masks", sizeof(unsigned) * (size_t)pl.slots_cap * mask_words(S), &masks));
     RG_CHECK(scratch(ctx, "rec", sizeof(int4) * (size_t)dv.n, &rec));
     RG_CHECK(scratch(ctx, "visf", sizeof(float2) * (size_t)dv.n, &visf));
+    void *feat = nullptr;
+    if (lt) RG_CHECK(scratch(ctx, "learned_feat", sizeof(float4) * (size_t)dv.n, &feat));
     RG_CHECK(scratch(ctx, "slot_of_bin", sizeof(int) * (size_t)nbins_cap, &slot_of_bin));
     RG_CHECK(scratch(ctx, "bin_of_slot", sizeof(int) * (size_t)nbins_cap, &bin_of_slot));
     RG_CHECK(scratch(ctx, "tower_first", sizeof(int) * (size_t)ntowers, &tfirst));
@@ -489,12 +491,12 @@ static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *t
     g.chunk = chunk;
     g.nchunk = nchunk;
     g.ksize = K;
-    g.ov = wkern->oversampling;
-    g.planes = wkern->plane_count;
+    g.ov = lt ? 1 : wkern->oversampling;
+    g.planes = lt ? 1 : wkern->plane_count;
     g.theta = theta;
     g.winc = winc;
-    g.wk_wmin = wkern->w_min;
-    g.wk_wstep = wkern->w_step;
+    g.wk_wmin = lt ? 0.0 : wkern->w_min;
+    g.wk_wstep = lt ? 1.0 : wkern->w_step;
 
     begin_stage(ctx, "w_range");
     launch_minmax_w(st, dv.u, dv.v, dv.w, dv.n, (double *)mm, d.err);
@@ -503,7 +505,7 @@ static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *t
     begin_stage(ctx, "prepare");
     if (dv.n > 0)
         launch_prepare_towers(st, dv.u, dv.v, dv.w, dv.vis, dv.n, g, range, (int4 *)rec, (float2 *)visf,
-                              (int *)active, (unsigned char *)marks, d.err, d.counters);
+                              (int *)active, (unsigned char *)marks, d.err, d.counters, (float4 *)feat);
     end_stage(ctx);
     begin_stage(ctx, "compact");
     launch_compact_bins(st, (const int *)active, range, (int *)slot_of_bin, (int *)bin_of_slot, counts,
@@ -518,11 +520,20 @@ static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *t
         end_stage(ctx);
         pl.zeroed_slots = (size_t)pl.slots_cap;
     }
-    begin_stage(ctx, "romein");
-    if (dv.n > 0)
-        launch_romein(st, (const int4 *)rec, (const float2 *)visf, dv.n, taps, (float2 *)slots,
-                      (const int *)slot_of_bin, sub_cells, S, K, ctx->sm_count, pl.slots_cap);
-    end_stage(ctx);
+    if (lt) {
+        begin_stage(ctx, "learned_gridding");
+        if (dv.n > 0)
+            launch_learned_towers(st, (const int4 *)rec, (const float2 *)visf, (const float4 *)feat, dv.n,
+                                  (const int *)slot_of_bin, pl.slots_cap, (float2 *)slots, S, lt->P, lt->PB,
+                                  lt->ksize, lt->inv_wmax, lt->scale, ctx->sm_count);
+        end_stage(ctx);
+    } else {
+        begin_stage(ctx, "romein");
+        if (dv.n > 0)
+            launch_romein(st, (const int4 *)rec, (const float2 *)visf, dv.n, taps, (float2 *)slots,
+                          (const int *)slot_of_bin, sub_cells, S, K, ctx->sm_count, pl.slots_cap);
+        end_stage(ctx);
+    }
     begin_stage(ctx, "fft_cols_backward");
     launch_slot_masks(st, (const unsigned char *)marks, (const int *)bin_of_slot, counts, pl.slots_cap, S,
                       (unsigned *)masks);
@@ -579,13 +590,10 @@ static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *t
     return RG_OK;
 }
 
-}  // namespace rg
-
-extern "C" {
-
-rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double theta,
-                          const rg_vis *vis, const rg_wkern *wkern, int subgrid_size,
-                          int subgrid_margin, double wincrement, int flags)
+// W-towers with table taps (lt == nullptr) or learned taps (wkern unused).
+rg_status grid_wtowers_impl(rg_context *ctx, double *uvgrid, int grid_size, double theta, const rg_vis *vis,
+                            const rg_wkern *wkern, const LearnedTaps *lt, int subgrid_size, int subgrid_margin,
+                            double wincrement, int flags)
 {
     if (!ctx || !uvgrid) return fail(RG_ERR_INVALID_ARGUMENT, "ctx and uvgrid must be non-NULL");
     if (grid_size < 2 || grid_size > 16384) return fail(RG_ERR_UNSUPPORTED, "grid_size must be in [2, 16384]");
@@ -593,8 +601,10 @@ rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double
     if (!(wincrement > 0.0) || !std::isfinite(wincrement))
         return fail(RG_ERR_INVALID_ARGUMENT, "wincrement must be > 0");
     RG_CHECK(check_vis(vis));
-    RG_CHECK(check_wkern(wkern));
-    const int S = subgrid_size, M = subgrid_margin, K = wkern->size;
+    if (!lt) RG_CHECK(check_wkern(wkern));
+    const int S = subgrid_size, M = subgrid_margin, K = lt ? lt->ksize : wkern->size;
+    if (lt && wincrement / 2 > lt->wmax)
+        return fail(RG_ERR_INVALID_ARGUMENT, "the learned kernel's w range is narrower than wincrement / 2");
     // src/reference/grid.c:300-302
     if (M < K) return fail(RG_ERR_INVALID_ARGUMENT, "subgrid margin must be >= the kernel support");
     if (S % 2 || M % 2) return fail(RG_ERR_INVALID_ARGUMENT, "subgrid size and margin must be even");
@@ -610,16 +620,16 @@ rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double
     DevVis dv;
     begin_stage(ctx, "stage_in");
     RG_CHECK(stage_vis(ctx, vis, &dv));
-    float2 *taps;
-    RG_CHECK(stage_taps(ctx, wkern, &taps));
+    float2 *taps = nullptr;
+    if (!lt) RG_CHECK(stage_taps(ctx, wkern, &taps));
     OutView ov;
     RG_CHECK(out_view(ctx, uvgrid, sizeof(double2) * (size_t)cells, "out_grid",
                       !(flags & RG_GRID_OVERWRITE), &ov));
     end_stage(ctx);
 
     char keybuf[200];
-    std::snprintf(keybuf, sizeof(keybuf), "%d_%d_%d_%.17g_%.17g_%lld", N, S, M, theta, wincrement,
-                  (long long)dv.n);
+    std::snprintf(keybuf, sizeof(keybuf), "%d_%d_%d_%.17g_%.17g_%lld_%c", N, S, M, theta, wincrement,
+                  (long long)dv.n, lt ? 'L' : 'T');
     TowerPlan &pl = ctx->tower_plans[keybuf];
     if (!pl.valid) {  // first call for this shape: generous capacities, learn the real sizes
         pl.floors_cap = 256;
@@ -631,7 +641,7 @@ rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double
     // checks the live counts), so it can simply be rerun with larger ones.
     for (int attempt = 0; attempt < 4; attempt++) {
         bool overflow = false;
-        RG_CHECK(wtowers_pass(ctx, dv, taps, wkern, (double *)ov.dev, N, theta, S, M, wincrement, flags, pl,
+        RG_CHECK(wtowers_pass(ctx, dv, taps, wkern, lt, (double *)ov.dev, N, theta, S, M, wincrement, flags, pl,
                               &overflow));
         if (!overflow) break;
         if (attempt == 3) return fail(RG_ERR_UNSUPPORTED, "W-towers capacities could not be sized");
@@ -654,6 +664,18 @@ rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double
     collect_timings(ctx);
     ctx->stats[5] = ctx->launches;
     return RG_OK;
+}
+
+}  // namespace rg
+
+extern "C" {
+
+rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double theta,
+                          const rg_vis *vis, const rg_wkern *wkern, int subgrid_size,
+                          int subgrid_margin, double wincrement, int flags)
+{
+    return rg::grid_wtowers_impl(ctx, uvgrid, grid_size, theta, vis, wkern, nullptr, subgrid_size, subgrid_margin,
+                                 wincrement, flags);
 }
 
 rg_status rg_weight(rg_context *ctx, int grid_size, double theta, const rg_vis *vis, double *vis_out)

@@ -50,18 +50,17 @@ struct Buffer {
     size_t bytes = 0;
 };
 
-// k_mlp.cu — learned w-kernel
-int mlp_param_count();
-int mlp_bf16_count();
-void launch_mlp_grad(cudaStream_t s, const float *P, const void *PB, const float *in, const float2 *target,
-                     int n, int ksize, float inv_wmax, float inv_scale, float *grad, float *loss);
-void launch_mlp_adam(cudaStream_t s, float *P, void *PB, float *grad, float *m, float *v, float lr, int step);
-void launch_mlp_to_bf16(cudaStream_t s, const float *P, void *PB);
-void launch_mlp_eval(cudaStream_t s, const float *P, const void *PB, const float *in, int n, int ksize,
-                     float inv_wmax, float scale, float2 *out, int sm_count);
-void launch_learned_wproj(cudaStream_t s, const double *u, const double *v, const double *w,
-                          const double2 *vis, int64_t n, int N, double theta, const float *P, const void *PB,
-                          int ksize, float inv_wmax, float scale, float2 *grid, int sm_count);
+// Learned taps for the W-towers gridder (the network of an rg_mlp).
+struct LearnedTaps {
+    const float *P;
+    const void *PB;
+    int ksize;
+    float inv_wmax, scale;
+    double wmax;
+};
+rg_status grid_wtowers_impl(rg_context *ctx, double *uvgrid, int grid_size, double theta, const rg_vis *vis,
+                            const rg_wkern *wkern, const LearnedTaps *lt, int subgrid_size, int subgrid_margin,
+                            double wincrement, int flags);
 
 }  // namespace rg
 
@@ -160,10 +159,13 @@ void launch_w_floors(cudaStream_t s, const double *wrange, double winc, int floo
 // marked strips are ever non-zero, so the column transforms and the row stage
 // touch only them.
 constexpr int kStripCols = 8;
+// feat == nullptr: table taps (frac_coord cells and oversampled sub-cell
+// indices, the reference's).  feat != nullptr: learned taps — cell = floor(x)
+// with the continuous offsets feat[i] = {w - w_mid, du, dv, 0}; no table.
 void launch_prepare_towers(cudaStream_t s, const double *u, const double *v, const double *w,
                            const double2 *vis, int64_t n, TowerGeom g, const int *range,
                            int4 *rec, float2 *visf, int *active, unsigned char *marks, unsigned *err,
-                           unsigned long long *counters);
+                           unsigned long long *counters, float4 *feat = nullptr);
 void launch_prepare_wproj(cudaStream_t s, const double *u, const double *v, const double *w,
                           const double2 *vis, int64_t n, int grid_size, double theta,
                           int ksize, int ov, int planes, double wk_wmin, double wk_wstep,
@@ -235,5 +237,11 @@ void launch_mlp_eval(cudaStream_t s, const float *P, const void *PB, const float
 void launch_learned_wproj(cudaStream_t s, const double *u, const double *v, const double *w,
                           const double2 *vis, int64_t n, int N, double theta, const float *P, const void *PB,
                           int ksize, float inv_wmax, float scale, float2 *grid, int sm_count);
+// W-towers with learned taps: per record, taps from the network at the
+// visibility's continuous (w - w_mid, du, dv) (feat), scattered into its slot's
+// sub-grid with the linear index rule of the table gridder.
+void launch_learned_towers(cudaStream_t s, const int4 *rec, const float2 *visf, const float4 *feat, int64_t n,
+                           const int *slot_of_bin, int slot_cap, float2 *slots, int subgrid, const float *P,
+                           const void *PB, int ksize, float inv_wmax, float scale, int sm_count);
 
 }  // namespace rg

@@ -255,4 +255,20 @@ rg_status rg_grid_wprojection_learned(rg_context *ctx, rg_mlp *mlp, double *uvgr
     return RG_OK;
 }
 
+rg_status rg_grid_wtowers_learned(rg_context *ctx, rg_mlp *mlp, double *uvgrid, int grid_size, double theta,
+                                  const rg_vis *vis, int subgrid_size, int subgrid_margin, double wincrement,
+                                  int flags)
+{
+    RG_CHECK(check_mlp(ctx, mlp));
+    LearnedTaps lt;
+    lt.P = mlp->P;
+    lt.PB = mlp->PB;
+    lt.ksize = mlp->ksize;
+    lt.inv_wmax = (float)(1.0 / mlp->wmax);
+    lt.scale = (float)mlp->out_scale;
+    lt.wmax = mlp->wmax;
+    return grid_wtowers_impl(ctx, uvgrid, grid_size, theta, vis, nullptr, &lt, subgrid_size, subgrid_margin,
+                             wincrement, flags);
+}
+
 }  // extern "C"

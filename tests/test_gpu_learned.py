@@ -94,3 +94,39 @@ def test_learned_gridder_matches_cpu_evaluation(rg, ctx, MO):
         r0, c0 = int(cy) - K // 2 + n // 2, int(cx) - K // 2 + n // 2
         ref[r0:r0 + K, c0:c0 + K] += vis[i] * np.conj(tap)
     assert np.linalg.norm(g - ref) / np.linalg.norm(ref) < 3e-2
+
+
+def test_learned_wtowers_equals_table_wtowers_on_the_lattice(rg, ctx, MO):
+    """W-towers with learned taps against W-towers with a table made from the
+    same network.  With theta = 1/8, integer u, v and w on the table planes,
+    every visibility's offsets fall exactly on the 8x oversampling lattice, so
+    the table's nearest sub-cell/plane lookup and the network's continuous
+    evaluation see the same inputs and the two grids agree to the gridders'
+    atomic-ordering noise — the learned path is the table pipeline with only
+    the taps replaced."""
+    from types import SimpleNamespace
+    rng = np.random.default_rng(11)
+    K, ov, th, n, S, M, winc = 8, 8, 0.125, 256, 128, 16, 5.0
+    planes = np.arange(-2.0, 3.0)
+    mlp = rg.LearnedKernel(ctx, K, 4.0, 0.05)
+    mlp.set_params(MO.pack(MO.init_params(12)).astype(np.float32) * 0.5)
+    # table[p][yf][xf][ty][tx] = network(w_p, xf/ov, yf/ov, tx, ty)
+    P_, YF, XF, TY, TX = np.meshgrid(np.arange(5), np.arange(ov), np.arange(ov), np.arange(K), np.arange(K),
+                                      indexing="ij")
+    taps = mlp.eval(rg.LearnedKernel.samples(planes[P_].ravel(), XF.ravel() / ov, YF.ravel() / ov,
+                                             TX.ravel(), TY.ravel()))
+    table = SimpleNamespace(data=taps.reshape(5, ov, ov, K, K), w_min=-2.0, w_step=1.0)
+    nv = 3000
+    u = rng.integers(-900, 900, nv).astype(np.float64)
+    v = rng.integers(-900, 900, nv).astype(np.float64)
+    w = rng.integers(-8, 9, nv) * winc + rng.integers(-2, 3, nv)
+    vis = rng.normal(size=nv) + 1j * rng.normal(size=nv)
+    V = rg.Visibilities(u, v, w.astype(np.float64), vis)
+    g_table = np.zeros((n, n), np.complex128)
+    ctx.grid_wtowers(g_table, n, th, V, table, S, M, winc)
+    g_learned = np.zeros((n, n), np.complex128)
+    rg.grid_wtowers_learned(ctx, mlp, g_learned, n, th, V, S, M, winc)
+    assert np.abs(g_table).max() > 0
+    assert np.linalg.norm(g_learned - g_table) / np.linalg.norm(g_table) < 1e-5
+    with pytest.raises(rg.RGError):  # network w range narrower than winc / 2
+        rg.grid_wtowers_learned(ctx, mlp, g_learned, n, th, V, S, M, 10.0)
