@@ -95,7 +95,9 @@ const char *rg_last_error(void);
  * (cf. the per-baseline check at src/reference/grid.c:519-530), 5 kernel
  * launches issued by the call; W-towers only: 6 sub-grid column strips of 8
  * columns holding data (the strips the transforms touch), 7 floor groups of
- * the row stage.
+ * the row stage, 8 Romein grid points per thread and 9 row-stage work items
+ * per SM in use (the tuned schedule), 10 one when the pass ran as a captured
+ * graph.
  * Returns the count written (<= n). */
 int rg_last_stats(rg_context *ctx, int64_t *out, int n);
 
@@ -105,6 +107,21 @@ int rg_last_stats(rg_context *ctx, int64_t *out, int n);
  * the stage names and milliseconds of the last call (count written). */
 rg_status rg_context_set_profiling(rg_context *ctx, int enabled);
 int rg_last_timings(rg_context *ctx, const char **names, float *ms, int n);
+
+/* W-towers schedules (no counterpart in the reference, whose launch shapes are
+ * fixed, src/grid/grid_cuda.cu:241-280 and :665-666).
+ * Autotuning (default on): the first call of a shape (grid size, sub-grid,
+ * margin, w increment, visibility count, table or learned taps) times whole
+ * passes into a scratch grid over the Romein points-per-thread and row-stage
+ * group-size choices and keeps the fastest for that shape; the caller's grid
+ * is written by an ordinary pass before tuning.
+ * Graph replay (default on): when the visibilities and the output grid are
+ * the caller's device buffers and profiling is off, the second and later calls
+ * of a tuned shape with the same buffers launch the whole pass as one captured
+ * CUDA graph; new buffer addresses or data that outgrow the sized capacities
+ * fall back to ordinary launches and capture again. */
+rg_status rg_context_set_autotune(rg_context *ctx, int enabled);
+rg_status rg_context_set_graphs(rg_context *ctx, int enabled);
 
 /* ---- gridders ---------------------------------------------------------- */
 

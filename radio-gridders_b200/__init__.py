@@ -37,7 +37,8 @@ STATUS = {0: "RG_OK", 1: "RG_ERR_INVALID_ARGUMENT", 2: "RG_ERR_CUDA", 3: "RG_ERR
 # every symbol include/radio_gridders.h declares
 EXPORTS = [
     "rg_context_create", "rg_context_destroy", "rg_context_set_stream", "rg_last_error",
-    "rg_last_stats", "rg_context_set_profiling", "rg_last_timings", "rg_grid_wprojection", "rg_grid_wtowers", "rg_weight",
+    "rg_last_stats", "rg_context_set_profiling", "rg_context_set_autotune", "rg_context_set_graphs",
+    "rg_last_timings", "rg_grid_wprojection", "rg_grid_wtowers", "rg_weight",
     "rg_make_hermitian", "rg_fft_shift", "rg_image_from_grid", "rg_fft2d", "rg_dft_image",
     "rg_grid_wprojection_noalloc", "rg_mlp_param_count", "rg_mlp_create", "rg_mlp_destroy",
     "rg_mlp_set_params", "rg_mlp_get_params", "rg_mlp_gradient", "rg_mlp_train", "rg_mlp_eval",
@@ -97,6 +98,8 @@ def lib():
         L.rg_last_stats.argtypes = [vp, ct.POINTER(i64), i]
         L.rg_last_stats.restype = i
         L.rg_context_set_profiling.argtypes = [vp, i]
+        L.rg_context_set_autotune.argtypes = [vp, i]
+        L.rg_context_set_graphs.argtypes = [vp, i]
         L.rg_last_timings.argtypes = [vp, ct.POINTER(ct.c_char_p), ct.POINTER(ct.c_float), i]
         L.rg_last_timings.restype = i
         L.rg_grid_wprojection.argtypes = [vp, vp, i, d, ct.POINTER(_Vis), ct.POINTER(_WKern), i]
@@ -211,6 +214,12 @@ class Context:
     def set_stream(self, stream_ptr):
         _check(lib().rg_context_set_stream(self._h, stream_ptr))
 
+    def set_autotune(self, enabled=True):
+        _check(lib().rg_context_set_autotune(self._h, int(bool(enabled))))
+
+    def set_graphs(self, enabled=True):
+        _check(lib().rg_context_set_graphs(self._h, int(bool(enabled))))
+
     def set_profiling(self, enabled=True):
         _check(lib().rg_context_set_profiling(self._h, 1 if enabled else 0))
 
@@ -222,10 +231,10 @@ class Context:
         return [(names[k].decode(), float(ms[k])) for k in range(n)]
 
     def last_stats(self):
-        out = (ct.c_int64 * 8)()
-        n = lib().rg_last_stats(self._h, out, 8)
+        out = (ct.c_int64 * 11)()
+        n = lib().rg_last_stats(self._h, out, 11)
         keys = ["gridded", "active_subgrids", "towers_with_data", "floors", "dropped", "launches",
-                "marked_strips", "floor_groups"]
+                "marked_strips", "floor_groups", "romein_points", "group_items_per_sm", "graph"]
         return {k: int(out[j]) for j, k in enumerate(keys[:n])}
 
     # ---- gridders (src/reference/grid.h:121-126) -------------------------

@@ -30,8 +30,17 @@ namespace rg {
 // decoded once for P taps.  A visibility whose sub-grid, linear origin and
 // origin residues equal the previous one's (about half of them along a track)
 // skips the per-point change tests: all of the thread's points are unchanged.
+// Occupancy floor for the register allocator: 48 resident warps per SM (24
+// with eight points per thread), at most 32 CTAs.
 template <int K, int P>
-__global__ void __launch_bounds__(K *K / P, 1536 / (K * K / P)) romein_kernel(
+struct RomeinBounds {
+    static constexpr int NT = K * K / P;
+    static constexpr int want = (P >= 8 ? 768 : 1536) / NT;
+    static constexpr int min_ctas = want > 32 ? 32 : (want < 1 ? 1 : want);
+};
+
+template <int K, int P>
+__global__ void __launch_bounds__(K *K / P, (RomeinBounds<K, P>::min_ctas)) romein_kernel(
     const int4 *__restrict__ rec, const float2 *__restrict__ visf, int64_t n,
     const float2 *__restrict__ taps, float2 *__restrict__ grids,
     const int *__restrict__ slot_of_bin, int64_t grid_stride, int side, int64_t chunk, int slot_cap)
@@ -143,15 +152,29 @@ static void romein_launch(cudaStream_t s, const int4 *rec, const float2 *visf, i
 
 void launch_romein(cudaStream_t s, const int4 *rec, const float2 *visf, int64_t n,
                    const float2 *taps, float2 *grids, const int *slot_of_bin, int64_t grid_stride,
-                   int grid_side, int ksize, int sm_count, int slot_cap)
+                   int grid_side, int ksize, int sm_count, int slot_cap, int points)
 {
+#define RG_ROMEIN(K, P) \
+    romein_launch<K, P>(s, rec, visf, n, taps, grids, slot_of_bin, grid_stride, grid_side, sm_count, slot_cap)
     switch (ksize) {
-        case 4: romein_launch<4, 1>(s, rec, visf, n, taps, grids, slot_of_bin, grid_stride, grid_side, sm_count, slot_cap); break;
-        case 8: romein_launch<8, 2>(s, rec, visf, n, taps, grids, slot_of_bin, grid_stride, grid_side, sm_count, slot_cap); break;
-        case 16: romein_launch<16, 4>(s, rec, visf, n, taps, grids, slot_of_bin, grid_stride, grid_side, sm_count, slot_cap); break;
-        case 32: romein_launch<32, 4>(s, rec, visf, n, taps, grids, slot_of_bin, grid_stride, grid_side, sm_count, slot_cap); break;
+        case 4: RG_ROMEIN(4, 1); break;
+        case 8:
+            if (points == 1) RG_ROMEIN(8, 1);
+            else if (points == 4) RG_ROMEIN(8, 4);
+            else RG_ROMEIN(8, 2);
+            break;
+        case 16:
+            if (points == 2) RG_ROMEIN(16, 2);
+            else if (points == 8) RG_ROMEIN(16, 8);
+            else RG_ROMEIN(16, 4);
+            break;
+        case 32:
+            if (points == 8) RG_ROMEIN(32, 8);
+            else RG_ROMEIN(32, 4);
+            break;
         default: break;
     }
+#undef RG_ROMEIN
 }
 
 }  // namespace rg

@@ -61,6 +61,7 @@ rg_status scratch(rg_context *ctx, const char *name, size_t bytes, void **out)
             want = bytes;
         }
         b.bytes = want;
+        ctx->scratch_gen++;
     }
     *out = b.ptr;
     return RG_OK;
@@ -182,6 +183,7 @@ struct DevVis {
     const double *u, *v, *w;
     const double2 *vis;
     int64_t n;
+    bool device = false;  // every array is the caller's own device buffer (nothing staged)
 };
 
 static rg_status stage_vis(rg_context *ctx, const rg_vis *vis, DevVis *dv)
@@ -197,6 +199,7 @@ static rg_status stage_vis(rg_context *ctx, const rg_vis *vis, DevVis *dv)
     RG_CHECK(stage_in(ctx, vis->vis, 2 * b, "in_vis", &p));
     dv->vis = (const double2 *)p;
     dv->n = vis->n;
+    dv->device = dv->u == vis->u && dv->v == vis->v && dv->w == vis->w && (const void *)dv->vis == vis->vis;
     return RG_OK;
 }
 
@@ -298,6 +301,12 @@ rg_status rg_context_create(int device, rg_context **out)
         return fail(RG_ERR_CUDA, "cudaStreamCreate failed");
     }
     ctx->stream = ctx->own_stream;
+    if (cudaMallocHost(&ctx->pinned, 256) != cudaSuccess) {
+        cudaGetLastError();
+        cudaStreamDestroy(ctx->own_stream);
+        delete ctx;
+        return fail(RG_ERR_OUT_OF_MEMORY, "pinned host allocation failed");
+    }
     *out = ctx;
     return RG_OK;
 }
@@ -307,8 +316,11 @@ rg_status rg_context_destroy(rg_context *ctx)
     if (!ctx) return RG_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    for (auto &kv : ctx->tower_plans)
+        if (kv.second.graph_exec) cudaGraphExecDestroy(kv.second.graph_exec);
     for (auto &kv : ctx->scratch)
         if (kv.second.ptr) cudaFree(kv.second.ptr);
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
     for (auto &e : ctx->events) {
         cudaEventDestroy(e.start);
         cudaEventDestroy(e.stop);
@@ -322,6 +334,20 @@ rg_status rg_context_set_stream(rg_context *ctx, void *stream)
 {
     if (!ctx) return fail(RG_ERR_INVALID_ARGUMENT, "ctx is NULL");
     ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    return RG_OK;
+}
+
+rg_status rg_context_set_autotune(rg_context *ctx, int enabled)
+{
+    if (!ctx) return fail(RG_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    ctx->autotune = enabled != 0;
+    return RG_OK;
+}
+
+rg_status rg_context_set_graphs(rg_context *ctx, int enabled)
+{
+    if (!ctx) return fail(RG_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    ctx->use_graphs = enabled != 0;
     return RG_OK;
 }
 
@@ -348,7 +374,7 @@ int rg_last_timings(rg_context *ctx, const char **names, float *ms, int n)
 int rg_last_stats(rg_context *ctx, int64_t *out, int n)
 {
     if (!ctx || !out) return 0;
-    int k = n < 8 ? n : 8;
+    int k = n < 11 ? n : 11;
     for (int i = 0; i < k; i++) out[i] = ctx->stats[i];
     return k;
 }
@@ -426,9 +452,13 @@ namespace rg {
 // waiting; one read-back at the end returns the error word, the counters and
 // the live counts.  *overflow is set when a capacity was too small (the caller
 // grows the plan and runs again).
-static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *taps, const rg_wkern *wkern,
-                              const LearnedTaps *lt, double *out_dev, int N, double theta, int S, int M,
-                              double winc, int flags, TowerPlan &pl, bool *overflow)
+// Enqueues one W-towers pass on ctx->stream, ending with the copy of the
+// diagnostics block (error word, counters, counts, floor range) into the
+// context's pinned host buffer; wtowers_check reads it after a sync.  Nothing
+// here synchronises, so the sequence can also be captured into a CUDA graph.
+static rg_status wtowers_enqueue(rg_context *ctx, const DevVis &dv, const float2 *taps, const rg_wkern *wkern,
+                                 const LearnedTaps *lt, double *out_dev, int N, double theta, int S, int M,
+                                 double winc, int flags, TowerPlan &pl)
 {
     cudaStream_t st = ctx->stream;
     const int K = lt ? lt->ksize : wkern->size;
@@ -509,7 +539,8 @@ static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *t
     end_stage(ctx);
     begin_stage(ctx, "compact");
     launch_compact_bins(st, (const int *)active, range, (int *)slot_of_bin, (int *)bin_of_slot, counts,
-                        (int *)tfirst, (int *)tcount, ntowers, tower_row_strips(S), 8 * ctx->sm_count, (int *)gbegin,
+                        (int *)tfirst, (int *)tcount, ntowers, tower_row_strips(S), pl.tune.group_items * ctx->sm_count,
+                        (int *)gbegin,
                         (int *)gend, (int *)tgfirst, (int *)tgcount);
     end_stage(ctx);
     // Sub-grids are left zeroed by the previous pass's column stage; only
@@ -531,7 +562,8 @@ static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *t
         begin_stage(ctx, "romein");
         if (dv.n > 0)
             launch_romein(st, (const int4 *)rec, (const float2 *)visf, dv.n, taps, (float2 *)slots,
-                          (const int *)slot_of_bin, sub_cells, S, K, ctx->sm_count, pl.slots_cap);
+                          (const int *)slot_of_bin, sub_cells, S, K, ctx->sm_count, pl.slots_cap,
+                          pl.tune.romein_points);
         end_stage(ctx);
     }
     begin_stage(ctx, "fft_cols_backward");
@@ -558,10 +590,15 @@ static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *t
     ctx->launches += 11;  // minmax, floors, prepare, compact, romein, masks, cols, rows, finish, cols, add-back
     RG_CHECK(check_launch("W-towers pass"));
 
-    // single read-back: error word, counters, counts, range
-    unsigned char host[64];
-    RG_CUDA(cudaMemcpyAsync(host, d.err, 64, cudaMemcpyDeviceToHost, st));
-    RG_CUDA(cudaStreamSynchronize(st));
+    RG_CUDA(cudaMemcpyAsync(ctx->pinned, d.err, 64, cudaMemcpyDeviceToHost, st));
+    return RG_OK;
+}
+
+// After the stream has passed a wtowers_enqueue: capacities seen, overflow,
+// input errors and the call statistics.
+static rg_status wtowers_check(rg_context *ctx, TowerPlan &pl, bool *overflow)
+{
+    const unsigned char *host = (const unsigned char *)ctx->pinned;
     unsigned err;
     unsigned long long ctr[2];
     int cnt[4], rng[3];
@@ -587,7 +624,118 @@ static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *t
     ctx->stats[4] = (int64_t)ctr[1];
     ctx->stats[6] = cnt[3];
     ctx->stats[7] = cnt[1];
+    ctx->stats[8] = pl.tune.romein_points;
+    ctx->stats[9] = pl.tune.group_items;
     return RG_OK;
+}
+
+static rg_status wtowers_pass(rg_context *ctx, const DevVis &dv, const float2 *taps, const rg_wkern *wkern,
+                              const LearnedTaps *lt, double *out_dev, int N, double theta, int S, int M,
+                              double winc, int flags, TowerPlan &pl, bool *overflow)
+{
+    RG_CHECK(wtowers_enqueue(ctx, dv, taps, wkern, lt, out_dev, N, theta, S, M, winc, flags, pl));
+    RG_CUDA(cudaStreamSynchronize(ctx->stream));
+    return wtowers_check(ctx, pl, overflow);
+}
+
+// Autotuner: coordinate search over the pass's schedule knobs — Romein grid
+// points per thread (threads per CTA) and the row stage's floor-group size
+// (work items per SM) — timing whole passes with CUDA events into a scratch
+// grid.  Each candidate runs twice and the second run is timed.  The search
+// runs once per shape, after the capacities are sized; results are per plan.
+static rg_status wtowers_autotune(rg_context *ctx, const DevVis &dv, const float2 *taps, const rg_wkern *wkern,
+                                  const LearnedTaps *lt, int N, double theta, int S, int M, double winc,
+                                  TowerPlan &pl)
+{
+    const int K = lt ? lt->ksize : wkern->size;
+    void *tmp;
+    RG_CHECK(scratch(ctx, "tune_grid", sizeof(double2) * (size_t)N * N, &tmp));
+    cudaEvent_t e0, e1;
+    RG_CUDA(cudaEventCreate(&e0));
+    RG_CUDA(cudaEventCreate(&e1));
+    const bool prof = ctx->profiling;
+    ctx->profiling = false;
+    auto time_pass = [&](float *ms) -> rg_status {
+        bool overflow = false;
+        for (int rep = 0; rep < 2; rep++) {
+            RG_CUDA(cudaEventRecord(e0, ctx->stream));
+            RG_CHECK(wtowers_pass(ctx, dv, taps, wkern, lt, (double *)tmp, N, theta, S, M, winc, RG_GRID_OVERWRITE,
+                                  pl, &overflow));
+            RG_CUDA(cudaEventRecord(e1, ctx->stream));
+            RG_CUDA(cudaEventSynchronize(e1));
+            if (overflow) return fail(RG_ERR_UNSUPPORTED, "capacity overflow while tuning");
+        }
+        RG_CUDA(cudaEventElapsedTime(ms, e0, e1));
+        return RG_OK;
+    };
+    rg_status st = RG_OK;
+    TowerTuning best = pl.tune;
+    float best_ms = 1e30f;
+    if (!lt) {  // Romein variants (the learned gridder has no points-per-thread knob)
+        int cand[3], nc = 0;
+        if (K == 16) { cand[0] = 2; cand[1] = 4; cand[2] = 8; nc = 3; }
+        else if (K == 8) { cand[0] = 1; cand[1] = 2; cand[2] = 4; nc = 3; }
+        else if (K == 32) { cand[0] = 4; cand[1] = 8; nc = 2; }
+        for (int c = 0; c < nc && st == RG_OK; c++) {
+            pl.tune.romein_points = cand[c];
+            float ms = 0;
+            st = time_pass(&ms);
+            if (st == RG_OK && ms < best_ms) { best_ms = ms; best = pl.tune; }
+        }
+        pl.tune = best;
+    }
+    const int gcand[3] = {4, 8, 16};
+    for (int c = 0; c < 3 && st == RG_OK; c++) {
+        pl.tune.group_items = gcand[c];
+        float ms = 0;
+        st = time_pass(&ms);
+        if (st == RG_OK && ms < best_ms) { best_ms = ms; best = pl.tune; }
+    }
+    pl.tune = best;
+    pl.tuned = true;
+    ctx->profiling = prof;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return st;
+}
+
+// Graph replay of a whole pass: captured once per plan and set of device
+// buffers (inputs, taps, output), then launched as one graph per call.
+static void drop_graph(TowerPlan &pl)
+{
+    if (pl.graph_exec) cudaGraphExecDestroy(pl.graph_exec);
+    pl.graph_exec = nullptr;
+    pl.graph_key.clear();
+}
+
+// Capture failure is not an error of the call (its grid is already written):
+// the plan simply keeps using ordinary launches.
+static void capture_pass(rg_context *ctx, const DevVis &dv, const float2 *taps, const rg_wkern *wkern,
+                         const LearnedTaps *lt, double *out_dev, int N, double theta, int S, int M, double winc,
+                         int flags, TowerPlan &pl, const std::string &key)
+{
+    drop_graph(pl);
+    const uint64_t gen0 = ctx->scratch_gen;
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    const int launches0 = ctx->launches;
+    const rg_status st = wtowers_enqueue(ctx, dv, taps, wkern, lt, out_dev, N, theta, S, M, winc, flags, pl);
+    pl.graph_launches = ctx->launches - launches0;
+    ctx->launches = launches0;
+    const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+    cudaGetLastError();
+    if (st == RG_OK && e == cudaSuccess && graph && ctx->scratch_gen == gen0 &&
+        cudaGraphInstantiate(&pl.graph_exec, graph, 0) == cudaSuccess) {
+        pl.graph_key = key;
+        pl.graph_scratch_gen = ctx->scratch_gen;
+    } else {
+        cudaGetLastError();
+        pl.graph_exec = nullptr;
+    }
+    if (graph) cudaGraphDestroy(graph);
 }
 
 // W-towers with table taps (lt == nullptr) or learned taps (wkern unused).
@@ -637,9 +785,31 @@ rg_status grid_wtowers_impl(rg_context *ctx, double *uvgrid, int grid_size, doub
         pl.groups_cap = pl.slots_cap;
         pl.valid = true;
     }
+    // Graph replay when nothing is profiled and every buffer lives on the
+    // device: the same plan and the same buffers reuse one captured pass.
+    char gkey[256];
+    std::snprintf(gkey, sizeof(gkey), "%p_%p_%p_%p_%p_%p_%d", (const void *)dv.u, (const void *)dv.v,
+                  (const void *)dv.w, (const void *)dv.vis, (const void *)taps, (void *)ov.dev, flags);
+    const bool graphable = ctx->use_graphs && !ctx->profiling && dv.device && !ov.host;
+    bool done = false;
+    if (graphable && pl.graph_exec && pl.graph_key == gkey && pl.graph_scratch_gen == ctx->scratch_gen &&
+        ctx->slots_owner == &pl && pl.zeroed_slots >= (size_t)pl.slots_cap) {
+        RG_CUDA(cudaGraphLaunch(pl.graph_exec, ctx->stream));
+        RG_CUDA(cudaStreamSynchronize(ctx->stream));
+        bool overflow = false;
+        RG_CHECK(wtowers_check(ctx, pl, &overflow));
+        ctx->launches += pl.graph_launches;
+        ctx->stats[10] = 1;
+        if (overflow) {
+            drop_graph(pl);  // the data outgrew the plan: size it again eagerly
+            begin_call(ctx);
+        } else {
+            done = true;
+        }
+    }
     // A pass whose capacities overflow writes nothing to the grid (the add-back
     // checks the live counts), so it can simply be rerun with larger ones.
-    for (int attempt = 0; attempt < 4; attempt++) {
+    for (int attempt = 0; attempt < 4 && !done; attempt++) {
         bool overflow = false;
         RG_CHECK(wtowers_pass(ctx, dv, taps, wkern, lt, (double *)ov.dev, N, theta, S, M, wincrement, flags, pl,
                               &overflow));
@@ -650,13 +820,28 @@ rg_status grid_wtowers_impl(rg_context *ctx, double *uvgrid, int grid_size, doub
         pl.floors_cap = pl.seen_floors > pl.floors_cap ? pl.seen_floors + 8 : pl.floors_cap;
         pl.slots_cap = pl.seen_slots > pl.slots_cap ? pl.seen_slots + pl.seen_slots / 8 + 8 : pl.slots_cap;
         pl.groups_cap = pl.seen_groups > pl.groups_cap ? pl.seen_groups + pl.seen_groups / 8 + 8 : pl.groups_cap;
+        drop_graph(pl);
         begin_call(ctx);
     }
     // shrink a first-call guess to the sizes seen (keeps memory proportional)
-    if (pl.slots_cap > pl.seen_slots + pl.seen_slots / 4 + 64) {
+    if (!done && pl.slots_cap > pl.seen_slots + pl.seen_slots / 4 + 64) {
         pl.slots_cap = pl.seen_slots + pl.seen_slots / 8 + 8;
         pl.groups_cap = pl.seen_groups + pl.seen_groups / 8 + 8;
+        drop_graph(pl);
     }
+    if (!done && ctx->autotune && !pl.tuned && !ctx->profiling) {
+        int64_t keep[11];
+        std::memcpy(keep, ctx->stats, sizeof(keep));
+        const int launches = ctx->launches;
+        RG_CHECK(wtowers_autotune(ctx, dv, taps, wkern, lt, N, theta, S, M, wincrement, pl));
+        std::memcpy(ctx->stats, keep, sizeof(keep));
+        ctx->stats[8] = pl.tune.romein_points;
+        ctx->stats[9] = pl.tune.group_items;
+        ctx->launches = launches;
+        drop_graph(pl);
+    }
+    if (!done && graphable && (!ctx->autotune || pl.tuned) && pl.zeroed_slots >= (size_t)pl.slots_cap)
+        capture_pass(ctx, dv, taps, wkern, lt, (double *)ov.dev, N, theta, S, M, wincrement, flags, pl, gkey);
     begin_stage(ctx, "stage_out");
     RG_CHECK(finish_out(ctx, ov));
     end_stage(ctx);
@@ -667,6 +852,7 @@ rg_status grid_wtowers_impl(rg_context *ctx, double *uvgrid, int grid_size, doub
 }
 
 }  // namespace rg
+
 
 extern "C" {
 

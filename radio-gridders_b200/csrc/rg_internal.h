@@ -64,11 +64,23 @@ rg_status grid_wtowers_impl(rg_context *ctx, double *uvgrid, int grid_size, doub
 
 }  // namespace rg
 
+// Schedule knobs of a W-towers pass (picked by the autotuner).
+struct TowerTuning {
+    int romein_points = 4;  // grid points per Romein thread (threads per CTA = K^2 / points)
+    int group_items = 8;    // row-stage work items per SM (sets the floor-group size)
+};
+
 struct TowerPlan {
     bool valid = false;
     int floors_cap = 0, slots_cap = 0, groups_cap = 0;
     int seen_floors = 0, seen_slots = 0, seen_groups = 0;
     size_t zeroed_slots = 0;  // sub-grids known to be zero (cleared on consumption)
+    TowerTuning tune;
+    bool tuned = false;
+    cudaGraphExec_t graph_exec = nullptr;  // captured pass for graph_key's buffers
+    std::string graph_key;
+    int graph_launches = 0;
+    uint64_t graph_scratch_gen = 0;  // scratch generation the graph's pointers belong to
 };
 
 struct rg_stage_event {
@@ -88,8 +100,11 @@ struct rg_context {
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     std::map<std::string, rg::Buffer> scratch;
-    void *pinned = nullptr;  // small pinned host buffer for scalars
-    int64_t stats[8] = {0};
+    uint64_t scratch_gen = 0;  // bumped on every scratch (re)allocation: captured graphs go stale
+    void *pinned = nullptr;  // small pinned host buffer (diagnostics read-back)
+    bool autotune = true;    // tune W-towers schedules once per shape
+    bool use_graphs = true;  // replay W-towers passes as CUDA graphs
+    int64_t stats[11] = {0};
     int launches = 0;
 };
 
@@ -180,9 +195,11 @@ void launch_compact_bins(cudaStream_t s, const int *active, const int *range, in
 // k_romein.cu
 // Sub-grids with slot index >= slot_cap are skipped (capacity overflow: the
 // caller detects it from the slot count and reruns).
+// points: grid points per thread (0: the default for ksize).
 void launch_romein(cudaStream_t s, const int4 *rec, const float2 *visf, int64_t n,
                    const float2 *taps, float2 *grids, const int *slot_of_bin,
-                   int64_t grid_stride, int grid_side, int ksize, int sm_count, int slot_cap = 1);
+                   int64_t grid_stride, int grid_side, int ksize, int sm_count, int slot_cap = 1,
+                   int points = 0);
 
 // k_towers.cu
 void launch_fresnel_table(cudaStream_t s, double *ph, int subgrid, double theta, double winc);

@@ -1,7 +1,7 @@
 """Measurement studies beyond the headline benchmark: the DFT precision study
 and the image error of the W-towers gridder against the direct DFT.
 
-Run on a B200:  python radio-gridders_b200/studies.py [dft|towers|learned|all]
+Run on a B200:  python radio-gridders_b200/studies.py [dft|towers|towers_ov|learned|learned_towers|learned_towers_c4|all]
 Each study prints one JSON object."""
 from __future__ import annotations
 
@@ -95,6 +95,55 @@ def towers_image_error(ctx, oversampling=8, w_step=1.0):
             "region": "central half of each axis", "dft_s": time.time() - t0}
 
 
+def learned_towers(ctx, config="C1", steps=20000, n_triples=4096):
+    """Learned-kernel W-towers against the table W-towers on the same
+    workload: a network trained on the GPU (own forward/backward kernels) on
+    generator kernels over the residual w range |w - w_mid| <= winc/2, then
+    both gridders timed (CUDA events around the call, inputs in HBM) and both
+    images compared with the FP64-reduced DFT.  C1: 2048^2, S 512, margin 16,
+    winc 10, 2.09M vis; C4: 4096^2, S 512, margin 32, winc 20, 8.4M vis."""
+    import torch
+    if config == "C4":
+        obs, n, S, M, winc = _sim.wtowers_full(), 4096, 512, 32, 20.0
+    else:
+        obs, n, S, M, winc = _sim.wtowers_plain(), 2048, 512, 16, 10.0
+    th = 0.1
+    half = winc / 2
+    u, v, w, vis = obs.flat()
+    t0 = time.time()
+    mlp, losses = _learned.train(ctx, wmax=half + 1.0, theta=th, ksize=16, n_triples=n_triples, steps=steps,
+                                 batch=16384, lr_max=4e-3)
+    train_s = time.time() - t0
+    err, held = _learned.tap_error(mlp, wmax=half + 1.0, theta=th)
+    wk = _sim.generate_wkernel(th, np.arange(-half - 1.0, half + 1.5, 1.0), 16, 32)
+    table_err = _learned.table_tap_error(wk, held)
+    dev = torch.device("cuda", 0)
+    ctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+    V = _rg.Visibilities(*(torch.from_numpy(a).to(dev) for a in (u, v, w)), torch.from_numpy(vis).to(dev))
+    dwk = torch.from_numpy(np.ascontiguousarray(wk.data)).to(dev)
+    g = torch.zeros((n, n), dtype=torch.complex128, device=dev)
+    table_ms = _events_ms(lambda: ctx.grid_wtowers(g, n, th, V, wk, S, M, winc, flags=1, wkern_data=dwk))
+    img_t = ctx.image_from_grid(g.cpu().numpy(), taper_1d=_sim.taper_1d(th, n, wk.c))
+    learned_ms = _events_ms(lambda: _rg.grid_wtowers_learned(ctx, mlp, g, n, th, V, S, M, winc, flags=1),
+                            repeats=2)
+    img_l = ctx.image_from_grid(g.cpu().numpy(), taper_1d=_sim.taper_1d(th, n, wk.c))
+    t1 = time.time()
+    ref = ctx.dft_image(n, th, _rg.Visibilities(u, v, w, vis), _rg.RG_DFT_FP64_REDUCED, 2.0)
+    dft_s = time.time() - t1
+    t_rms, t_pk = _learned.image_errors(img_t, ref)
+    l_rms, l_pk = _learned.image_errors(img_l, ref)
+    ctx.set_stream(None)
+    return {"config": config, "n_vis": len(u), "grid_size": n, "subgrid": S, "margin": M, "winc": winc,
+            "train_s": train_s, "train_steps": steps, "final_loss": losses[-1],
+            "tap_err": err, "table_tap_err_ov32": table_err,
+            "table_ms": table_ms, "table_vis_per_s": len(u) / (table_ms * 1e-3),
+            "learned_ms": learned_ms, "learned_vis_per_s": len(u) / (learned_ms * 1e-3),
+            "learned_over_table_speed": table_ms / learned_ms,
+            "table_image_rms": t_rms, "table_image_peak": t_pk,
+            "learned_image_rms": l_rms, "learned_image_peak": l_pk, "dft_s": dft_s,
+            "region": "central half of each axis"}
+
+
 def main(which):
     ctx = _rg.Context(0)
     if which in ("dft", "all"):
@@ -112,6 +161,11 @@ def main(which):
         print(json.dumps({"study": "learned_wproj", "tap_err": err,
                           "table_tap_err": _learned.table_tap_error(wk, held),
                           "final_loss": losses[-1], **r}), flush=True)
+
+
+    if which in ("learned_towers", "learned_towers_c4"):
+        cfg = "C4" if which.endswith("c4") else "C1"
+        print(json.dumps({"study": "learned_towers", **learned_towers(ctx, cfg)}), flush=True)
 
 
 if __name__ == "__main__":
