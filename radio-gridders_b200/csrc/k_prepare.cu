@@ -32,7 +32,7 @@ __global__ void minmax_w_kernel(const double *__restrict__ u, const double *__re
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
         const double ww = w[i];
-        if (!finite3(u[i], v[i], ww)) {
+        if (!isfinite(ww)) {  // u and v are checked by the binning kernel
             bad = true;
             continue;
         }
@@ -133,6 +133,16 @@ __global__ void prepare_towers_kernel(const double *__restrict__ u, const double
     const int wp_max = wp_min + nfloor - 1;
     const int taps_total = g.planes * g.ov * g.ov * g.ksize * g.ksize;
     unsigned local_err = 0, gridded = 0, dropped = 0;
+    // tower bounds per chunk index, computed once per CTA (three FP64
+    // divisions each) when they fit; the per-visibility search reads them
+    constexpr int kBoundsCache = 256;
+    __shared__ Bounds sb[kBoundsCache];
+    const bool cached = g.nchunk <= kBoundsCache;
+    if (cached)
+        for (int c = threadIdx.x; c < g.nchunk; c += blockDim.x) sb[c] = tower_axis(c, g.chunk, g.grid_size, g.theta);
+    __syncthreads();
+    // first guesses only (the exact half-open tests below decide)
+    const double inv_chunk = 1.0 / (double)g.chunk, inv_winc = 1.0 / g.winc;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
         const double uu = u[i], vv = v[i], ww = w[i];
@@ -145,21 +155,21 @@ __global__ void prepare_towers_kernel(const double *__restrict__ u, const double
             continue;
         }
         const double half_n = (double)(g.grid_size / 2);
-        const int cxc = (int)floor((uu * g.theta + 0.5 + half_n) / g.chunk);
-        const int cyc = (int)floor((vv * g.theta + 0.5 + half_n) / g.chunk);
-        const int wpc = (int)floor(ww / g.winc + 0.5);
+        const int cxc = (int)floor((uu * g.theta + 0.5 + half_n) * inv_chunk);
+        const int cyc = (int)floor((vv * g.theta + 0.5 + half_n) * inv_chunk);
+        const int wpc = (int)floor(ww * inv_winc + 0.5);
         int found_cx = -1, found_cy = -1, found_wp = 0;
         Bounds bx, by;
         for (int cy = cyc - 1; cy <= cyc + 1 && found_cy < 0; cy++) {
             if (cy < 0 || cy >= g.nchunk) continue;
-            Bounds t = tower_axis(cy, g.chunk, g.grid_size, g.theta);
+            const Bounds t = cached ? sb[cy] : tower_axis(cy, g.chunk, g.grid_size, g.theta);
             if (vv < t.lo || vv >= t.hi) continue;
             found_cy = cy;
             by = t;
         }
         for (int cx = cxc - 1; cx <= cxc + 1 && found_cx < 0; cx++) {
             if (cx < 0 || cx >= g.nchunk) continue;
-            Bounds t = tower_axis(cx, g.chunk, g.grid_size, g.theta);
+            const Bounds t = cached ? sb[cx] : tower_axis(cx, g.chunk, g.grid_size, g.theta);
             if (uu < t.lo || uu >= t.hi) continue;
             found_cx = cx;
             bx = t;

@@ -31,6 +31,16 @@ void launch_fresnel_table(cudaStream_t s, double *ph, int subgrid, double theta,
     fresnel_table_kernel<<<blocks, 256, 0, s>>>(ph, subgrid, theta, winc);
 }
 
+// a / d for 0 <= a < 2^24, d > 0: float reciprocal estimate, corrected to the
+// exact quotient (saves the integer division sequence).
+__device__ __forceinline__ int div_nonneg(int a, int d, float inv)
+{
+    int q = __float2int_rz((float)a * inv);
+    if (q * d > a) q--;
+    else if ((q + 1) * d <= a) q++;
+    return q;
+}
+
 // Owner-computes add-back (src/reference/grid.c:503-516): every master pixel
 // sums, in tower order (cy, then cx), the overlapping towers' forward-
 // transformed sub-images divided by S^2, in FP64.  Deterministic.
@@ -46,9 +56,10 @@ __global__ void add_back_kernel(const float2 *__restrict__ subimg, const int *__
     if (gx >= N || gy >= N) return;
     if (range && (!range[2] || counts[0] > slot_cap || counts[1] > group_cap)) return;
     const int ax = gx + M / 2, ay = gy + M / 2;  // x + N/2 + M/2 with x = gx - N/2
-    int cx_hi = ax / chunk, cy_hi = ay / chunk;
-    int cx_lo = (ax - S) >= 0 ? (ax - S) / chunk + 1 : 0;
-    int cy_lo = (ay - S) >= 0 ? (ay - S) / chunk + 1 : 0;
+    const float inv = 1.0f / (float)chunk;
+    int cx_hi = div_nonneg(ax, chunk, inv), cy_hi = div_nonneg(ay, chunk, inv);
+    int cx_lo = (ax - S) >= 0 ? div_nonneg(ax - S, chunk, inv) + 1 : 0;
+    int cy_lo = (ay - S) >= 0 ? div_nonneg(ay - S, chunk, inv) + 1 : 0;
     if (cx_hi >= nchunk) cx_hi = nchunk - 1;
     if (cy_hi >= nchunk) cy_hi = nchunk - 1;
     const int64_t at = (int64_t)gy * N + gx;
