@@ -66,9 +66,11 @@ __global__ void minmax_w_kernel(const double *__restrict__ u, const double *__re
 void launch_minmax_w(cudaStream_t s, const double *u, const double *v, const double *w, int64_t n,
                      double *out2, unsigned *err)
 {
-    // out2 as bit patterns: [0] = -0.0 (min so far), [1] = +0.0
-    unsigned long long init[2] = {0x8000000000000000ull, 0ull};
-    cudaMemcpyAsync(out2, init, sizeof(init), cudaMemcpyHostToDevice, s);
+    // out2 as bit patterns, both starting at +0.0 (all-zero bits): the range
+    // always contains 0, and a negative minimum's pattern (sign bit set)
+    // compares above zero as an unsigned integer.  A device memset keeps the
+    // sequence free of host copies (it is replayed from a captured graph).
+    cudaMemsetAsync(out2, 0, 2 * sizeof(double), s);
     int blocks = (int)((n + 255) / 256);
     if (blocks > 4096) blocks = 4096;
     if (blocks < 1) blocks = 1;
@@ -127,7 +129,14 @@ __global__ void prepare_towers_kernel(const double *__restrict__ u, const double
                                       int *__restrict__ active, unsigned char *__restrict__ marks,
                                       unsigned *err, unsigned long long *counters, float4 *__restrict__ feat)
 {
-    if (!range[2]) return;  // more floors than the bin capacity: the caller reruns
+    if (!range[2]) {
+        // more floors than the bin capacity: the caller reruns.  Every record is
+        // marked dropped so the gridding kernels of this pass read none of the
+        // buffer's earlier contents.
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+            rec[i] = make_int4(-1, 0, 0, 0);
+        return;
+    }
     const int wp_min = range[0], nfloor = range[1];
     const double half_over_ov = 0.5 / (double)g.ov;
     const int wp_max = wp_min + nfloor - 1;

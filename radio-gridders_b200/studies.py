@@ -1,7 +1,7 @@
 """Measurement studies beyond the headline benchmark: the DFT precision study
 and the image error of the W-towers gridder against the direct DFT.
 
-Run on a B200:  python radio-gridders_b200/studies.py [dft|towers|towers_ov|learned|learned_towers|learned_towers_c4|all]
+Run on a B200:  python radio-gridders_b200/studies.py [dft|towers|towers_ov|learned|learned_towers|learned_towers_c4|parity_c1|parity_c4|all]
 Each study prints one JSON object."""
 from __future__ import annotations
 
@@ -144,6 +144,29 @@ def learned_towers(ctx, config="C1", steps=20000, n_triples=4096):
             "region": "central half of each axis"}
 
 
+def parity_full(ctx, config="C4"):
+    """Grid parity at full size against the CPU restatement of grid.c (which
+    the tests pin bit-identical to the reference's own grid.c): relative RMS of
+    the FP64 master grid.  C4: 4096^2, S 512, margin 32, winc 20, 8.37M vis."""
+    import oracle
+    if config == "C4":
+        obs, n, S, M, winc = _sim.wtowers_full(), 4096, 512, 32, 20.0
+    else:
+        obs, n, S, M, winc = _sim.wtowers_plain(), 2048, 512, 16, 10.0
+    th, half = 0.1, winc / 2
+    u, v, w, vis = obs.flat()
+    wk = _sim.generate_wkernel(th, np.arange(-half - 1.0, half + 1.5, 1.0), 16, 32)
+    g = np.zeros((n, n), np.complex128)
+    ctx.grid_wtowers(g, n, th, _rg.Visibilities(u, v, w, vis), wk, S, M, winc)
+    st = ctx.last_stats()
+    t0 = time.time()
+    ref = oracle.grid_wtowers(n, th, u, v, w, vis, wk, S, M, winc)
+    d = g - ref
+    return {"config": config, "n_vis": len(u), "grid_size": n, "active_subgrids": st["active_subgrids"],
+            "rel_rms": float(np.sqrt(np.mean(np.abs(d) ** 2) / np.mean(np.abs(ref) ** 2))),
+            "oracle_s": time.time() - t0}
+
+
 def main(which):
     ctx = _rg.Context(0)
     if which in ("dft", "all"):
@@ -163,6 +186,8 @@ def main(which):
                           "final_loss": losses[-1], **r}), flush=True)
 
 
+    if which in ("parity_c1", "parity_c4"):
+        print(json.dumps({"study": "parity_full", **parity_full(ctx, which[-2:].upper())}), flush=True)
     if which in ("learned_towers", "learned_towers_c4"):
         cfg = "C4" if which.endswith("c4") else "C1"
         print(json.dumps({"study": "learned_towers", **learned_towers(ctx, cfg)}), flush=True)
