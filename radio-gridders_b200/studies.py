@@ -1,7 +1,7 @@
 """Measurement studies beyond the headline benchmark: the DFT precision study
 and the image error of the W-towers gridder against the direct DFT.
 
-Run on a B200:  python radio-gridders_b200/studies.py [dft|towers|towers_ov|learned|learned_towers|learned_towers_c4|parity_c1|parity_c4|all]
+Run on a B200:  python radio-gridders_b200/studies.py [dft|towers|towers_ov|learned|learned_towers|learned_towers_c4|parity_c1|parity_c4|baselines|all]
 Each study prints one JSON object."""
 from __future__ import annotations
 
@@ -167,6 +167,92 @@ def parity_full(ctx, config="C4"):
             "oracle_s": time.time() - t0}
 
 
+def baselines(ctx):
+    """GPU against the reference's CPU code on the configurations C0, C2, C3,
+    C4 (C1 is bench.py's line).  GPU: CUDA events around whole calls, inputs
+    in HBM.  CPU: the reference's grid.c built from its sources (IEEE build,
+    one core, for W-projection; OpenMP build on all cores for W-towers, on the
+    baselines it can grid safely) and the OpenMP FP64 DFT oracle, each on a
+    bounded sample scaled to the metric's unit."""
+    import os
+    import torch
+    import oracle
+    cores = len(os.sched_getaffinity(0))
+    dev = torch.device("cuda", 0)
+    ctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+
+    def dV(u, v, w, vis):
+        return _rg.Visibilities(*(torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in (u, v, w)),
+                                torch.from_numpy(np.ascontiguousarray(vis)).to(dev))
+
+    out = {"host_cores": cores}
+    # C0: plain W-projection, 512^2, 22,464 vis
+    obs = _sim.wproj_plain()
+    u, v, w, vis = obs.flat()
+    n, th = obs.meta["grid_size"], obs.meta["theta"]
+    wk = _sim.wkernel_for(w, th, 10.0, size=16, oversampling=8)
+    g = torch.zeros((n, n), dtype=torch.complex128, device=dev)
+    dwk = torch.from_numpy(np.ascontiguousarray(wk.data)).to(dev)
+    V = dV(u, v, w, vis)
+    ms = _events_ms(lambda: ctx.grid_wprojection(g, n, th, V, wk, flags=1, wkern_data=dwk), repeats=5)
+    t0 = time.time()
+    oracle.ref_grid_wprojection(n, th, obs, wk)
+    cpu_s = time.time() - t0
+    img = ctx.image_from_grid(g.cpu().numpy(), taper_1d=_sim.taper_1d(th, n, wk.c))
+    ref = ctx.dft_image(n, th, _rg.Visibilities(u, v, w, vis), _rg.RG_DFT_FP64_REDUCED, 2.0)
+    rms, pk = _learned.image_errors(img, ref)
+    out["C0"] = {"n_vis": len(u), "gpu_ms": ms, "gpu_vis_per_s": len(u) / (ms * 1e-3), "cpu_s": cpu_s,
+                 "cpu_vis_per_s": len(u) / cpu_s, "cpu_cores": 1, "image_rms": rms, "image_peak": pk}
+    # C2: direct DFT, 1024^2 at theta 0.05, 200k vis; CPU on a 2,000-visibility sample
+    obs = _sim.dft_study(n_vis=200_000)
+    u, v, w, vis = (a[:200_000] for a in obs.flat())
+    th, n = obs.meta["theta"], 1024
+    img = torch.zeros((n, n), dtype=torch.float64, device=dev)
+    V = dV(u, v, w, vis)
+    ms = _events_ms(lambda: ctx.dft_image(n, th, V, _rg.RG_DFT_FP64_REDUCED, 2.0, image=img), repeats=2)
+    k = 2000
+    t0 = time.time()
+    oracle.dft_image(n, th, u[:k], v[:k], w[:k], vis[:k])
+    cpu_s = time.time() - t0
+    out["C2"] = {"n_vis": len(u), "grid_size": n, "gpu_ms": ms, "gpu_pairs_per_s": n * n * len(u) / (ms * 1e-3),
+                 "cpu_sample_vis": k, "cpu_s": cpu_s, "cpu_pairs_per_s": n * n * k / cpu_s, "cpu_cores": cores}
+    # C3: table W-projection on the learned-kernel workload (2048^2, 1M vis); CPU on a 100k sample
+    obs = _sim.learned_wproj(n_vis=1_000_000)
+    u, v, w, vis = (a[:1_000_000] for a in obs.flat())
+    n, th = obs.meta["grid_size"], obs.meta["theta"]
+    wk = _sim.generate_wkernel(th, np.arange(-2010.0, 2011.0, 10.0), 16, 8)
+    g = torch.zeros((n, n), dtype=torch.complex128, device=dev)
+    dwk = torch.from_numpy(np.ascontiguousarray(wk.data)).to(dev)
+    V = dV(u, v, w, vis)
+    ms = _events_ms(lambda: ctx.grid_wprojection(g, n, th, V, wk, flags=1, wkern_data=dwk), repeats=3)
+    k = 100_000
+    t0 = time.time()
+    oracle.grid_wprojection(n, th, u[:k], v[:k], w[:k], vis[:k], wk)
+    cpu_s = time.time() - t0
+    out["C3_table"] = {"n_vis": len(u), "gpu_ms": ms, "gpu_vis_per_s": len(u) / (ms * 1e-3),
+                       "cpu_sample_vis": k, "cpu_s": cpu_s, "cpu_vis_per_s": k / cpu_s, "cpu_cores": 1,
+                       "cpu_kind": "restatement of grid.c (bit-identical to it)"}
+    # C4: table W-towers, 4096^2, S 512, margin 32, winc 20, 8.37M vis
+    obs = _sim.wtowers_full()
+    u, v, w, vis = obs.flat()
+    n, th, S, M, winc = 4096, 0.1, 512, 32, 20.0
+    wk = _sim.generate_wkernel(th, np.arange(-11.0, 11.5, 1.0), 16, 32)
+    g = torch.zeros((n, n), dtype=torch.complex128, device=dev)
+    dwk = torch.from_numpy(np.ascontiguousarray(wk.data)).to(dev)
+    V = dV(u, v, w, vis)
+    ms = _events_ms(lambda: ctx.grid_wtowers(g, n, th, V, wk, S, M, winc, flags=1, wkern_data=dwk))
+    mask = oracle.reference_safe_baselines(obs, n, th, S, M, 16, 32)
+    sub = oracle.subset_baselines(obs, mask)
+    t0 = time.time()
+    oracle.ref_grid_wtowers(n, th, sub, wk, S, M, winc, omp=True)
+    cpu_s = time.time() - t0
+    out["C4_table"] = {"n_vis": len(u), "gpu_ms": ms, "gpu_vis_per_s": len(u) / (ms * 1e-3),
+                       "cpu_vis": sub.nvis, "cpu_s": cpu_s, "cpu_vis_per_s": sub.nvis / cpu_s, "cpu_cores": cores,
+                       "cpu_kind": "reference grid.c, -DOMP_TOWERS, its makefile flags"}
+    ctx.set_stream(None)
+    return out
+
+
 def main(which):
     ctx = _rg.Context(0)
     if which in ("dft", "all"):
@@ -186,6 +272,8 @@ def main(which):
                           "final_loss": losses[-1], **r}), flush=True)
 
 
+    if which == "baselines":
+        print(json.dumps({"study": "baselines", **baselines(ctx)}), flush=True)
     if which in ("parity_c1", "parity_c4"):
         print(json.dumps({"study": "parity_full", **parity_full(ctx, which[-2:].upper())}), flush=True)
     if which in ("learned_towers", "learned_towers_c4"):
