@@ -222,7 +222,8 @@ using StripGeom = ColGeom<N1, kStripCols>;
 
 // Persistent: the (slot, strip) pairs of the live slots are dealt round-robin
 // to the CTAs; each CTA gathers its marked pairs into a shared list, then
-// transforms them one after another.
+// transforms them one after another, loading the next strip while the
+// current one finishes.
 template <int N1>
 __global__ void __launch_bounds__(kSparseColThreads) sparse_cols_kernel(
     float2 *__restrict__ slots, const unsigned *__restrict__ masks, const int *__restrict__ counts, int slot_cap,
@@ -260,13 +261,11 @@ __global__ void __launch_bounds__(kSparseColThreads) sparse_cols_kernel(
         if (f) list[warp_base[warp] + __popc(b & ((1u << lane) - 1u))] = (int)(i - base);
         __syncthreads();
         const int n = warp_base[NW];
-        for (int k = 0; k < n; k++) {
+        auto strip_of = [&](int k) -> float2 * {
             const int64_t item = base + list[k];
-            const int64_t slot = item / STRIPS;
-            const int st = (int)(item % STRIPS);
-            float2 *col = slots + slot * N * N + st * C;
-            col_step1<N1, +1, C>(col, N, T, W);
-            __syncthreads();
+            return slots + (item / STRIPS) * N * N + (item % STRIPS) * C;
+        };
+        auto step2 = [&](float2 *col) {
             for (int it = threadIdx.x; it < C * 32; it += blockDim.x) {
                 const int c = it % C, k2 = it / C;
                 float2 v[N1];
@@ -276,7 +275,44 @@ __global__ void __launch_bounds__(kSparseColThreads) sparse_cols_kernel(
 #pragma unroll
                 for (int j = 0; j < N1; j++) col[(int64_t)(k2 + 32 * bitrevc(j, G::LB)) * N + c] = v[j];
             }
-            __syncthreads();
+        };
+        if constexpr (C * N1 <= kSparseColThreads) {
+            // one step-1 item per thread: the next strip's loads are issued
+            // before this strip's step 2, so they are in flight meanwhile
+            const bool act = threadIdx.x < C * N1;
+            const int c = threadIdx.x % C, n1 = threadIdx.x / C;
+            float2 a[32];
+            if (n > 0 && act) {
+                const float2 *src = strip_of(0);
+#pragma unroll
+                for (int n2 = 0; n2 < 32; n2++) a[n2] = src[(int64_t)(n1 + n2 * N1) * N + c];
+            }
+            for (int k = 0; k < n; k++) {
+                if (act) {
+                    reg_fft<32, +1>(a);
+#pragma unroll
+                    for (int j = 0; j < 32; j++) {
+                        const int k2 = bitrevc(j, 5);
+                        T[c * G::CS + n1 * kPad + k2] = cmulf(a[j], twiddle<+1>(W, k2 * N1 + n1));
+                    }
+                }
+                __syncthreads();
+                if (k + 1 < n && act) {
+                    const float2 *src = strip_of(k + 1);
+#pragma unroll
+                    for (int n2 = 0; n2 < 32; n2++) a[n2] = src[(int64_t)(n1 + n2 * N1) * N + c];
+                }
+                step2(strip_of(k));
+                __syncthreads();
+            }
+        } else {
+            for (int k = 0; k < n; k++) {
+                float2 *col = strip_of(k);
+                col_step1<N1, +1, C>(col, N, T, W);
+                __syncthreads();
+                step2(col);
+                __syncthreads();
+            }
         }
     }
 }
