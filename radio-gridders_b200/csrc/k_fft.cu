@@ -261,9 +261,10 @@ __global__ void __launch_bounds__(kSparseColThreads) sparse_cols_kernel(
         if (f) list[warp_base[warp] + __popc(b & ((1u << lane) - 1u))] = (int)(i - base);
         __syncthreads();
         const int n = warp_base[NW];
+        // strips are contiguous N x C blocks (strip-major sub-grids): row stride C
         auto strip_of = [&](int k) -> float2 * {
             const int64_t item = base + list[k];
-            return slots + (item / STRIPS) * N * N + (item % STRIPS) * C;
+            return slots + (item / STRIPS) * N * N + (item % STRIPS) * (int64_t)(C * N);
         };
         auto step2 = [&](float2 *col) {
             for (int it = threadIdx.x; it < C * 32; it += blockDim.x) {
@@ -273,7 +274,7 @@ __global__ void __launch_bounds__(kSparseColThreads) sparse_cols_kernel(
                 for (int n1 = 0; n1 < N1; n1++) v[n1] = T[c * G::CS + n1 * kPad + k2];
                 reg_fft<N1, +1>(v);
 #pragma unroll
-                for (int j = 0; j < N1; j++) col[(int64_t)(k2 + 32 * bitrevc(j, G::LB)) * N + c] = v[j];
+                for (int j = 0; j < N1; j++) col[(k2 + 32 * bitrevc(j, G::LB)) * C + c] = v[j];
             }
         };
         if constexpr (C * N1 <= kSparseColThreads) {
@@ -285,7 +286,7 @@ __global__ void __launch_bounds__(kSparseColThreads) sparse_cols_kernel(
             if (n > 0 && act) {
                 const float2 *src = strip_of(0);
 #pragma unroll
-                for (int n2 = 0; n2 < 32; n2++) a[n2] = src[(int64_t)(n1 + n2 * N1) * N + c];
+                for (int n2 = 0; n2 < 32; n2++) a[n2] = src[(n1 + n2 * N1) * C + c];
             }
             for (int k = 0; k < n; k++) {
                 if (act) {
@@ -300,7 +301,7 @@ __global__ void __launch_bounds__(kSparseColThreads) sparse_cols_kernel(
                 if (k + 1 < n && act) {
                     const float2 *src = strip_of(k + 1);
 #pragma unroll
-                    for (int n2 = 0; n2 < 32; n2++) a[n2] = src[(int64_t)(n1 + n2 * N1) * N + c];
+                    for (int n2 = 0; n2 < 32; n2++) a[n2] = src[(n1 + n2 * N1) * C + c];
                 }
                 step2(strip_of(k));
                 __syncthreads();
@@ -308,7 +309,7 @@ __global__ void __launch_bounds__(kSparseColThreads) sparse_cols_kernel(
         } else {
             for (int k = 0; k < n; k++) {
                 float2 *col = strip_of(k);
-                col_step1<N1, +1, C>(col, N, T, W);
+                col_step1<N1, +1, C>(col, C, T, W);
                 __syncthreads();
                 step2(col);
                 __syncthreads();
@@ -435,18 +436,30 @@ __global__ void __launch_bounds__(kRowThreads) tower_rows_kernel(
             G::WORDS > 2 ? (smask[2] | (G::WORDS > 3 ? (unsigned long long)smask[3] << 32 : 0ull)) : 0ull;
         for (int it = threadIdx.x; it < G::ITEMS1; it += blockDim.x) {
             const int n1 = it % N1, r = it / N1;
-            float2 *src = slots + ((int64_t)slot * N + row0 + r) * N + n1;
+            // strip-major sub-grid: column col of row (row0 + r) at (col/8)*8N + row*8 + col%8;
+            // for N1 >= 8 element n2 lies n2 * (N1/8) strips after the thread's first,
+            // a compile-time offset from one per-thread base
+            float2 *row_base = slots + (int64_t)slot * N * N + (row0 + r) * kStripCols;
+            float2 *src = row_base + (n1 / kStripCols) * (kStripCols * N) + n1 % kStripCols;
+            auto elem = [&](int n2) -> float2 * {
+                if constexpr (N1 >= kStripCols) {
+                    return src + n2 * (N1 / kStripCols) * (kStripCols * N);
+                } else {
+                    const int col = n1 + n2 * N1;
+                    return row_base + (col / kStripCols) * (kStripCols * N) + col % kStripCols;
+                }
+            };
             const unsigned on = element_bits<N1>(m_lo, m_hi, n1);
             float2 a[32];
             // all 32 loads issue before any clearing store
 #pragma unroll
             for (int n2 = 0; n2 < 32; n2++) {
                 a[n2] = make_float2(0.f, 0.f);
-                ld_if(a[n2], src + n2 * N1, (on >> n2) & 1u);
+                ld_if(a[n2], elem(n2), (on >> n2) & 1u);
             }
 #pragma unroll
             for (int n2 = 0; n2 < 32; n2++)
-                if ((on >> n2) & 1u) src[n2 * N1] = make_float2(0.f, 0.f);  // leave the sub-grid zeroed
+                if ((on >> n2) & 1u) *elem(n2) = make_float2(0.f, 0.f);  // leave the sub-grid zeroed
             reg_fft<32, +1>(a);
 #pragma unroll
             for (int j = 0; j < 32; j++) {

@@ -477,7 +477,8 @@ __global__ void __launch_bounds__(256) mlp_eval_kernel(const float *__restrict__
 __device__ __forceinline__ void learned_scatter(InferSmem &S, const float *__restrict__ P,
                                                 const bf16 *__restrict__ PB, float wf, float du, float dv,
                                                 float vr, float vi, float2 *grid, int64_t goff, int64_t ld,
-                                                int64_t limit, int ksize, float inv_wmax, float scale)
+                                                int64_t limit, int ksize, float inv_wmax, float scale,
+                                                int strip_lg = 0)
 {
     const int taps = ksize * ksize;
     for (int t0 = 0; t0 < taps; t0 += IR) {
@@ -497,7 +498,8 @@ __device__ __forceinline__ void learned_scatter(InferSmem &S, const float *__res
             const float kr = k.x * scale, ki = k.y * scale;
             const int64_t idx = goff + (int64_t)(t / ksize) * ld + (t % ksize);
             if (t < taps && idx >= 0 && idx < limit)
-                atomicAdd(grid + idx, make_float2(vr * kr + vi * ki, vi * kr - vr * ki));
+                atomicAdd(grid + (strip_lg ? (int64_t)strip_addr((int)idx, strip_lg) : idx),
+                          make_float2(vr * kr + vi * ki, vi * kr - vr * ki));
         }
         __syncthreads();
     }
@@ -531,6 +533,7 @@ __global__ void __launch_bounds__(256) learned_towers_kernel(
     const int *__restrict__ slot_of_bin, int slot_cap, float2 *__restrict__ slots, int sub,
     const float *__restrict__ P, const bf16 *__restrict__ PB, int ksize, float inv_wmax, float scale)
 {
+    const int strip_lg = __ffs(sub) - 1;  // sub-grids are strip-major (strip_addr)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     InferSmem &S = *reinterpret_cast<InferSmem *>(smem_raw);
     const int64_t cells = (int64_t)sub * sub;
@@ -542,7 +545,7 @@ __global__ void __launch_bounds__(256) learned_towers_kernel(
         const float4 f = feat[i];
         const float2 vz = visf[i];
         learned_scatter(S, P, PB, f.x, f.y, f.z, vz.x, vz.y, slots + (int64_t)slot * cells, r.y, sub, cells, ksize,
-                        inv_wmax, scale);
+                        inv_wmax, scale, strip_lg);
     }
 }
 

@@ -12,7 +12,8 @@
 // grid += v * conj(wk) (src/reference/grid.c:177-182).
 //
 // The linear index grid_offset + cv * side + cu is the reference's
-// grid_offset + y*size + x; points outside [0, side^2) are dropped (the
+// grid_offset + y*size + x (mapped to the strip-major sub-grid layout when
+// strip_lg is set); points outside [0, side^2) are dropped (the
 // reference does not check, grid.c:177-182; its GPU gridder drops them,
 // src/grid/grid_cuda.cu:25-41).  The record carries grid_offset and the
 // footprint origin's residues modulo 64, so a thread's tap (cu, cv) is two
@@ -39,11 +40,11 @@ struct RomeinBounds {
     static constexpr int min_ctas = want > 32 ? 32 : (want < 1 ? 1 : want);
 };
 
-template <int K, int P>
+template <int K, int P, bool STRIP>
 __global__ void __launch_bounds__(K *K / P, (RomeinBounds<K, P>::min_ctas)) romein_kernel(
     const int4 *__restrict__ rec, const float2 *__restrict__ visf, int64_t n,
     const float2 *__restrict__ taps, float2 *__restrict__ grids,
-    const int *__restrict__ slot_of_bin, int64_t grid_stride, int side, int64_t chunk, int slot_cap)
+    const int *__restrict__ slot_of_bin, int64_t grid_stride, int side, int64_t chunk, int slot_cap, int strip_lg)
 {
     constexpr int NT = K * K / P;     // threads
     constexpr int BATCH = 256;        // visibilities staged per round
@@ -52,6 +53,7 @@ __global__ void __launch_bounds__(K *K / P, (RomeinBounds<K, P>::min_ctas)) rome
     __shared__ float2 svis[BATCH];
     const int myU = threadIdx.x % K, myV0 = threadIdx.x / K;
     const int limit = side * side;
+    auto addr = [strip_lg](int L) { return STRIP ? strip_addr(L, strip_lg) : L; };
 
     for (int64_t c0 = (int64_t)blockIdx.x * chunk; c0 < n; c0 += (int64_t)gridDim.x * chunk) {
         const int64_t c1 = c0 + chunk < n ? c0 + chunk : n;
@@ -102,7 +104,7 @@ __global__ void __launch_bounds__(K *K / P, (RomeinBounds<K, P>::min_ctas)) rome
                 if (r.x != cur_bin) {
 #pragma unroll
                     for (int p = 0; p < P; p++) {
-                        if (cur_grid && (unsigned)cur_idx[p] < (unsigned)limit) atomicAdd(cur_grid + cur_idx[p], sum[p]);
+                        if (cur_grid && (unsigned)cur_idx[p] < (unsigned)limit) atomicAdd(cur_grid + addr(cur_idx[p]), sum[p]);
                         cur_idx[p] = idx[p];
                         sum[p] = make_float2(0.f, 0.f);
                     }
@@ -113,7 +115,7 @@ __global__ void __launch_bounds__(K *K / P, (RomeinBounds<K, P>::min_ctas)) rome
 #pragma unroll
                 for (int p = 0; p < P; p++) {
                     if (idx[p] != cur_idx[p]) {
-                        if (cur_grid && (unsigned)cur_idx[p] < (unsigned)limit) atomicAdd(cur_grid + cur_idx[p], sum[p]);
+                        if (cur_grid && (unsigned)cur_idx[p] < (unsigned)limit) atomicAdd(cur_grid + addr(cur_idx[p]), sum[p]);
                         cur_idx[p] = idx[p];
                         sum[p] = make_float2(0.f, 0.f);
                     }
@@ -125,7 +127,7 @@ __global__ void __launch_bounds__(K *K / P, (RomeinBounds<K, P>::min_ctas)) rome
         if (cur_grid) {
 #pragma unroll
             for (int p = 0; p < P; p++)
-                if ((unsigned)cur_idx[p] < (unsigned)limit) atomicAdd(cur_grid + cur_idx[p], sum[p]);
+                if ((unsigned)cur_idx[p] < (unsigned)limit) atomicAdd(cur_grid + addr(cur_idx[p]), sum[p]);
         }
     }
 }
@@ -133,29 +135,34 @@ __global__ void __launch_bounds__(K *K / P, (RomeinBounds<K, P>::min_ctas)) rome
 template <int K, int P>
 static void romein_launch(cudaStream_t s, const int4 *rec, const float2 *visf, int64_t n, const float2 *taps,
                           float2 *grids, const int *slot_of_bin, int64_t grid_stride, int grid_side, int sm_count,
-                          int slot_cap)
+                          int slot_cap, int strip_lg)
 {
     // Every CTA resident at once, each with an equal contiguous run of
     // visibilities: occupancy, not the chunk size, decides the grid.
     constexpr int NT = K * K / P;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, romein_kernel<K, P>, NT, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, romein_kernel<K, P, false>, NT, 0);
     if (per_sm < 1) per_sm = 1;
     int64_t blocks = (int64_t)sm_count * per_sm;
     int64_t chunk = (n + blocks - 1) / blocks;
     if (chunk < 32) chunk = 32;
     blocks = (n + chunk - 1) / chunk;
     if (blocks < 1) blocks = 1;
-    romein_kernel<K, P><<<(unsigned)blocks, NT, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin, grid_stride,
-                                                         grid_side, chunk, slot_cap);
+    if (strip_lg)
+        romein_kernel<K, P, true><<<(unsigned)blocks, NT, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin, grid_stride,
+                                                                  grid_side, chunk, slot_cap, strip_lg);
+    else
+        romein_kernel<K, P, false><<<(unsigned)blocks, NT, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin,
+                                                                   grid_stride, grid_side, chunk, slot_cap, 0);
 }
 
 void launch_romein(cudaStream_t s, const int4 *rec, const float2 *visf, int64_t n,
                    const float2 *taps, float2 *grids, const int *slot_of_bin, int64_t grid_stride,
-                   int grid_side, int ksize, int sm_count, int slot_cap, int points)
+                   int grid_side, int ksize, int sm_count, int slot_cap, int points, int strip_lg)
 {
 #define RG_ROMEIN(K, P) \
-    romein_launch<K, P>(s, rec, visf, n, taps, grids, slot_of_bin, grid_stride, grid_side, sm_count, slot_cap)
+    romein_launch<K, P>(s, rec, visf, n, taps, grids, slot_of_bin, grid_stride, grid_side, sm_count, slot_cap, \
+                        strip_lg)
     switch (ksize) {
         case 4: RG_ROMEIN(4, 1); break;
         case 8:

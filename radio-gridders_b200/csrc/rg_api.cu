@@ -257,6 +257,13 @@ void collect_timings(rg_context *ctx)
     }
 }
 
+static int ilog2_int(int n)
+{
+    int l = 0;
+    while ((1 << l) < n) l++;
+    return l;
+}
+
 static rg_status get_twiddles32(rg_context *ctx, int n, float2 **tw)
 {
     std::string name = "tw32_" + std::to_string(n);
@@ -563,7 +570,7 @@ static rg_status wtowers_enqueue(rg_context *ctx, const DevVis &dv, const float2
         if (dv.n > 0)
             launch_romein(st, (const int4 *)rec, (const float2 *)visf, dv.n, taps, (float2 *)slots,
                           (const int *)slot_of_bin, sub_cells, S, K, ctx->sm_count, pl.slots_cap,
-                          pl.tune.romein_points);
+                          pl.tune.romein_points, ilog2_int(S));
         end_stage(ctx);
     }
     begin_stage(ctx, "fft_cols_backward");

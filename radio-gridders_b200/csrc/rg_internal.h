@@ -174,6 +174,14 @@ void launch_w_floors(cudaStream_t s, const double *wrange, double winc, int floo
 // marked strips are ever non-zero, so the column transforms and the row stage
 // touch only them.
 constexpr int kStripCols = 8;
+// Sub-grids of the W-towers pass are stored strip-major: element (row, col)
+// of an S x S sub-grid (S = 2^lg) at (col / 8) * 8S + row * 8 + col % 8, so a
+// column strip is one contiguous 8S-element block.  L is the row-major linear
+// index row * S + col, 0 <= L < S^2.
+__host__ __device__ __forceinline__ int strip_addr(int L, int lg)
+{
+    return ((L & ((1 << lg) - 1)) >> 3) * (8 << lg) + (L >> lg) * 8 + (L & 7);
+}
 // feat == nullptr: table taps (frac_coord cells and oversampled sub-cell
 // indices, the reference's).  feat != nullptr: learned taps — cell = floor(x)
 // with the continuous offsets feat[i] = {w - w_mid, du, dv, 0}; no table.
@@ -195,11 +203,12 @@ void launch_compact_bins(cudaStream_t s, const int *active, const int *range, in
 // k_romein.cu
 // Sub-grids with slot index >= slot_cap are skipped (capacity overflow: the
 // caller detects it from the slot count and reruns).
-// points: grid points per thread (0: the default for ksize).
+// points: grid points per thread (0: the default for ksize).  strip_lg = 0:
+// row-major grids; otherwise log2(grid_side) and strip-major sub-grids.
 void launch_romein(cudaStream_t s, const int4 *rec, const float2 *visf, int64_t n,
                    const float2 *taps, float2 *grids, const int *slot_of_bin,
                    int64_t grid_stride, int grid_side, int ksize, int sm_count, int slot_cap = 1,
-                   int points = 0);
+                   int points = 0, int strip_lg = 0);
 
 // k_towers.cu
 void launch_fresnel_table(cudaStream_t s, double *ph, int subgrid, double theta, double winc);
