@@ -27,6 +27,23 @@ void launch_convert_table(cudaStream_t s, const double2 *src, float2 *dst, int64
     convert_table_kernel<<<blocks_for(n), 256, 0, s>>>(src, dst, n);
 }
 
+// Each kk-tap slice written twice in a row: dst[s][0..2kk) = src[s][t mod kk].
+__global__ void convert_table_dup_kernel(const double2 *__restrict__ src, float2 *__restrict__ dst, int64_t n_out,
+                                         int kk)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_out;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t slice = i / (2 * kk);
+        const double2 z = src[slice * kk + (int)(i % (2 * kk)) % kk];
+        dst[i] = make_float2((float)z.x, (float)z.y);
+    }
+}
+
+void launch_convert_table_dup(cudaStream_t s, const double2 *src, float2 *dst, int64_t n, int kk)
+{
+    convert_table_dup_kernel<<<blocks_for(2 * n), 256, 0, s>>>(src, dst, 2 * n, kk);
+}
+
 // make_hermitian, src/reference/grid.c:639-662: the pointer walk pairs linear
 // index base + t with N^2 - 1 - t (base = N + 1 for even N, 0 for odd) until
 // they meet at the zero frequency (N + 1) * (N / 2).  Pairs are disjoint, so

@@ -13,7 +13,8 @@
 //
 // The linear index grid_offset + cv * side + cu is the reference's
 // grid_offset + y*size + x (mapped to the strip-major sub-grid layout when
-// strip_lg is set); points outside [0, side^2) are dropped (the
+// strip_lg is set: the W-towers sub-grids, whose kernel table then holds every
+// slice twice); points outside [0, side^2) are dropped (the
 // reference does not check, grid.c:177-182; its GPU gridder drops them,
 // src/grid/grid_cuda.cu:25-41).  The record carries grid_offset and the
 // footprint origin's residues modulo 64, so a thread's tap (cu, cv) is two
@@ -78,13 +79,17 @@ __global__ void __launch_bounds__(K *K / P, (RomeinBounds<K, P>::min_ctas)) rome
                 const int4 r = srec[j];
                 if (r.x < 0) continue;
                 const int cu = (myU - (r.w & 0xff)) & (K - 1);
-                const int r0 = r.w >> 8;
+                const int cv0 = (myV0 - (r.w >> 8)) & (K - 1);  // slice row of the thread's first point
                 float2 t[P];
-                int cv[P];
+                if (STRIP) {
+                    // duplicated slices (2K rows): rows cv0 + p*RS need no wrap, so the
+                    // loads are one base plus compile-time offsets
+                    const float2 *tp = taps + 2 * (int64_t)r.z + cv0 * K + cu;
 #pragma unroll
-                for (int p = 0; p < P; p++) {
-                    cv[p] = (myV0 + p * RS - r0) & (K - 1);
-                    t[p] = __ldg(taps + r.z + cv[p] * K + cu);
+                    for (int p = 0; p < P; p++) t[p] = __ldg(tp + p * RS * K);
+                } else {
+#pragma unroll
+                    for (int p = 0; p < P; p++) t[p] = __ldg(taps + r.z + ((cv0 + p * RS) & (K - 1)) * K + cu);
                 }
                 const float2 vz = svis[j];
                 if (r.x == cur_bin && r.y == cur_goff && r.w == cur_res) {
@@ -100,7 +105,7 @@ __global__ void __launch_bounds__(K *K / P, (RomeinBounds<K, P>::min_ctas)) rome
                 cur_res = r.w;
                 int idx[P];
 #pragma unroll
-                for (int p = 0; p < P; p++) idx[p] = r.y + cv[p] * side + cu;
+                for (int p = 0; p < P; p++) idx[p] = r.y + ((cv0 + p * RS) & (K - 1)) * side + cu;
                 if (r.x != cur_bin) {
 #pragma unroll
                     for (int p = 0; p < P; p++) {

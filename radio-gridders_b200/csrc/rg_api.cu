@@ -203,14 +203,18 @@ static rg_status stage_vis(rg_context *ctx, const rg_vis *vis, DevVis *dv)
     return RG_OK;
 }
 
-static rg_status stage_taps(rg_context *ctx, const rg_wkern *wk, float2 **taps)
+// dup: the W-towers layout with each slice stored twice (launch_convert_table_dup)
+static rg_status stage_taps(rg_context *ctx, const rg_wkern *wk, float2 **taps, bool dup = false)
 {
     const int64_t ntaps = (int64_t)wk->plane_count * wk->oversampling * wk->oversampling * wk->size * wk->size;
     const void *src;
     RG_CHECK(stage_in(ctx, wk->data, sizeof(double2) * ntaps, "in_wkern", &src));
     void *dst;
-    RG_CHECK(scratch(ctx, "taps32", sizeof(float2) * ntaps, &dst));
-    launch_convert_table(ctx->stream, (const double2 *)src, (float2 *)dst, ntaps);
+    RG_CHECK(scratch(ctx, dup ? "taps32_dup" : "taps32", sizeof(float2) * ntaps * (dup ? 2 : 1), &dst));
+    if (dup)
+        launch_convert_table_dup(ctx->stream, (const double2 *)src, (float2 *)dst, ntaps, wk->size * wk->size);
+    else
+        launch_convert_table(ctx->stream, (const double2 *)src, (float2 *)dst, ntaps);
     ctx->launches++;
     *taps = (float2 *)dst;
     return check_launch("convert w-kernel table");
@@ -776,7 +780,7 @@ rg_status grid_wtowers_impl(rg_context *ctx, double *uvgrid, int grid_size, doub
     begin_stage(ctx, "stage_in");
     RG_CHECK(stage_vis(ctx, vis, &dv));
     float2 *taps = nullptr;
-    if (!lt) RG_CHECK(stage_taps(ctx, wkern, &taps));
+    if (!lt) RG_CHECK(stage_taps(ctx, wkern, &taps, true));
     OutView ov;
     RG_CHECK(out_view(ctx, uvgrid, sizeof(double2) * (size_t)cells, "out_grid",
                       !(flags & RG_GRID_OVERWRITE), &ov));

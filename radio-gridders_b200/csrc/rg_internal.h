@@ -132,6 +132,9 @@ bool is_device_pointer(const void *p);
 
 // k_image.cu
 void launch_convert_table(cudaStream_t s, const double2 *src, float2 *dst, int64_t n);
+// The W-towers gridder's copy: every K x K slice stored twice (2 K^2 taps), so
+// a thread's rows (r0 + j) mod K are read as r0 + j without wrapping.
+void launch_convert_table_dup(cudaStream_t s, const double2 *src, float2 *dst, int64_t n, int kk);
 void launch_make_hermitian(cudaStream_t s, double2 *grid, int n);
 void launch_fft_shift(cudaStream_t s, double2 *grid, int n);
 void launch_real_part(cudaStream_t s, const double2 *grid, double *img, int n,
