@@ -159,6 +159,18 @@ rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double
                           const rg_vis *vis, const rg_wkern *wkern, int subgrid_size,
                           int subgrid_margin, double wincrement, int flags);
 
+/* count observations of one shape (same visibility count) with one kernel
+ * table: the same result as count rg_grid_wtowers calls in order (grid i from
+ * vis[i] into uvgrids[i]), with the host-to-device copies of the next
+ * observation and the device-to-host copy of the previous grid overlapping each
+ * pass (two staging sets, three streams).  For streams of snapshots imaged
+ * with one set of kernels; no counterpart in the reference.  Inputs and grids
+ * in pinned host memory overlap fully; device buffers are used in place.
+ * Returns the first error; the grids of the steps before it are complete. */
+rg_status rg_grid_wtowers_batch(rg_context *ctx, int count, double *const *uvgrids, int grid_size, double theta,
+                                const rg_vis *vis, const rg_wkern *wkern, int subgrid_size, int subgrid_margin,
+                                double wincrement, int flags);
+
 /* Uniform weighting: vis_out[i] = vis[i] / (visibilities in its nearest cell).
  * Replaces weight() (src/reference/grid.h:116-117, grid.c:59-81) as called by
  * src/reference/main.c:153.  vis_out: 2*n doubles (may alias vis->vis). */

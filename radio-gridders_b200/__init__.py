@@ -42,7 +42,7 @@ EXPORTS = [
     "rg_make_hermitian", "rg_fft_shift", "rg_image_from_grid", "rg_fft2d", "rg_dft_image",
     "rg_grid_wprojection_noalloc", "rg_mlp_param_count", "rg_mlp_create", "rg_mlp_destroy",
     "rg_mlp_set_params", "rg_mlp_get_params", "rg_mlp_gradient", "rg_mlp_train", "rg_mlp_eval",
-    "rg_grid_wprojection_learned", "rg_grid_wtowers_learned", "rg_read_vis_hdf5", "rg_free_vis_data", "rg_read_wkern_hdf5",
+    "rg_grid_wprojection_learned", "rg_grid_wtowers_learned", "rg_grid_wtowers_batch", "rg_read_vis_hdf5", "rg_free_vis_data", "rg_read_wkern_hdf5",
     "rg_free_wkern_data", "rg_write_vis_hdf5", "rg_write_wkern_hdf5", "rg_hdf5_read_f64",
     "rg_hdf5_attr_f64",
 ]
@@ -104,6 +104,8 @@ def lib():
         L.rg_last_timings.restype = i
         L.rg_grid_wprojection.argtypes = [vp, vp, i, d, ct.POINTER(_Vis), ct.POINTER(_WKern), i]
         L.rg_grid_wtowers.argtypes = [vp, vp, i, d, ct.POINTER(_Vis), ct.POINTER(_WKern), i, i, d, i]
+        L.rg_grid_wtowers_batch.argtypes = [vp, i, ct.POINTER(vp), i, d, ct.POINTER(_Vis), ct.POINTER(_WKern),
+                                            i, i, d, i]
         L.rg_weight.argtypes = [vp, i, d, ct.POINTER(_Vis), vp]
         L.rg_make_hermitian.argtypes = [vp, vp, i]
         L.rg_fft_shift.argtypes = [vp, vp, i]
@@ -254,6 +256,18 @@ class Context:
                                      ct.byref(vs), ct.byref(s), int(subgrid_size),
                                      int(subgrid_margin), float(wincrement), int(flags)))
         return uvgrid
+
+    def grid_wtowers_batch(self, uvgrids, grid_size, theta, vis_list, wkern, subgrid_size, subgrid_margin,
+                           wincrement, flags=RG_GRID_ACCUMULATE, wkern_data=None):
+        """rg_grid_wtowers_batch: one grid per Visibilities of vis_list, with
+        the copies of neighbouring observations overlapping each pass."""
+        s, keep = _wkern_struct(wkern, wkern_data)
+        count = len(vis_list)
+        vs = (_Vis * count)(*[v.struct() for v in vis_list])
+        gp = (ct.c_void_p * count)(*[_ptr(g) for g in uvgrids])
+        _check(lib().rg_grid_wtowers_batch(self._h, count, gp, int(grid_size), float(theta), vs, ct.byref(s),
+                                           int(subgrid_size), int(subgrid_margin), float(wincrement), int(flags)))
+        return uvgrids
 
     def weight(self, grid_size, theta, vis: Visibilities, out=None):
         if out is None:

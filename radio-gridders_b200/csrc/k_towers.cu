@@ -45,16 +45,22 @@ __device__ __forceinline__ int div_nonneg(int a, int d, float inv)
 // sums, in tower order (cy, then cx), the overlapping towers' forward-
 // transformed sub-images divided by S^2, in FP64.  Deterministic.
 // When a capacity overflowed (range[2] == 0 or a live count above its
-// capacity) nothing is written, so the caller can rerun on the same grid.
+// capacity) nothing is written, so the caller can rerun on the same grid.  In
+// a batch (poison != nullptr) an overflow also stops the later passes' writes
+// until the batch reruns them.
 __global__ void add_back_kernel(const float2 *__restrict__ subimg, const int *__restrict__ tower_count,
                                 double2 *__restrict__ master, int N, int S, int M, int chunk,
                                 int nchunk, int overwrite, const int *__restrict__ range,
-                                const int *__restrict__ counts, int slot_cap, int group_cap)
+                                const int *__restrict__ counts, int slot_cap, int group_cap, int *poison)
 {
     const int gx = blockIdx.x * blockDim.x + threadIdx.x;
     const int gy = blockIdx.y * blockDim.y + threadIdx.y;
     if (gx >= N || gy >= N) return;
-    if (range && (!range[2] || counts[0] > slot_cap || counts[1] > group_cap)) return;
+    if (range && (!range[2] || counts[0] > slot_cap || counts[1] > group_cap)) {
+        if (poison) *poison = 1;  // later passes of a batch may see unconsumed sub-grids
+        return;
+    }
+    if (poison && *poison) return;
     const int ax = gx + M / 2, ay = gy + M / 2;  // x + N/2 + M/2 with x = gx - N/2
     const float inv = 1.0f / (float)chunk;
     int cx_hi = div_nonneg(ax, chunk, inv), cy_hi = div_nonneg(ay, chunk, inv);
@@ -83,12 +89,12 @@ __global__ void add_back_kernel(const float2 *__restrict__ subimg, const int *__
 
 void launch_add_back(cudaStream_t s, const float2 *subimg, const int *tower_count, double2 *master,
                      int grid_size, int subgrid, int margin, int chunk, int nchunk, int overwrite,
-                     const int *range, const int *counts, int slot_cap, int group_cap)
+                     const int *range, const int *counts, int slot_cap, int group_cap, int *poison)
 {
     dim3 blk(32, 8);
     dim3 grd((grid_size + 31) / 32, (grid_size + 7) / 8);
     add_back_kernel<<<grd, blk, 0, s>>>(subimg, tower_count, master, grid_size, subgrid, margin,
-                                        chunk, nchunk, overwrite, range, counts, slot_cap, group_cap);
+                                        chunk, nchunk, overwrite, range, counts, slot_cap, group_cap, poison);
 }
 
 }  // namespace rg

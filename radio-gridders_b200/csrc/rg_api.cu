@@ -329,6 +329,18 @@ rg_status rg_context_destroy(rg_context *ctx)
     cudaStreamSynchronize(ctx->stream);
     for (auto &kv : ctx->tower_plans)
         if (kv.second.graph_exec) cudaGraphExecDestroy(kv.second.graph_exec);
+    for (int b = 0; b < 2; b++)
+        for (cudaEvent_t e : {ctx->ev_in[b], ctx->ev_used[b], ctx->ev_done[b], ctx->ev_out[b]})
+            if (e) cudaEventDestroy(e);
+    if (ctx->copy_in) {
+        cudaStreamSynchronize(ctx->copy_in);
+        cudaStreamDestroy(ctx->copy_in);
+    }
+    if (ctx->copy_out) {
+        cudaStreamSynchronize(ctx->copy_out);
+        cudaStreamDestroy(ctx->copy_out);
+    }
+    if (ctx->pinned_steps) cudaFreeHost(ctx->pinned_steps);
     for (auto &kv : ctx->scratch)
         if (kv.second.ptr) cudaFree(kv.second.ptr);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
@@ -469,7 +481,8 @@ namespace rg {
 // here synchronises, so the sequence can also be captured into a CUDA graph.
 static rg_status wtowers_enqueue(rg_context *ctx, const DevVis &dv, const float2 *taps, const rg_wkern *wkern,
                                  const LearnedTaps *lt, double *out_dev, int N, double theta, int S, int M,
-                                 double winc, int flags, TowerPlan &pl)
+                                 double winc, int flags, TowerPlan &pl, void *diag_host = nullptr,
+                                 int *poison = nullptr)
 {
     cudaStream_t st = ctx->stream;
     const int K = lt ? lt->ksize : wkern->size;
@@ -596,20 +609,20 @@ static rg_status wtowers_enqueue(rg_context *ctx, const DevVis &dv, const float2
     end_stage(ctx);
     begin_stage(ctx, "add_back");
     launch_add_back(st, (const float2 *)subimg, (const int *)tcount, (double2 *)out_dev, N, S, M, chunk, nchunk,
-                    (flags & RG_GRID_OVERWRITE) ? 1 : 0, range, counts, pl.slots_cap, pl.groups_cap);
+                    (flags & RG_GRID_OVERWRITE) ? 1 : 0, range, counts, pl.slots_cap, pl.groups_cap, poison);
     end_stage(ctx);
     ctx->launches += 11;  // minmax, floors, prepare, compact, romein, masks, cols, rows, finish, cols, add-back
     RG_CHECK(check_launch("W-towers pass"));
 
-    RG_CUDA(cudaMemcpyAsync(ctx->pinned, d.err, 64, cudaMemcpyDeviceToHost, st));
+    RG_CUDA(cudaMemcpyAsync(diag_host ? diag_host : ctx->pinned, d.err, 64, cudaMemcpyDeviceToHost, st));
     return RG_OK;
 }
 
 // After the stream has passed a wtowers_enqueue: capacities seen, overflow,
 // input errors and the call statistics.
-static rg_status wtowers_check(rg_context *ctx, TowerPlan &pl, bool *overflow)
+static rg_status wtowers_check(rg_context *ctx, TowerPlan &pl, bool *overflow, const void *diag_host = nullptr)
 {
-    const unsigned char *host = (const unsigned char *)ctx->pinned;
+    const unsigned char *host = (const unsigned char *)(diag_host ? diag_host : ctx->pinned);
     unsigned err;
     unsigned long long ctr[2];
     int cnt[4], rng[3];
@@ -862,6 +875,144 @@ rg_status grid_wtowers_impl(rg_context *ctx, double *uvgrid, int grid_size, doub
     return RG_OK;
 }
 
+// Several observations of one shape in one call, pipelined over three
+// streams: the inputs of step k+1 are copied in (copy_in) and the grid of step
+// k-1 copied out (copy_out) while step k's pass runs (ctx->stream), with two
+// sets of staging buffers.  Step 0 runs as an ordinary call (it sizes the plan,
+// tunes and stages the kernel table, which the later steps reuse) unless an
+// earlier call already sized and tuned the shape.  Each
+// pass's diagnostics land in their own pinned slot; after the last step they
+// are checked in order.  A pass that overflows its capacities writes nothing
+// and stops the writes of every later pass of the batch (a device flag), and
+// those steps are run again as ordinary calls.
+static rg_status batch_streams(rg_context *ctx)
+{
+    if (!ctx->copy_in) RG_CUDA(cudaStreamCreateWithFlags(&ctx->copy_in, cudaStreamNonBlocking));
+    if (!ctx->copy_out) RG_CUDA(cudaStreamCreateWithFlags(&ctx->copy_out, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; b++)
+        for (cudaEvent_t *e : {&ctx->ev_in[b], &ctx->ev_used[b], &ctx->ev_done[b], &ctx->ev_out[b]})
+            if (!*e) RG_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    return RG_OK;
+}
+
+rg_status grid_wtowers_batch_impl(rg_context *ctx, int count, double *const *uvgrids, int grid_size, double theta,
+                                  const rg_vis *vis, const rg_wkern *wkern, int S, int M, double winc, int flags)
+{
+    if (!ctx || !uvgrids || !vis || count < 0) return fail(RG_ERR_INVALID_ARGUMENT, "bad batch arguments");
+    if (count == 0) return RG_OK;
+    bool same = true;
+    for (int i = 0; i < count; i++) {
+        RG_CHECK(check_vis(&vis[i]));
+        if (!uvgrids[i]) return fail(RG_ERR_INVALID_ARGUMENT, "uvgrids must be non-NULL");
+        same = same && vis[i].n == vis[0].n;
+    }
+    const int N = grid_size;
+    const size_t grid_bytes = sizeof(double2) * (size_t)N * N;
+    const int64_t n = vis[0].n;
+    const size_t vb = sizeof(double) * (size_t)n;
+    char keybuf[200];
+    std::snprintf(keybuf, sizeof(keybuf), "%d_%d_%d_%.17g_%.17g_%lld_%c", N, S, M, theta, winc, (long long)n, 'T');
+    // a shape already sized (and tuned) by an earlier call pipelines from step 0;
+    // otherwise step 0 is an ordinary call that sizes and tunes it
+    auto known = ctx->tower_plans.find(keybuf);
+    const bool ready = known != ctx->tower_plans.end() && known->second.valid &&
+                       (known->second.tuned || !ctx->autotune);
+    int first = 0;
+    if (!ready || !same || ctx->profiling) {
+        RG_CHECK(grid_wtowers_impl(ctx, uvgrids[0], grid_size, theta, &vis[0], wkern, nullptr, S, M, winc, flags));
+        first = 1;
+    }
+    if (count == first) return RG_OK;
+    if (!same || ctx->profiling) {
+        for (int i = 1; i < count; i++)
+            RG_CHECK(grid_wtowers_impl(ctx, uvgrids[i], grid_size, theta, &vis[i], wkern, nullptr, S, M, winc, flags));
+        return RG_OK;
+    }
+    RG_CHECK(check_wkern(wkern));
+    RG_CUDA(cudaSetDevice(ctx->device));
+    begin_call(ctx);
+    RG_CHECK(batch_streams(ctx));
+    TowerPlan &pl = ctx->tower_plans[keybuf];
+    float2 *taps = nullptr;
+    RG_CHECK(stage_taps(ctx, wkern, &taps, true));  // once for the batch (step 0 staged it already if it ran)
+    void *poison = nullptr;  // set by the first pass that overflows; the later passes then write nothing
+    RG_CHECK(scratch(ctx, "batch_poison", sizeof(int), &poison));
+    RG_CUDA(cudaMemsetAsync(poison, 0, sizeof(int), ctx->stream));
+    if (ctx->pinned_steps_bytes < (size_t)count * 64) {
+        if (ctx->pinned_steps) cudaFreeHost(ctx->pinned_steps);
+        ctx->pinned_steps = nullptr;
+        ctx->pinned_steps_bytes = 0;
+        RG_CUDA(cudaMallocHost(&ctx->pinned_steps, (size_t)count * 64));
+        ctx->pinned_steps_bytes = (size_t)count * 64;
+    }
+    // two staging sets for inputs in host memory and for grids in host memory
+    void *in[2][4], *outb[2];
+    static const char *in_names[2][4] = {{"batch_u0", "batch_v0", "batch_w0", "batch_vis0"},
+                                         {"batch_u1", "batch_v1", "batch_w1", "batch_vis1"}};
+    for (int b = 0; b < 2; b++) {
+        for (int f = 0; f < 4; f++) RG_CHECK(scratch(ctx, in_names[b][f], f == 3 ? 2 * vb : vb, &in[b][f]));
+        RG_CHECK(scratch(ctx, b ? "batch_out1" : "batch_out0", grid_bytes, &outb[b]));
+    }
+    // the copy streams start after everything already on the context stream
+    RG_CUDA(cudaEventRecord(ctx->ev_done[0], ctx->stream));
+    RG_CUDA(cudaStreamWaitEvent(ctx->copy_in, ctx->ev_done[0], 0));
+    RG_CUDA(cudaStreamWaitEvent(ctx->copy_out, ctx->ev_done[0], 0));
+    bool used[2] = {false, false}, out_pending[2] = {false, false};
+    for (int i = first; i < count; i++) {
+        const int b = i & 1;
+        const rg_vis &v = vis[i];
+        const void *src[4] = {v.u, v.v, v.w, v.vis};
+        const void *dev[4];
+        if (used[b]) RG_CUDA(cudaStreamWaitEvent(ctx->copy_in, ctx->ev_used[b], 0));  // step i-2 done with set b
+        if (out_pending[b]) RG_CUDA(cudaStreamWaitEvent(ctx->copy_in, ctx->ev_out[b], 0));  // its grid copied out
+        for (int f = 0; f < 4; f++) {
+            if (n == 0 || is_device_pointer(src[f])) {
+                dev[f] = src[f];
+            } else {
+                RG_CUDA(cudaMemcpyAsync(in[b][f], src[f], f == 3 ? 2 * vb : vb, cudaMemcpyHostToDevice,
+                                        ctx->copy_in));
+                dev[f] = in[b][f];
+            }
+        }
+        DevVis dv;
+        dv.u = (const double *)dev[0];
+        dv.v = (const double *)dev[1];
+        dv.w = (const double *)dev[2];
+        dv.vis = (const double2 *)dev[3];
+        dv.n = n;
+        const bool host_out = !is_device_pointer(uvgrids[i]);
+        double *out_dev = host_out ? (double *)outb[b] : uvgrids[i];
+        if (host_out && !(flags & RG_GRID_OVERWRITE))
+            RG_CUDA(cudaMemcpyAsync(out_dev, uvgrids[i], grid_bytes, cudaMemcpyHostToDevice, ctx->copy_in));
+        RG_CUDA(cudaEventRecord(ctx->ev_in[b], ctx->copy_in));
+        RG_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev_in[b], 0));
+        RG_CHECK(wtowers_enqueue(ctx, dv, (const float2 *)taps, wkern, nullptr, out_dev, N, theta, S, M, winc, flags,
+                                 pl, (char *)ctx->pinned_steps + (size_t)i * 64, (int *)poison));
+        RG_CUDA(cudaEventRecord(ctx->ev_used[b], ctx->stream));
+        if (host_out) {
+            RG_CUDA(cudaStreamWaitEvent(ctx->copy_out, ctx->ev_used[b], 0));
+            RG_CUDA(cudaMemcpyAsync(uvgrids[i], out_dev, grid_bytes, cudaMemcpyDeviceToHost, ctx->copy_out));
+            RG_CUDA(cudaEventRecord(ctx->ev_out[b], ctx->copy_out));
+        }
+        used[b] = true;
+        out_pending[b] = host_out;
+    }
+    RG_CUDA(cudaStreamSynchronize(ctx->stream));
+    RG_CUDA(cudaStreamSynchronize(ctx->copy_in));
+    RG_CUDA(cudaStreamSynchronize(ctx->copy_out));
+    // from the first step that overflowed on, nothing was written: those steps
+    // run again as ordinary calls (which size the plan afresh)
+    int redo = count;
+    for (int i = first; i < count && redo == count; i++) {
+        bool overflow = false;
+        RG_CHECK(wtowers_check(ctx, pl, &overflow, (const char *)ctx->pinned_steps + (size_t)i * 64));
+        if (overflow) redo = i;
+    }
+    for (int i = redo; i < count; i++)
+        RG_CHECK(grid_wtowers_impl(ctx, uvgrids[i], grid_size, theta, &vis[i], wkern, nullptr, S, M, winc, flags));
+    return RG_OK;
+}
+
 }  // namespace rg
 
 
@@ -873,6 +1024,14 @@ rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double
 {
     return rg::grid_wtowers_impl(ctx, uvgrid, grid_size, theta, vis, wkern, nullptr, subgrid_size, subgrid_margin,
                                  wincrement, flags);
+}
+
+rg_status rg_grid_wtowers_batch(rg_context *ctx, int count, double *const *uvgrids, int grid_size, double theta,
+                                const rg_vis *vis, const rg_wkern *wkern, int subgrid_size, int subgrid_margin,
+                                double wincrement, int flags)
+{
+    return rg::grid_wtowers_batch_impl(ctx, count, uvgrids, grid_size, theta, vis, wkern, subgrid_size,
+                                       subgrid_margin, wincrement, flags);
 }
 
 rg_status rg_weight(rg_context *ctx, int grid_size, double theta, const rg_vis *vis, double *vis_out)

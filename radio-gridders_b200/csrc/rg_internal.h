@@ -101,6 +101,12 @@ struct rg_context {
     cudaStream_t stream = nullptr;
     std::map<std::string, rg::Buffer> scratch;
     uint64_t scratch_gen = 0;  // bumped on every scratch (re)allocation: captured graphs go stale
+    // batched W-towers calls: copy streams, their events, per-step diagnostics
+    cudaStream_t copy_in = nullptr, copy_out = nullptr;
+    cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_used[2] = {nullptr, nullptr};
+    cudaEvent_t ev_done[2] = {nullptr, nullptr}, ev_out[2] = {nullptr, nullptr};
+    void *pinned_steps = nullptr;
+    size_t pinned_steps_bytes = 0;
     void *pinned = nullptr;  // small pinned host buffer (diagnostics read-back)
     bool autotune = true;    // tune W-towers schedules once per shape
     bool use_graphs = true;  // replay W-towers passes as CUDA graphs
@@ -247,7 +253,7 @@ int tower_row_strips(int subgrid);  // row strips per sub-grid in the row stage
 void launch_add_back(cudaStream_t s, const float2 *subimg, const int *tower_count,
                      double2 *master, int grid_size, int subgrid, int margin, int chunk,
                      int nchunk, int overwrite, const int *range, const int *counts, int slot_cap,
-                     int group_cap);
+                     int group_cap, int *poison = nullptr);
 
 // k_dft.cu
 void launch_dft(cudaStream_t s, const double *u, const double *v, const double *w,
