@@ -245,6 +245,12 @@ rg_status rg_write_vis_hdf5(const char *path, int n_bl, int n_time, int n_freq, 
                             const int *ant2, const double *time, const double *freq,
                             const double *uvw, const double *vis);
 rg_status rg_write_wkern_hdf5(const char *path, double theta, const rg_wkern *wk);
+/* The legacy flat layout (src/common/hdf5.c:199-300): /vis with attribute
+ * type = "Visibility" and rows of one time sample each — antenna1/antenna2
+ * [rows] int64, time [rows], uvw [rows][3] metres, frequency [nf] Hz (shared by
+ * all rows), vis [rows][nf][1] complex. */
+rg_status rg_write_vis_flat_hdf5(const char *path, int n_rows, int n_freq, const int *ant1, const int *ant2,
+                                 const double *time, const double *freq, const double *uvw, const double *vis);
 /* Generic access used for other crocodile files (e.g. the separable kernels
  * of src/common/hdf5.c:372-500): a float64 / int64 / {r, i} dataset by path
  * (out may be NULL to query dims; up to 8 dims; a compound element adds a

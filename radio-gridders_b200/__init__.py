@@ -43,7 +43,7 @@ EXPORTS = [
     "rg_grid_wprojection_noalloc", "rg_mlp_param_count", "rg_mlp_create", "rg_mlp_destroy",
     "rg_mlp_set_params", "rg_mlp_get_params", "rg_mlp_gradient", "rg_mlp_train", "rg_mlp_eval",
     "rg_grid_wprojection_learned", "rg_grid_wtowers_learned", "rg_grid_wtowers_batch", "rg_read_vis_hdf5", "rg_free_vis_data", "rg_read_wkern_hdf5",
-    "rg_free_wkern_data", "rg_write_vis_hdf5", "rg_write_wkern_hdf5", "rg_hdf5_read_f64",
+    "rg_free_wkern_data", "rg_write_vis_hdf5", "rg_write_vis_flat_hdf5", "rg_write_wkern_hdf5", "rg_hdf5_read_f64",
     "rg_hdf5_attr_f64",
 ]
 
@@ -131,6 +131,7 @@ def lib():
         L.rg_free_wkern_data.restype = None
         L.rg_write_vis_hdf5.argtypes = [ct.c_char_p, i, i, i, vp, vp, vp, vp, vp, vp]
         L.rg_write_wkern_hdf5.argtypes = [ct.c_char_p, d, ct.POINTER(_WKern)]
+        L.rg_write_vis_flat_hdf5.argtypes = [ct.c_char_p, i, i, vp, vp, vp, vp, vp, vp]
         L.rg_hdf5_read_f64.argtypes = [ct.c_char_p, ct.c_char_p, vp, i64, ct.POINTER(i64), ct.POINTER(i)]
         L.rg_hdf5_attr_f64.argtypes = [ct.c_char_p, ct.c_char_p, ct.c_char_p, ct.POINTER(d)]
         for name in EXPORTS:
@@ -503,6 +504,20 @@ def write_vis_hdf5(path, ant1, ant2, time, freq, uvw, vis):
     t = np.ascontiguousarray(time, np.float64).reshape(n_bl, n_time)
     _check(lib().rg_write_vis_hdf5(os.fsencode(path), n_bl, n_time, freq.shape[1], _ptr(a1), _ptr(a2),
                                    _ptr(t), _ptr(freq), _ptr(uvw), _ptr(vis)))
+
+
+def write_vis_flat_hdf5(path, ant1, ant2, time, freq, uvw, vis):
+    """Legacy flat visibility file: one row per time sample, uvw [rows, 3]
+    metres, a shared frequency axis freq [nf] Hz, vis [rows, nf] complex."""
+    uvw = np.ascontiguousarray(uvw, np.float64).reshape(-1, 3)
+    rows = uvw.shape[0]
+    freq = np.ascontiguousarray(freq, np.float64).ravel()
+    vis = np.ascontiguousarray(vis, np.complex128).reshape(rows, freq.size)
+    a1 = np.ascontiguousarray(ant1, np.int32)
+    a2 = np.ascontiguousarray(ant2, np.int32)
+    t = np.ascontiguousarray(time, np.float64).ravel()
+    _check(lib().rg_write_vis_flat_hdf5(os.fsencode(path), rows, freq.size, _ptr(a1), _ptr(a2), _ptr(t), _ptr(freq),
+                                        _ptr(uvw), _ptr(vis)))
 
 
 def write_wkern_hdf5(path, theta, wkern):

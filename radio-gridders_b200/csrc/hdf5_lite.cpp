@@ -560,6 +560,7 @@ struct Writer::Node {
     int kind = 0;  // 1 f64, 2 i64, 3 c128
     std::vector<uint8_t> data;
     std::vector<std::pair<std::string, double>> attrs;
+    std::vector<std::pair<std::string, std::string>> sattrs;
     uint64_t ohdr = 0;
 };
 
@@ -611,6 +612,11 @@ void Writer::add_dataset_c128(int parent, const std::string &name, const std::ve
 }
 
 void Writer::add_attr_f64(int group, const std::string &name, double v) { nodes_[group]->attrs.emplace_back(name, v); }
+
+void Writer::add_attr_str(int group, const std::string &name, const std::string &v)
+{
+    nodes_[group]->sattrs.emplace_back(name, v);
+}
 
 bool Writer::write(const std::string &path, std::string *err)
 {
@@ -738,9 +744,27 @@ bool Writer::write(const std::string &path, std::string *err)
             m.insert(m.end(), val, val + 8);
             message(area, 0x000C, m);
         }
+        for (auto &at : n->sattrs) {
+            // attribute message v1: string datatype (class 3, version 1, null
+            // terminated ASCII, no properties: 8 bytes), scalar dataspace
+            const uint32_t len = (uint32_t)at.second.size() + 1;
+            std::vector<uint8_t> m = {1, 0, (uint8_t)(at.first.size() + 1), 0, 8, 0, 8, 0};
+            std::vector<uint8_t> nm(at.first.begin(), at.first.end());
+            nm.resize(pad8(at.first.size() + 1), 0);
+            m.insert(m.end(), nm.begin(), nm.end());
+            const uint8_t dt[8] = {0x13, 0, 0, 0, (uint8_t)len, (uint8_t)(len >> 8), (uint8_t)(len >> 16),
+                                   (uint8_t)(len >> 24)};
+            m.insert(m.end(), dt, dt + 8);
+            const uint8_t space[8] = {1, 0, 0, 0, 0, 0, 0, 0};
+            m.insert(m.end(), space, space + 8);
+            std::vector<uint8_t> val(at.second.begin(), at.second.end());
+            val.push_back(0);
+            m.insert(m.end(), val.begin(), val.end());
+            message(area, 0x000C, m);
+        }
         const uint64_t hdr = o.alloc(16 + area.size());
         o.b[hdr] = 1;
-        o.put(hdr + 2, 1 + n->attrs.size(), 2);
+        o.put(hdr + 2, 1 + n->attrs.size() + n->sattrs.size(), 2);
         o.put(hdr + 4, 1, 4);
         o.put(hdr + 8, area.size(), 4);
         std::memcpy(o.b.data() + hdr + 16, area.data(), area.size());

@@ -82,6 +82,8 @@ public:
     void add_dataset_c128(int parent, const std::string &name, const std::vector<uint64_t> &dims,
                           const double *interleaved);
     void add_attr_f64(int group, const std::string &name, double v);
+    // fixed-length, null-terminated ASCII string attribute
+    void add_attr_str(int group, const std::string &name, const std::string &v);
     bool write(const std::string &path, std::string *err);
 
 private:

@@ -276,6 +276,26 @@ rg_status rg_write_vis_hdf5(const char *path, int n_bl, int n_time, int n_freq, 
     return RG_OK;
 }
 
+rg_status rg_write_vis_flat_hdf5(const char *path, int n_rows, int n_freq, const int *ant1, const int *ant2,
+                                 const double *time, const double *freq, const double *uvw, const double *vis)
+{
+    if (!path || n_rows < 0 || n_freq < 1 || (n_rows > 0 && (!ant1 || !ant2 || !time || !freq || !uvw || !vis)))
+        return fail(RG_ERR_INVALID_ARGUMENT, "bad visibility arrays");
+    h5::Writer wr;
+    const int vg = wr.add_group(0, "vis");
+    wr.add_attr_str(vg, "type", "Visibility");
+    std::vector<int64_t> a1(ant1, ant1 + n_rows), a2(ant2, ant2 + n_rows);
+    wr.add_dataset_i64(vg, "antenna1", {(uint64_t)n_rows}, a1.data());
+    wr.add_dataset_i64(vg, "antenna2", {(uint64_t)n_rows}, a2.data());
+    wr.add_dataset_f64(vg, "frequency", {(uint64_t)n_freq}, freq);
+    wr.add_dataset_f64(vg, "time", {(uint64_t)n_rows}, time);
+    wr.add_dataset_f64(vg, "uvw", {(uint64_t)n_rows, 3}, uvw);
+    wr.add_dataset_c128(vg, "vis", {(uint64_t)n_rows, (uint64_t)n_freq, 1}, vis);
+    std::string err;
+    if (!wr.write(path, &err)) return fail(RG_ERR_IO, err);
+    return RG_OK;
+}
+
 rg_status rg_write_wkern_hdf5(const char *path, double theta, const rg_wkern *wk)
 {
     if (!path || !wk || !wk->data || wk->plane_count < 1 || wk->size < 1 || wk->oversampling < 1)

@@ -118,3 +118,27 @@ def test_reads_libhdf5_written_files(rg, rel, shape):
     assert np.isfinite(kern).all() and np.abs(kern).max() > 0
     for name in ("du", "dw", "x0"):
         assert np.isfinite(rg.hdf5_attr(path, "/", name))
+
+
+def test_legacy_flat_layout_round_trip(rg, obs, tmp_path):
+    """The legacy flat /vis group (rows of one time sample, a shared frequency
+    axis, type attribute "Visibility"; src/common/hdf5.c:199-300): every row is
+    its own baseline for the length cut."""
+    n_bl, n_time = obs.uvw.shape[:2]
+    rows = n_bl * n_time
+    p = tmp_path / "flat.h5"
+    rg.write_vis_flat_hdf5(str(p), np.repeat(obs.antenna1, n_time), np.repeat(obs.antenna2, n_time),
+                           np.tile(obs.time, n_bl), obs.freq[0], obs.uvw.reshape(rows, 3),
+                           obs.vis.reshape(rows, -1))
+    vis, n_rows = rg.read_vis_hdf5(str(p))
+    u, v, w, x = obs.flat()
+    assert n_rows == rows
+    for a, b in ((vis.u, u), (vis.v, v), (vis.w, w), (vis.vis, x)):
+        np.testing.assert_array_equal(a, b)
+    import ctypes as ct
+    buf = ct.c_double()
+    assert rg.lib().rg_hdf5_attr_f64(str(p).encode(), b"vis", b"type", ct.byref(buf)) == 5  # a string
+    length = np.sqrt((obs.uvw.reshape(rows, 3)[:, :2] ** 2).sum(-1))
+    lo = np.quantile(length, 0.5)
+    _, kept = rg.read_vis_hdf5(str(p), lo)
+    assert kept == int((length >= lo).sum())
