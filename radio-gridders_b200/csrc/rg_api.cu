@@ -957,6 +957,16 @@ rg_status grid_wtowers_batch_impl(rg_context *ctx, int count, double *const *uvg
     RG_CUDA(cudaEventRecord(ctx->ev_done[0], ctx->stream));
     RG_CUDA(cudaStreamWaitEvent(ctx->copy_in, ctx->ev_done[0], 0));
     RG_CUDA(cudaStreamWaitEvent(ctx->copy_out, ctx->ev_done[0], 0));
+    // on any early return, leave no copy or pass of this batch in flight
+    struct Quiesce {
+        rg_context *c;
+        ~Quiesce()
+        {
+            cudaStreamSynchronize(c->stream);
+            cudaStreamSynchronize(c->copy_in);
+            cudaStreamSynchronize(c->copy_out);
+        }
+    } quiesce{ctx};
     bool used[2] = {false, false}, out_pending[2] = {false, false};
     for (int i = first; i < count; i++) {
         const int b = i & 1;
