@@ -95,7 +95,7 @@ def towers_image_error(ctx, oversampling=8, w_step=1.0):
             "region": "central half of each axis", "dft_s": time.time() - t0}
 
 
-def learned_towers(ctx, config="C1", steps=20000, n_triples=4096):
+def learned_towers(ctx, config="C1", steps=60000, n_triples=8192):
     """Learned-kernel W-towers against the table W-towers on the same
     workload: a network trained on the GPU (own forward/backward kernels) on
     generator kernels over the residual w range |w - w_mid| <= winc/2, then
@@ -112,7 +112,7 @@ def learned_towers(ctx, config="C1", steps=20000, n_triples=4096):
     u, v, w, vis = obs.flat()
     t0 = time.time()
     mlp, losses = _learned.train(ctx, wmax=half + 1.0, theta=th, ksize=16, n_triples=n_triples, steps=steps,
-                                 batch=16384, lr_max=4e-3)
+                                 batch=32768, lr_max=2e-3)
     train_s = time.time() - t0
     err, held = _learned.tap_error(mlp, wmax=half + 1.0, theta=th)
     wk = _sim.generate_wkernel(th, np.arange(-half - 1.0, half + 1.5, 1.0), 16, 32)
