@@ -125,6 +125,15 @@ __device__ __forceinline__ void zero_acc(float (&acc)[WM / 16][WN / 8][4])
 }
 
 __device__ __forceinline__ float silu_f(float z) { return z / (1.f + __expf(-z)); }
+// Inference SiLU: z * sigmoid(z) = z * (1 + tanh(z / 2)) / 2 with the hardware
+// tanh approximation (one MUFU op; its ~2^-11 relative error is below the
+// BF16 rounding of the activation it feeds).
+__device__ __forceinline__ float silu_fast(float z)
+{
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(0.5f * z));
+    return 0.5f * z * (1.f + t);
+}
 __device__ __forceinline__ float dsilu_f(float z)
 {
     const float s = 1.f / (1.f + __expf(-z));
@@ -157,9 +166,45 @@ __device__ __forceinline__ void tap_features(float w, float du, float dv, float 
     for (int k = MNFEAT; k < MFIN; k++) f[k] = __float2bfloat16(0.f);
 }
 
+// The same features from per-visibility tables: the Fourier terms depend on
+// the tap only through p = tx - K/2 - du (q likewise), so a visibility needs
+// them at K values of each; tab[t*8 + 2(k-1)], tab[t*8 + 2(k-1) + 1] = cos,
+// sin(pi k p_t / (K/2 + 1)) for tap index t.
+__device__ __forceinline__ void axis_table(float d, int t, int ksize, float *tab)
+{
+    const float half = 0.5f * (float)ksize;
+    const float p = (float)t - half - d, inv = 1.f / (half + 1.f);
+#pragma unroll
+    for (int k = 1; k <= 4; k++) {
+        float sn, cs;
+        sincospif((float)k * p * inv, &sn, &cs);
+        tab[t * 8 + 2 * (k - 1)] = cs;
+        tab[t * 8 + 2 * (k - 1) + 1] = sn;
+    }
+}
+
+__device__ __forceinline__ void tap_features_tab(float w, float du, float dv, int tx, int ty, int ksize,
+                                                 float inv_wmax, const float *ptab, const float *qtab, bf16 *f)
+{
+    const float half = 0.5f * (float)ksize;
+    const float p = (float)tx - half - du, q = (float)ty - half - dv;
+    f[0] = __float2bfloat16(w * inv_wmax);
+    f[1] = __float2bfloat16(2.f * du - 1.f);
+    f[2] = __float2bfloat16(2.f * dv - 1.f);
+    f[3] = __float2bfloat16(p / half);
+    f[4] = __float2bfloat16(q / half);
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        f[5 + j] = __float2bfloat16(ptab[tx * 8 + j]);
+        f[13 + j] = __float2bfloat16(qtab[ty * 8 + j]);
+    }
+#pragma unroll
+    for (int k = MNFEAT; k < MFIN; k++) f[k] = __float2bfloat16(0.f);
+}
+
 // Epilogue of a 32x32 (per warp) hidden-layer tile: z = acc + b; Z (fp32,
 // optional) and H = bf16(silu(z)).
-template <int WM, int WN>
+template <int WM, int WN, bool FAST = false>
 __device__ __forceinline__ void hidden_epilogue(const float (&acc)[WM / 16][WN / 8][4], int m0, int n0,
                                                 const float *__restrict__ bias, float *Z, bf16 *Hout)
 {
@@ -175,8 +220,9 @@ __device__ __forceinline__ void hidden_epilogue(const float (&acc)[WM / 16][WN /
                 const float z0 = acc[mi][ni][2 * h] + bias[c];
                 const float z1 = acc[mi][ni][2 * h + 1] + bias[c + 1];
                 if (Z) *reinterpret_cast<float2 *>(Z + r * LDZ + c) = make_float2(z0, z1);
+                const float h0 = FAST ? silu_fast(z0) : silu_f(z0), h1 = FAST ? silu_fast(z1) : silu_f(z1);
                 *reinterpret_cast<uint32_t *>(Hout + r * LDH + c) =
-                    pack_bf16(__float2bfloat16(silu_f(z0)), __float2bfloat16(silu_f(z1)));
+                    pack_bf16(__float2bfloat16(h0), __float2bfloat16(h1));
             }
 }
 
@@ -391,6 +437,7 @@ struct InferSmem {
     bf16 F[IR * LDF];
     bf16 H[2][IR * LDH];
     float2 Y[IR];
+    float ftab[2][32 * 8];  // per-visibility Fourier terms (learned_scatter)
 };
 
 // Rows of S.F -> S.Y (taps / out_scale).  All threads of the block.
@@ -403,21 +450,21 @@ __device__ __forceinline__ void mlp_forward_rows(InferSmem &S, const float *__re
         float acc[4][4][4];
         zero_acc<64, 32>(acc);
         warp_gemm<64, 32, false, true>(S.F, LDF, PB + BOFF_W1T, MFIN, MFIN, m0, n0, acc);
-        hidden_epilogue<64, 32>(acc, m0, n0, P + OFF_B1, nullptr, S.H[0]);
+        hidden_epilogue<64, 32, true>(acc, m0, n0, P + OFF_B1, nullptr, S.H[0]);
     }
     __syncthreads();
     {
         float acc[4][4][4];
         zero_acc<64, 32>(acc);
         warp_gemm<64, 32, false, true>(S.H[0], LDH, PB + BOFF_W2T, MH, MH, m0, n0, acc);
-        hidden_epilogue<64, 32>(acc, m0, n0, P + OFF_B2, nullptr, S.H[1]);
+        hidden_epilogue<64, 32, true>(acc, m0, n0, P + OFF_B2, nullptr, S.H[1]);
     }
     __syncthreads();
     {
         float acc[4][4][4];
         zero_acc<64, 32>(acc);
         warp_gemm<64, 32, false, true>(S.H[1], LDH, PB + BOFF_W3T, MH, MH, m0, n0, acc);
-        hidden_epilogue<64, 32>(acc, m0, n0, P + OFF_B3, nullptr, S.H[0]);
+        hidden_epilogue<64, 32, true>(acc, m0, n0, P + OFF_B3, nullptr, S.H[0]);
     }
     __syncthreads();
     // output layer: two threads per row, half of k each, combined by shuffle
@@ -481,12 +528,15 @@ __device__ __forceinline__ void learned_scatter(InferSmem &S, const float *__res
                                                 int strip_lg = 0)
 {
     const int taps = ksize * ksize;
+    if (threadIdx.x < ksize) axis_table(du, threadIdx.x, ksize, S.ftab[0]);
+    else if (threadIdx.x >= 32 && threadIdx.x < 32 + ksize) axis_table(dv, threadIdx.x - 32, ksize, S.ftab[1]);
+    __syncthreads();
     for (int t0 = 0; t0 < taps; t0 += IR) {
         if (threadIdx.x < IR) {
             const int t = t0 + threadIdx.x;
             if (t < taps)
-                tap_features(wf, du, dv, (float)(t % ksize), (float)(t / ksize), ksize, inv_wmax,
-                             S.F + threadIdx.x * LDF);
+                tap_features_tab(wf, du, dv, t % ksize, t / ksize, ksize, inv_wmax, S.ftab[0], S.ftab[1],
+                                 S.F + threadIdx.x * LDF);
             else
                 for (int k = 0; k < MFIN; k++) S.F[threadIdx.x * LDF + k] = __float2bfloat16(0.f);
         }

@@ -253,6 +253,21 @@ def baselines(ctx):
     return out
 
 
+def learned_small(ctx, stations=64, steps=2000):
+    """A short learned W-towers run (a briefly trained network, 2048^2, S 512,
+    margin 16, winc 10, `stations` stations) for profiling the learned
+    gridding kernel; prints its time and the visibility count."""
+    obs = _sim.wtowers_plain(n_st=stations)
+    u, v, w, vis = obs.flat()
+    mlp, _ = _learned.train(ctx, wmax=6.0, theta=0.1, ksize=16, n_triples=512, steps=steps, batch=16384,
+                            lr_max=4e-3)
+    g = np.zeros((2048, 2048), np.complex128)
+    V = _rg.Visibilities(u, v, w, vis)
+    ms = _events_ms(lambda: _rg.grid_wtowers_learned(ctx, mlp, g, 2048, 0.1, V, 512, 16, 10.0, flags=1),
+                    repeats=2)
+    return {"n_vis": len(u), "learned_ms": ms, "learned_vis_per_s": len(u) / (ms * 1e-3)}
+
+
 def main(which):
     ctx = _rg.Context(0)
     if which in ("dft", "all"):
@@ -272,6 +287,8 @@ def main(which):
                           "final_loss": losses[-1], **r}), flush=True)
 
 
+    if which == "learned_small":
+        print(json.dumps({"study": "learned_small", **learned_small(ctx)}), flush=True)
     if which == "baselines":
         print(json.dumps({"study": "baselines", **baselines(ctx)}), flush=True)
     if which in ("parity_c1", "parity_c4"):
