@@ -4,9 +4,11 @@
 // oversampled w-kernel tables, src/reference/grid.c:157-185): 21 input features
 // of a tap (w, sub-cell offsets du, dv, tap x, tap y and 16 Fourier features of
 // the tap's offset from the visibility) -> 128 -> 128 -> 128 (SiLU) -> 2
-// (complex tap / out_scale).  Layers 1-3 run as BF16 x BF16 -> FP32
-// mma.sync.m16n8k16 tiles from shared memory; the 128 -> 2 output layer and all
-// element-wise work are FP32.
+// (complex tap / out_scale).  Layers 1-3 are BF16 x BF16 -> FP32 products:
+// in inference (evaluation and both gridders) tcgen05 MMAs with TMEM
+// accumulators, in training mma.sync.m16n8k16 tiles (the backward pass needs
+// the activations and gradients in registers and shared memory anyway); the
+// 128 -> 2 output layer and all element-wise work are FP32.
 //
 // Parameters: one FP32 buffer, W1[32][128] (rows >= 21 unused), b1[128],
 // W2[128][128], b2, W3[128][128], b3, W4[128][2], b4[2] (W[in][out]); plus BF16
@@ -125,15 +127,6 @@ __device__ __forceinline__ void zero_acc(float (&acc)[WM / 16][WN / 8][4])
 }
 
 __device__ __forceinline__ float silu_f(float z) { return z / (1.f + __expf(-z)); }
-// Inference SiLU: z * sigmoid(z) = z * (1 + tanh(z / 2)) / 2 with the hardware
-// tanh approximation (one MUFU op; its ~2^-11 relative error is below the
-// BF16 rounding of the activation it feeds).
-__device__ __forceinline__ float silu_fast(float z)
-{
-    float t;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(0.5f * z));
-    return 0.5f * z * (1.f + t);
-}
 __device__ __forceinline__ float dsilu_f(float z)
 {
     const float s = 1.f / (1.f + __expf(-z));
@@ -204,7 +197,7 @@ __device__ __forceinline__ void tap_features_tab(float w, float du, float dv, in
 
 // Epilogue of a 32x32 (per warp) hidden-layer tile: z = acc + b; Z (fp32,
 // optional) and H = bf16(silu(z)).
-template <int WM, int WN, bool FAST = false>
+template <int WM, int WN>
 __device__ __forceinline__ void hidden_epilogue(const float (&acc)[WM / 16][WN / 8][4], int m0, int n0,
                                                 const float *__restrict__ bias, float *Z, bf16 *Hout)
 {
@@ -220,9 +213,8 @@ __device__ __forceinline__ void hidden_epilogue(const float (&acc)[WM / 16][WN /
                 const float z0 = acc[mi][ni][2 * h] + bias[c];
                 const float z1 = acc[mi][ni][2 * h + 1] + bias[c + 1];
                 if (Z) *reinterpret_cast<float2 *>(Z + r * LDZ + c) = make_float2(z0, z1);
-                const float h0 = FAST ? silu_fast(z0) : silu_f(z0), h1 = FAST ? silu_fast(z1) : silu_f(z1);
                 *reinterpret_cast<uint32_t *>(Hout + r * LDH + c) =
-                    pack_bf16(__float2bfloat16(h0), __float2bfloat16(h1));
+                    pack_bf16(__float2bfloat16(silu_f(z0)), __float2bfloat16(silu_f(z1)));
             }
 }
 
@@ -429,174 +421,438 @@ __global__ void mlp_to_bf16_kernel(const float *__restrict__ P, bf16 *__restrict
 }
 
 // ---------------------------------------------------------------------------
-// inference: 128 rows per pass
+// Inference on the 5th-generation tensor cores (tcgen05).  Rows (taps) go in
+// tiles of 128; each hidden layer is an M = 128, N = 128 BF16 x BF16 -> FP32
+// product issued as K = 16 steps by one thread from shared-memory operands
+// into an accumulator in tensor memory (TMEM), and its epilogue (bias, SiLU,
+// BF16 pack back into shared memory as the next layer's A operand) is done by
+// the tile's 128 threads, each owning one TMEM lane (row).  The 128 -> 2
+// output layer runs in FP32 in the last epilogue.
+//
+// A CTA (one per SM) holds one copy of W1..W3 (72 KB) and runs TC_GROUPS
+// independent tile groups of four warps, each with its own feature / hidden
+// buffers, mbarrier and 128 TMEM columns: while one group's epilogue runs on
+// the CUDA cores, another group's MMAs run on the tensor core.
+//
+// Operands use the K-major layout without swizzle: 8-row x 16-byte core
+// matrices, rows 16 bytes apart, the two core matrices of a K = 16 step
+// 128 bytes apart (leading byte offset), 8-row groups K * 16 bytes apart
+// (stride byte offset).
 // ---------------------------------------------------------------------------
-constexpr int IR = 128;
+constexpr int IR = 128;  // rows per tile
+constexpr int TC_GROUPS = 2;
+constexpr int TC_THREADS = TC_GROUPS * IR;
+constexpr int TC_KMAX = 16;  // largest kernel support (feature tables)
 
-struct InferSmem {
-    bf16 F[IR * LDF];
-    bf16 H[2][IR * LDH];
-    float2 Y[IR];
-    float ftab[2][32 * 8];  // per-visibility Fourier terms (learned_scatter)
-};
-
-// Rows of S.F -> S.Y (taps / out_scale).  All threads of the block.
-__device__ __forceinline__ void mlp_forward_rows(InferSmem &S, const float *__restrict__ P,
-                                                 const bf16 *__restrict__ PB)
+__host__ __device__ constexpr int core_off(int row, int k, int K)
 {
-    const int warp = threadIdx.x >> 5;
-    const int m0 = (warp >> 2) * 64, n0 = (warp & 3) * 32;
-    {
-        float acc[4][4][4];
-        zero_acc<64, 32>(acc);
-        warp_gemm<64, 32, false, true>(S.F, LDF, PB + BOFF_W1T, MFIN, MFIN, m0, n0, acc);
-        hidden_epilogue<64, 32, true>(acc, m0, n0, P + OFF_B1, nullptr, S.H[0]);
+    return (row >> 3) * (K * 16) + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2;
+}
+
+struct TcSmem {
+    alignas(16) unsigned char W1[MH * MFIN * 2];  // B operands: W^T [out][in], K-major
+    alignas(16) unsigned char W2[MH * MH * 2];
+    alignas(16) unsigned char W3[MH * MH * 2];
+    alignas(16) unsigned char F[TC_GROUPS][IR * MFIN * 2];  // A of layer 1 (features)
+    alignas(16) unsigned char H[TC_GROUPS][IR * MH * 2];    // A of layers 2, 3 (activations)
+    float hb[3][MH];                                         // b1..b3 / 2
+    float2 w4[MH];
+    float ftab[TC_GROUPS][2][TC_KMAX * 8];  // per-visibility Fourier terms
+    unsigned long long bar[TC_GROUPS];
+    int abort_flag[TC_GROUPS];
+    uint32_t tmem_base;
+};
+static_assert(sizeof(TcSmem) <= 227 * 1024, "tensor-core inference shared memory");
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor: start address, leading and stride byte
+// offsets (all >> 4), descriptor version 1, base offset 0, no swizzle.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
+{
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor, kind::f16: FP32 accumulator (bits 4-5 = 1), A and B
+// BF16 (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+constexpr uint32_t kIdescBf16 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(MH >> 3) << 17) |
+                                ((uint32_t)(IR >> 4) << 24);
+
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+        :
+        : "r"(d_tmem), "l"(a), "l"(b), "r"(kIdescBf16), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void group_sync(int g)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(IR) : "memory");
+}
+
+// Bounded wait for the completion of the mbarrier phase with this parity
+// (about two seconds of SM clock); false when it did not complete.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+{
+    const long long t0 = clock64();
+    for (;;) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > (1ll << 32)) return false;
     }
-    __syncthreads();
-    {
-        float acc[4][4][4];
-        zero_acc<64, 32>(acc);
-        warp_gemm<64, 32, false, true>(S.H[0], LDH, PB + BOFF_W2T, MH, MH, m0, n0, acc);
-        hidden_epilogue<64, 32, true>(acc, m0, n0, P + OFF_B2, nullptr, S.H[1]);
+}
+
+// 32 consecutive FP32 columns of this thread's TMEM lane (32x32b shape: the
+// warp reads lanes 32 (warp % 4) .. + 31).
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]),
+          "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+          "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// SiLU from the half pre-activation hz = z / 2: z sigmoid(z) = hz (1 + tanh hz),
+// with the hardware tanh approximation (one MUFU op; its ~2^-11 relative error
+// is below the BF16 rounding of the activation it feeds).
+__device__ __forceinline__ float silu_half(float hz)
+{
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(hz));
+    return fmaf(hz, t, hz);
+}
+
+// CTA prologue: weights into the core-matrix layout, biases, mbarriers and
+// TMEM columns (warp 0 allocates TC_GROUPS * 128 columns).
+__device__ __forceinline__ void tc_prologue(TcSmem &S, const float *__restrict__ P, const bf16 *__restrict__ PB)
+{
+    for (int c = threadIdx.x; c < MH * (MFIN / 8); c += blockDim.x) {
+        const int row = c / (MFIN / 8), kc = c % (MFIN / 8);
+        *reinterpret_cast<uint4 *>(S.W1 + core_off(row, kc * 8, MFIN)) =
+            *reinterpret_cast<const uint4 *>(PB + BOFF_W1T + row * MFIN + kc * 8);
     }
-    __syncthreads();
-    {
-        float acc[4][4][4];
-        zero_acc<64, 32>(acc);
-        warp_gemm<64, 32, false, true>(S.H[1], LDH, PB + BOFF_W3T, MH, MH, m0, n0, acc);
-        hidden_epilogue<64, 32, true>(acc, m0, n0, P + OFF_B3, nullptr, S.H[0]);
+    for (int c = threadIdx.x; c < MH * (MH / 8); c += blockDim.x) {
+        const int row = c / (MH / 8), kc = c % (MH / 8);
+        *reinterpret_cast<uint4 *>(S.W2 + core_off(row, kc * 8, MH)) =
+            *reinterpret_cast<const uint4 *>(PB + BOFF_W2T + row * MH + kc * 8);
+        *reinterpret_cast<uint4 *>(S.W3 + core_off(row, kc * 8, MH)) =
+            *reinterpret_cast<const uint4 *>(PB + BOFF_W3T + row * MH + kc * 8);
     }
+    for (int n = threadIdx.x; n < MH; n += blockDim.x) {
+        S.hb[0][n] = 0.5f * P[OFF_B1 + n];
+        S.hb[1][n] = 0.5f * P[OFF_B2 + n];
+        S.hb[2][n] = 0.5f * P[OFF_B3 + n];
+        S.w4[n] = make_float2(P[OFF_W4 + 2 * n], P[OFF_W4 + 2 * n + 1]);
+    }
+    if (threadIdx.x < TC_GROUPS) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&S.bar[threadIdx.x])) : "memory");
+        S.abort_flag[threadIdx.x] = 0;
+    }
+    if (threadIdx.x == 0) asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    if (threadIdx.x < 32) {
+        constexpr uint32_t cols = TC_GROUPS * IR <= 256 ? 256 : 512;
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&S.tmem_base)),
+                     "r"(cols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_async_smem();
+    tc_fence_before();
     __syncthreads();
-    // output layer: two threads per row, half of k each, combined by shuffle
-    {
-        const int r = threadIdx.x >> 1, half = threadIdx.x & 1;
-        float y0 = 0.f, y1 = 0.f;
-        const bf16 *h = S.H[0] + r * LDH + half * 64;
-        const float *w4 = P + OFF_W4 + half * 64 * 2;
-#pragma unroll 8
-        for (int k = 0; k < 64; k++) {
-            const float hv = __bfloat162float(h[k]);
-            y0 = fmaf(hv, w4[2 * k], y0);
-            y1 = fmaf(hv, w4[2 * k + 1], y1);
+    tc_fence_after();
+}
+
+__device__ __forceinline__ void tc_epilogue(TcSmem &S)
+{
+    tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        tc_fence_after();
+        constexpr uint32_t cols = TC_GROUPS * IR <= 256 ? 256 : 512;
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(S.tmem_base), "r"(cols)
+                     : "memory");
+    }
+}
+
+// Row r of a tile: features into the group's A buffer (core layout, K = 32).
+__device__ __forceinline__ void tc_store_features(unsigned char *F, int r, const bf16 (&f)[MFIN])
+{
+#pragma unroll
+    for (int j = 0; j < MFIN / 8; j++) {
+        uint4 q;
+        q.x = pack_bf16(f[8 * j + 0], f[8 * j + 1]);
+        q.y = pack_bf16(f[8 * j + 2], f[8 * j + 3]);
+        q.z = pack_bf16(f[8 * j + 4], f[8 * j + 5]);
+        q.w = pack_bf16(f[8 * j + 6], f[8 * j + 7]);
+        *reinterpret_cast<uint4 *>(F + core_off(r, 8 * j, MFIN)) = q;
+    }
+}
+
+// Issue one hidden layer (K / 16 MMA steps) and commit it to the group's
+// mbarrier.  One thread.
+__device__ __forceinline__ void tc_issue_layer(uint32_t d_tmem, const unsigned char *A, const unsigned char *B, int K,
+                                               uint32_t bar)
+{
+    tc_fence_after();
+    const uint32_t a = smem_u32(A), b = smem_u32(B);
+    for (int s = 0; s < K / 16; s++)
+        umma_bf16(d_tmem, umma_desc(a + s * 256, 128, K * 16), umma_desc(b + s * 256, 128, K * 16), s > 0);
+    umma_commit(bar);
+}
+
+// Hidden epilogue of row r: TMEM accumulator -> SiLU(z + b) as BF16 into H.
+__device__ __forceinline__ void tc_hidden_epilogue(uint32_t taddr, const float *__restrict__ hb, unsigned char *H,
+                                                   int r)
+{
+#pragma unroll 1
+    for (int c = 0; c < MH / 32; c++) {
+        uint32_t v[32];
+        tmem_ld32(taddr + c * 32, v);
+        tmem_wait_ld();
+        uint32_t pk[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const float h0 = silu_half(fmaf(__uint_as_float(v[2 * j]), 0.5f, hb[c * 32 + 2 * j]));
+            const float h1 = silu_half(fmaf(__uint_as_float(v[2 * j + 1]), 0.5f, hb[c * 32 + 2 * j + 1]));
+            pk[j] = pack_bf16(__float2bfloat16(h0), __float2bfloat16(h1));
         }
-        y0 += __shfl_xor_sync(0xffffffffu, y0, 1);
-        y1 += __shfl_xor_sync(0xffffffffu, y1, 1);
-        if (half == 0) S.Y[r] = make_float2(y0 + P[OFF_B4], y1 + P[OFF_B4 + 1]);
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            *reinterpret_cast<uint4 *>(H + core_off(r, c * 32 + 8 * j, MH)) =
+                make_uint4(pk[4 * j], pk[4 * j + 1], pk[4 * j + 2], pk[4 * j + 3]);
     }
-    __syncthreads();
+}
+
+// Output epilogue of row r: SiLU(z + b3) rounded to BF16, times W4, plus b4.
+__device__ __forceinline__ float2 tc_output_epilogue(uint32_t taddr, const float *__restrict__ hb,
+                                                     const float2 *__restrict__ w4, float2 b4)
+{
+    float y0 = b4.x, y1 = b4.y;
+#pragma unroll 1
+    for (int c = 0; c < MH / 32; c++) {
+        uint32_t v[32];
+        tmem_ld32(taddr + c * 32, v);
+        tmem_wait_ld();
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+            const float h = __bfloat162float(
+                __float2bfloat16(silu_half(fmaf(__uint_as_float(v[j]), 0.5f, hb[c * 32 + j]))));
+            const float2 wv = w4[c * 32 + j];
+            y0 = fmaf(h, wv.x, y0);
+            y1 = fmaf(h, wv.y, y1);
+        }
+    }
+    return make_float2(y0, y1);
+}
+
+// The network on the 128 feature rows the group has just stored in S.F[g]:
+// returns row r's output (tap / out_scale).  All threads of group g.  On a
+// wait that timed out the error word gets DERR_TIMEOUT and *ok turns false
+// for the whole group (read after a group barrier).
+__device__ __forceinline__ float2 tc_tile(TcSmem &S, int g, int r, uint32_t &phase, float2 b4,
+                                          unsigned *__restrict__ err, bool *ok)
+{
+    const uint32_t bar = smem_u32(&S.bar[g]);
+    const uint32_t d_tmem = S.tmem_base + (uint32_t)(g * IR);
+    const uint32_t taddr = d_tmem + ((uint32_t)((r >> 5) * 32) << 16);
+    float2 y = make_float2(0.f, 0.f);
+    fence_async_smem();
+    tc_fence_before();
+    group_sync(g);
+    if (S.abort_flag[g]) {
+        *ok = false;
+        return y;
+    }
+#pragma unroll 1
+    for (int layer = 0; layer < 3; layer++) {
+        if (r == 0) {
+            if (layer == 0) tc_issue_layer(d_tmem, S.F[g], S.W1, MFIN, bar);
+            else tc_issue_layer(d_tmem, S.H[g], layer == 1 ? S.W2 : S.W3, MH, bar);
+        }
+        if (!mbar_wait(bar, phase)) {
+            S.abort_flag[g] = 1;
+            atomicOr(err, DERR_TIMEOUT);
+        }
+        phase ^= 1u;
+        tc_fence_after();
+        if (layer < 2) {
+            tc_hidden_epilogue(taddr, S.hb[layer], S.H[g], r);
+            fence_async_smem();
+            tc_fence_before();
+            group_sync(g);
+            if (S.abort_flag[g]) {
+                *ok = false;
+                return y;
+            }
+        } else {
+            y = tc_output_epilogue(taddr, S.hb[2], S.w4, b4);
+        }
+    }
+    return y;
 }
 
 // Evaluate taps at arbitrary inputs: in [5][n] -> out float2 (scaled taps).
-__global__ void __launch_bounds__(256) mlp_eval_kernel(const float *__restrict__ P, const bf16 *__restrict__ PB,
-                                                       const float *__restrict__ in, int n, int ksize,
-                                                       float inv_wmax, float scale, float2 *__restrict__ out)
+__global__ void __launch_bounds__(TC_THREADS, 1) mlp_eval_kernel(const float *__restrict__ P,
+                                                                  const bf16 *__restrict__ PB,
+                                                                  const float *__restrict__ in, int n, int ksize,
+                                                                  float inv_wmax, float scale,
+                                                                  float2 *__restrict__ out, unsigned *err)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    InferSmem &S = *reinterpret_cast<InferSmem *>(smem_raw);
-    for (int base = blockIdx.x * IR; base < n; base += gridDim.x * IR) {
-        if (threadIdx.x < IR) {
-            const int i = base + threadIdx.x;
-            if (i < n) tap_features(in[i], in[n + i], in[2 * n + i], in[3 * n + i], in[4 * n + i], ksize,
-                                    inv_wmax, S.F + threadIdx.x * LDF);
-            else
-                for (int k = 0; k < MFIN; k++) S.F[threadIdx.x * LDF + k] = __float2bfloat16(0.f);
-        }
-        __syncthreads();
-        mlp_forward_rows(S, P, PB);
-        if (threadIdx.x < IR && base + threadIdx.x < n) {
-            const float2 y = S.Y[threadIdx.x];
-            out[base + threadIdx.x] = make_float2(y.x * scale, y.y * scale);
-        }
-        __syncthreads();
+    TcSmem &S = *reinterpret_cast<TcSmem *>(smem_raw);
+    tc_prologue(S, P, PB);
+    const int g = threadIdx.x / IR, r = threadIdx.x % IR;
+    const float2 b4 = make_float2(P[OFF_B4], P[OFF_B4 + 1]);
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int base = (blockIdx.x * TC_GROUPS + g) * IR; base < n && ok; base += gridDim.x * TC_GROUPS * IR) {
+        const int i = base + r;
+        bf16 f[MFIN];
+        if (i < n) tap_features(in[i], in[n + i], in[2 * n + i], in[3 * n + i], in[4 * n + i], ksize, inv_wmax, f);
+        else
+            for (int k = 0; k < MFIN; k++) f[k] = __float2bfloat16(0.f);
+        tc_store_features(S.F[g], r, f);
+        const float2 y = tc_tile(S, g, r, phase, b4, err, &ok);
+        if (ok && i < n) out[i] = make_float2(y.x * scale, y.y * scale);
     }
+    tc_epilogue(S);
 }
 
 // ---------------------------------------------------------------------------
-// W-projection with learned taps.  Per visibility: x = theta u, cell =
-// floor(x), du = x - cell (continuous — no oversampling quantisation);
-// footprint column cell - K/2 + tx; taps from the network at (w, du, dv, tx,
-// ty); grid[idx] += vis * conj(tap) with the reference's linear index rule
-// (dropped outside [0, N^2)).  K = 16: two 128-row passes per visibility.
+// Gridding with learned taps.  A visibility's K x K taps are K*K / 128 tiles
+// (one half-filled tile for K = 8); tap t = ty * K + tx of the tile row is
+// scattered as grid[goff + ty * ld + tx] += vis * conj(tap) where that index
+// lies in [0, limit).  The groups of a CTA take visibilities in turn.
 // ---------------------------------------------------------------------------
-// One visibility: taps from the network in passes of IR rows, each scattered
-// as grid[goff + ty*ld + tx] += vis * conj(tap) where the index lies in
-// [0, limit).  All threads of the CTA take part (barriers inside).
-__device__ __forceinline__ void learned_scatter(InferSmem &S, const float *__restrict__ P,
-                                                const bf16 *__restrict__ PB, float wf, float du, float dv,
-                                                float vr, float vi, float2 *grid, int64_t goff, int64_t ld,
-                                                int64_t limit, int ksize, float inv_wmax, float scale,
-                                                int strip_lg = 0)
-{
-    const int taps = ksize * ksize;
-    if (threadIdx.x < ksize) axis_table(du, threadIdx.x, ksize, S.ftab[0]);
-    else if (threadIdx.x >= 32 && threadIdx.x < 32 + ksize) axis_table(dv, threadIdx.x - 32, ksize, S.ftab[1]);
-    __syncthreads();
-    for (int t0 = 0; t0 < taps; t0 += IR) {
-        if (threadIdx.x < IR) {
-            const int t = t0 + threadIdx.x;
-            if (t < taps)
-                tap_features_tab(wf, du, dv, t % ksize, t / ksize, ksize, inv_wmax, S.ftab[0], S.ftab[1],
-                                 S.F + threadIdx.x * LDF);
-            else
-                for (int k = 0; k < MFIN; k++) S.F[threadIdx.x * LDF + k] = __float2bfloat16(0.f);
-        }
-        __syncthreads();
-        mlp_forward_rows(S, P, PB);
-        if (threadIdx.x < IR) {
-            const int t = t0 + threadIdx.x;
-            const float2 k = S.Y[threadIdx.x];
-            const float kr = k.x * scale, ki = k.y * scale;
-            const int64_t idx = goff + (int64_t)(t / ksize) * ld + (t % ksize);
-            if (t < taps && idx >= 0 && idx < limit)
-                atomicAdd(grid + (strip_lg ? (int64_t)strip_addr((int)idx, strip_lg) : idx),
-                          make_float2(vr * kr + vi * ki, vi * kr - vr * ki));
-        }
-        __syncthreads();
-    }
-}
+struct LearnedVis {
+    float wf, du, dv, vr, vi;
+    float2 *grid;
+    int64_t goff, ld, limit;
+};
 
-__global__ void __launch_bounds__(256) learned_wproj_kernel(
-    const double *__restrict__ u, const double *__restrict__ v, const double *__restrict__ w,
-    const double2 *__restrict__ vis, int64_t nvis, int N, double theta, const float *__restrict__ P,
-    const bf16 *__restrict__ PB, int ksize, float inv_wmax, float scale, float2 *__restrict__ grid)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    InferSmem &S = *reinterpret_cast<InferSmem *>(smem_raw);
-    for (int64_t i = blockIdx.x; i < nvis; i += gridDim.x) {
+// W-projection: x = theta u, cell = floor(x), du = x - cell (continuous — no
+// oversampling quantisation); footprint column cell - K/2 + tx; the
+// reference's linear index rule (dropped outside [0, N^2)).
+struct WprojVisSource {
+    const double *u, *v, *w;
+    const double2 *vis;
+    int N, ksize;
+    double theta;
+    float2 *grid;
+    __device__ bool get(int64_t i, LearnedVis &o) const
+    {
         const double x = theta * u[i], y = theta * v[i];
         const double cx = floor(x), cy = floor(y);
         const double2 vz = vis[i];
-        const int64_t goff = ((int64_t)cy - ksize / 2 + N / 2) * N + ((int64_t)cx - ksize / 2 + N / 2);
-        learned_scatter(S, P, PB, (float)w[i], (float)(x - cx), (float)(y - cy), (float)vz.x, (float)vz.y, grid,
-                        goff, N, (int64_t)N * N, ksize, inv_wmax, scale);
+        o.goff = ((int64_t)cy - ksize / 2 + N / 2) * N + ((int64_t)cx - ksize / 2 + N / 2);
+        o.wf = (float)w[i];
+        o.du = (float)(x - cx);
+        o.dv = (float)(y - cy);
+        o.vr = (float)vz.x;
+        o.vi = (float)vz.y;
+        o.grid = grid;
+        o.ld = N;
+        o.limit = (int64_t)N * N;
+        return true;
     }
-}
+};
 
-// ---------------------------------------------------------------------------
-// W-towers with learned taps: the records of the tower binning (sub-grid slot
-// via slot_of_bin, footprint origin in the sub-grid) and the continuous
-// offsets feat = {w - w_mid, du, dv}; same scatter as above into the slot's
-// S x S sub-grid.
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) learned_towers_kernel(
-    const int4 *__restrict__ rec, const float2 *__restrict__ visf, const float4 *__restrict__ feat, int64_t nvis,
-    const int *__restrict__ slot_of_bin, int slot_cap, float2 *__restrict__ slots, int sub,
-    const float *__restrict__ P, const bf16 *__restrict__ PB, int ksize, float inv_wmax, float scale)
-{
-    const int strip_lg = __ffs(sub) - 1;  // sub-grids are strip-major (strip_addr)
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    InferSmem &S = *reinterpret_cast<InferSmem *>(smem_raw);
-    const int64_t cells = (int64_t)sub * sub;
-    for (int64_t i = blockIdx.x; i < nvis; i += gridDim.x) {
+// W-towers: the records of the tower binning (sub-grid slot via slot_of_bin,
+// footprint origin in the sub-grid) and the continuous offsets
+// feat = {w - w_mid, du, dv}; scattered into the slot's strip-major S x S
+// sub-grid.
+struct TowersVisSource {
+    const int4 *rec;
+    const float2 *visf;
+    const float4 *feat;
+    const int *slot_of_bin;
+    int slot_cap, sub;
+    float2 *slots;
+    __device__ bool get(int64_t i, LearnedVis &o) const
+    {
         const int4 r = rec[i];
-        if (r.x < 0) continue;  // uniform across the CTA
+        if (r.x < 0) return false;
         const int slot = slot_of_bin[r.x];
-        if (slot >= slot_cap) continue;
+        if (slot >= slot_cap) return false;
         const float4 f = feat[i];
         const float2 vz = visf[i];
-        learned_scatter(S, P, PB, f.x, f.y, f.z, vz.x, vz.y, slots + (int64_t)slot * cells, r.y, sub, cells, ksize,
-                        inv_wmax, scale, strip_lg);
+        o.wf = f.x;
+        o.du = f.y;
+        o.dv = f.z;
+        o.vr = vz.x;
+        o.vi = vz.y;
+        o.grid = slots + (int64_t)slot * sub * sub;
+        o.goff = r.y;
+        o.ld = sub;
+        o.limit = (int64_t)sub * sub;
+        return true;
     }
+};
+
+template <class Src>
+__global__ void __launch_bounds__(TC_THREADS, 1) learned_grid_kernel(Src src, int64_t nvis, const float *__restrict__ P,
+                                                                      const bf16 *__restrict__ PB, int ksize,
+                                                                      float inv_wmax, float scale, int strip_lg,
+                                                                      unsigned *err)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TcSmem &S = *reinterpret_cast<TcSmem *>(smem_raw);
+    tc_prologue(S, P, PB);
+    const int g = threadIdx.x / IR, r = threadIdx.x % IR;
+    const float2 b4 = make_float2(P[OFF_B4], P[OFF_B4 + 1]);
+    const int taps = ksize * ksize;
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int64_t i = (int64_t)blockIdx.x * TC_GROUPS + g; i < nvis && ok; i += (int64_t)gridDim.x * TC_GROUPS) {
+        LearnedVis o;
+        if (!src.get(i, o)) continue;  // uniform across the group
+        // the previous visibility's last tile read the tables before its barriers
+        if (r < ksize) axis_table(o.du, r, ksize, S.ftab[g][0]);
+        else if (r >= 32 && r < 32 + ksize) axis_table(o.dv, r - 32, ksize, S.ftab[g][1]);
+        group_sync(g);
+        for (int t0 = 0; t0 < taps && ok; t0 += IR) {
+            const int t = t0 + r;
+            bf16 f[MFIN];
+            if (t < taps)
+                tap_features_tab(o.wf, o.du, o.dv, t % ksize, t / ksize, ksize, inv_wmax, S.ftab[g][0],
+                                 S.ftab[g][1], f);
+            else
+                for (int k = 0; k < MFIN; k++) f[k] = __float2bfloat16(0.f);
+            tc_store_features(S.F[g], r, f);
+            const float2 y = tc_tile(S, g, r, phase, b4, err, &ok);
+            const float kr = y.x * scale, ki = y.y * scale;
+            const int64_t idx = o.goff + (int64_t)(t / ksize) * o.ld + (t % ksize);
+            if (ok && t < taps && idx >= 0 && idx < o.limit)
+                atomicAdd(o.grid + (strip_lg ? (int64_t)strip_addr((int)idx, strip_lg) : idx),
+                          make_float2(o.vr * kr + o.vi * ki, o.vi * kr - o.vr * ki));
+        }
+    }
+    tc_epilogue(S);
 }
 
 // ---------------------------------------------------------------------------
@@ -623,39 +879,45 @@ void launch_mlp_to_bf16(cudaStream_t s, const float *P, void *PB)
     mlp_to_bf16_kernel<<<(MLP_NPARAM + 255) / 256, 256, 0, s>>>(P, (bf16 *)PB);
 }
 
-void launch_mlp_eval(cudaStream_t s, const float *P, const void *PB, const float *in, int n, int ksize,
-                     float inv_wmax, float scale, float2 *out, int sm_count)
+static int tc_blocks(int64_t groups_of_work, int sm_count)
 {
-    const size_t sm = sizeof(InferSmem);
+    int64_t b = (groups_of_work + TC_GROUPS - 1) / TC_GROUPS;
+    if (b > sm_count) b = sm_count;
+    return b < 1 ? 1 : (int)b;
+}
+
+void launch_mlp_eval(cudaStream_t s, const float *P, const void *PB, const float *in, int n, int ksize,
+                     float inv_wmax, float scale, float2 *out, int sm_count, unsigned *err)
+{
+    const size_t sm = sizeof(TcSmem);
     cudaFuncSetAttribute(mlp_eval_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    int blocks = (n + IR - 1) / IR;
-    if (blocks > sm_count * 4) blocks = sm_count * 4;
-    if (blocks < 1) blocks = 1;
-    mlp_eval_kernel<<<blocks, 256, sm, s>>>(P, (const bf16 *)PB, in, n, ksize, inv_wmax, scale, out);
+    mlp_eval_kernel<<<tc_blocks((n + IR - 1) / IR, sm_count), TC_THREADS, sm, s>>>(P, (const bf16 *)PB, in, n, ksize,
+                                                                                  inv_wmax, scale, out, err);
 }
 
 void launch_learned_towers(cudaStream_t s, const int4 *rec, const float2 *visf, const float4 *feat, int64_t n,
                            const int *slot_of_bin, int slot_cap, float2 *slots, int subgrid, const float *P,
-                           const void *PB, int ksize, float inv_wmax, float scale, int sm_count)
+                           const void *PB, int ksize, float inv_wmax, float scale, int sm_count, unsigned *err)
 {
-    const size_t sm = sizeof(InferSmem);
-    cudaFuncSetAttribute(learned_towers_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    int64_t blocks = n < (int64_t)sm_count * 4 ? n : (int64_t)sm_count * 4;
-    if (blocks < 1) blocks = 1;
-    learned_towers_kernel<<<(unsigned)blocks, 256, sm, s>>>(rec, visf, feat, n, slot_of_bin, slot_cap, slots, subgrid,
-                                                            P, (const bf16 *)PB, ksize, inv_wmax, scale);
+    const size_t sm = sizeof(TcSmem);
+    auto kern = learned_grid_kernel<TowersVisSource>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    TowersVisSource src{rec, visf, feat, slot_of_bin, slot_cap, subgrid, slots};
+    int strip_lg = 0;
+    while ((1 << strip_lg) < subgrid) strip_lg++;  // sub-grids are strip-major (strip_addr)
+    kern<<<tc_blocks(n, sm_count), TC_THREADS, sm, s>>>(src, n, P, (const bf16 *)PB, ksize, inv_wmax, scale,
+                                                        strip_lg, err);
 }
 
 void launch_learned_wproj(cudaStream_t s, const double *u, const double *v, const double *w,
                           const double2 *vis, int64_t n, int N, double theta, const float *P, const void *PB,
-                          int ksize, float inv_wmax, float scale, float2 *grid, int sm_count)
+                          int ksize, float inv_wmax, float scale, float2 *grid, int sm_count, unsigned *err)
 {
-    const size_t sm = sizeof(InferSmem);
-    cudaFuncSetAttribute(learned_wproj_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    int64_t blocks = n < (int64_t)sm_count * 4 ? n : (int64_t)sm_count * 4;
-    if (blocks < 1) blocks = 1;
-    learned_wproj_kernel<<<(unsigned)blocks, 256, sm, s>>>(u, v, w, vis, n, N, theta, P, (const bf16 *)PB,
-                                                           ksize, inv_wmax, scale, grid);
+    const size_t sm = sizeof(TcSmem);
+    auto kern = learned_grid_kernel<WprojVisSource>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    WprojVisSource src{u, v, w, vis, N, ksize, theta, grid};
+    kern<<<tc_blocks(n, sm_count), TC_THREADS, sm, s>>>(src, n, P, (const bf16 *)PB, ksize, inv_wmax, scale, 0, err);
 }
 
 }  // namespace rg

@@ -580,7 +580,7 @@ static rg_status wtowers_enqueue(rg_context *ctx, const DevVis &dv, const float2
         if (dv.n > 0)
             launch_learned_towers(st, (const int4 *)rec, (const float2 *)visf, (const float4 *)feat, dv.n,
                                   (const int *)slot_of_bin, pl.slots_cap, (float2 *)slots, S, lt->P, lt->PB,
-                                  lt->ksize, lt->inv_wmax, lt->scale, ctx->sm_count);
+                                  lt->ksize, lt->inv_wmax, lt->scale, ctx->sm_count, d.err);
         end_stage(ctx);
     } else {
         begin_stage(ctx, "romein");
@@ -633,6 +633,7 @@ static rg_status wtowers_check(rg_context *ctx, TowerPlan &pl, bool *overflow, c
     pl.seen_floors = rng[1];
     pl.seen_slots = cnt[0];
     pl.seen_groups = cnt[1];
+    if (err & DERR_TIMEOUT) return fail(RG_ERR_CUDA, "a bounded wait for tensor-core work timed out");
     *overflow = (err & DERR_CAPACITY) || !rng[2] || cnt[0] > pl.slots_cap || cnt[1] > pl.groups_cap;
     if (*overflow) {
         pl.zeroed_slots = 0;  // some sub-grids may not have been consumed (cleared)

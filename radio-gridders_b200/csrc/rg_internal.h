@@ -40,6 +40,7 @@ enum DeviceError : unsigned {
     DERR_PLANE_RANGE = 1u << 1,   // w outside the kernel table
     DERR_GRID_RANGE = 1u << 2,    // footprint leaves the grid (W-projection)
     DERR_CAPACITY = 1u << 3,      // internal capacity exceeded
+    DERR_TIMEOUT = 1u << 4,       // a bounded wait for tensor-core work gave up
 };
 
 // ---------------------------------------------------------------------------
@@ -268,15 +269,15 @@ void launch_mlp_grad(cudaStream_t s, const float *P, const void *PB, const float
 void launch_mlp_adam(cudaStream_t s, float *P, void *PB, float *grad, float *m, float *v, float lr, int step);
 void launch_mlp_to_bf16(cudaStream_t s, const float *P, void *PB);
 void launch_mlp_eval(cudaStream_t s, const float *P, const void *PB, const float *in, int n, int ksize,
-                     float inv_wmax, float scale, float2 *out, int sm_count);
+                     float inv_wmax, float scale, float2 *out, int sm_count, unsigned *err);
 void launch_learned_wproj(cudaStream_t s, const double *u, const double *v, const double *w,
                           const double2 *vis, int64_t n, int N, double theta, const float *P, const void *PB,
-                          int ksize, float inv_wmax, float scale, float2 *grid, int sm_count);
+                          int ksize, float inv_wmax, float scale, float2 *grid, int sm_count, unsigned *err);
 // W-towers with learned taps: per record, taps from the network at the
 // visibility's continuous (w - w_mid, du, dv) (feat), scattered into its slot's
 // sub-grid with the linear index rule of the table gridder.
 void launch_learned_towers(cudaStream_t s, const int4 *rec, const float2 *visf, const float4 *feat, int64_t n,
                            const int *slot_of_bin, int slot_cap, float2 *slots, int subgrid, const float *P,
-                           const void *PB, int ksize, float inv_wmax, float scale, int sm_count);
+                           const void *PB, int ksize, float inv_wmax, float scale, int sm_count, unsigned *err);
 
 }  // namespace rg

@@ -35,6 +35,26 @@ rg_status upload_params(rg_context *ctx, rg_mlp *mlp, const float *params)
     return RG_OK;
 }
 
+// Error word of the tensor-core kernels (DERR_TIMEOUT when a bounded wait
+// gave up), zeroed before the launch and read after the stream has drained.
+rg_status tc_err_begin(rg_context *ctx, unsigned **err)
+{
+    void *p;
+    RG_CHECK(scratch(ctx, "tc_err", 16, &p));
+    RG_CUDA(cudaMemsetAsync(p, 0, 16, ctx->stream));
+    *err = (unsigned *)p;
+    return RG_OK;
+}
+
+rg_status tc_err_end(rg_context *ctx, const unsigned *err)
+{
+    unsigned h = 0;
+    RG_CUDA(cudaMemcpyAsync(&h, err, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    RG_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (h & DERR_TIMEOUT) return fail(RG_ERR_CUDA, "a bounded wait for tensor-core work timed out");
+    return RG_OK;
+}
+
 rg_status check_mlp(rg_context *ctx, rg_mlp *mlp)
 {
     if (!ctx || !mlp) return fail(RG_ERR_INVALID_ARGUMENT, "ctx and mlp must be non-NULL");
@@ -198,10 +218,13 @@ rg_status rg_mlp_eval(rg_context *ctx, rg_mlp *mlp, const float *samples, int64_
     const bool dev_out = is_device_pointer(taps_out);
     if (dev_out) out = taps_out;
     else RG_CHECK(scratch(ctx, "mlp_eval_out", sizeof(float) * 2 * (size_t)n, &out));
+    unsigned *err;
+    RG_CHECK(tc_err_begin(ctx, &err));
     launch_mlp_eval(ctx->stream, mlp->P, mlp->PB, (const float *)in, (int)n, mlp->ksize, (float)(1.0 / mlp->wmax),
-                    (float)mlp->out_scale, (float2 *)out, ctx->sm_count);
+                    (float)mlp->out_scale, (float2 *)out, ctx->sm_count, err);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "mlp evaluation");
+    RG_CHECK(tc_err_end(ctx, err));
     if (!dev_out) RG_CUDA(cudaMemcpyAsync(taps_out, out, sizeof(float) * 2 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
     RG_CUDA(cudaStreamSynchronize(ctx->stream));
     return RG_OK;
@@ -231,14 +254,17 @@ rg_status rg_grid_wprojection_learned(rg_context *ctx, rg_mlp *mlp, double *uvgr
     void *grid32;
     RG_CHECK(scratch(ctx, "grid32", sizeof(float2) * (size_t)cells, &grid32));
     RG_CUDA(cudaMemsetAsync(grid32, 0, sizeof(float2) * (size_t)cells, ctx->stream));
+    unsigned *err;
+    RG_CHECK(tc_err_begin(ctx, &err));
     begin_stage(ctx, "learned_gridding");
     if (vis->n > 0)
         launch_learned_wproj(ctx->stream, (const double *)u, (const double *)v, (const double *)w,
                              (const double2 *)vz, vis->n, N, theta, mlp->P, mlp->PB, mlp->ksize,
-                             (float)(1.0 / mlp->wmax), (float)mlp->out_scale, (float2 *)grid32, ctx->sm_count);
+                             (float)(1.0 / mlp->wmax), (float)mlp->out_scale, (float2 *)grid32, ctx->sm_count, err);
     end_stage(ctx);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "learned gridding");
+    RG_CHECK(tc_err_end(ctx, err));
     const bool dev = is_device_pointer(uvgrid);
     void *g = uvgrid;
     if (!dev) {
