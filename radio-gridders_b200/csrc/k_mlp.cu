@@ -4,11 +4,11 @@
 // oversampled w-kernel tables, src/reference/grid.c:157-185): 21 input features
 // of a tap (w, sub-cell offsets du, dv, tap x, tap y and 16 Fourier features of
 // the tap's offset from the visibility) -> 128 -> 128 -> 128 (SiLU) -> 2
-// (complex tap / out_scale).  Layers 1-3 are BF16 x BF16 -> FP32 products:
-// in inference (evaluation and both gridders) tcgen05 MMAs with TMEM
-// accumulators, in training mma.sync.m16n8k16 tiles (the backward pass needs
-// the activations and gradients in registers and shared memory anyway); the
-// 128 -> 2 output layer and all element-wise work are FP32.
+// (complex tap / out_scale).  Layers 1-3 are tensor-core products with FP32
+// accumulation: in inference (evaluation and both gridders) FP16 tcgen05 MMAs
+// with TMEM accumulators, in training BF16 mma.sync.m16n8k16 tiles (the
+// backward pass needs the activations and gradients in registers and shared
+// memory anyway); the 128 -> 2 output layer is FP32.
 //
 // Parameters: one FP32 buffer, W1[32][128] (rows >= 21 unused), b1[128],
 // W2[128][128], b2, W3[128][128], b3, W4[128][2], b4[2] (W[in][out]); plus BF16
@@ -21,6 +21,7 @@
 // gradient buffer with atomics; mlp_adam_kernel applies Adam and refreshes the
 // BF16 copy.  Loss: mean over samples of |y - target / out_scale|^2.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include "rg_internal.h"
 
@@ -133,30 +134,37 @@ __device__ __forceinline__ float dsilu_f(float z)
     return s * (1.f + z * (1.f - s));
 }
 
+// A feature or activation as the tensor cores' element type: BF16 in
+// training, FP16 in inference.
+template <class T> __device__ __forceinline__ T to_elem(float x);
+template <> __device__ __forceinline__ bf16 to_elem<bf16>(float x) { return __float2bfloat16(x); }
+template <> __device__ __forceinline__ __half to_elem<__half>(float x) { return __float2half_rn(x); }
+
 // Features of one tap (the definition in oracle/mlp_oracle.py).
+template <class T>
 __device__ __forceinline__ void tap_features(float w, float du, float dv, float tx, float ty, int ksize,
-                                             float inv_wmax, bf16 *f)
+                                             float inv_wmax, T *f)
 {
     const float half = 0.5f * (float)ksize;
     const float p = tx - half - du, q = ty - half - dv;
     const float inv = 1.f / (half + 1.f);
-    f[0] = __float2bfloat16(w * inv_wmax);
-    f[1] = __float2bfloat16(2.f * du - 1.f);
-    f[2] = __float2bfloat16(2.f * dv - 1.f);
-    f[3] = __float2bfloat16(p / half);
-    f[4] = __float2bfloat16(q / half);
+    f[0] = to_elem<T>(w * inv_wmax);
+    f[1] = to_elem<T>(2.f * du - 1.f);
+    f[2] = to_elem<T>(2.f * dv - 1.f);
+    f[3] = to_elem<T>(p / half);
+    f[4] = to_elem<T>(q / half);
 #pragma unroll
     for (int k = 1; k <= 4; k++) {
         float s, c;
         sincospif((float)k * p * inv, &s, &c);
-        f[5 + 2 * (k - 1)] = __float2bfloat16(c);
-        f[6 + 2 * (k - 1)] = __float2bfloat16(s);
+        f[5 + 2 * (k - 1)] = to_elem<T>(c);
+        f[6 + 2 * (k - 1)] = to_elem<T>(s);
         sincospif((float)k * q * inv, &s, &c);
-        f[13 + 2 * (k - 1)] = __float2bfloat16(c);
-        f[14 + 2 * (k - 1)] = __float2bfloat16(s);
+        f[13 + 2 * (k - 1)] = to_elem<T>(c);
+        f[14 + 2 * (k - 1)] = to_elem<T>(s);
     }
 #pragma unroll
-    for (int k = MNFEAT; k < MFIN; k++) f[k] = __float2bfloat16(0.f);
+    for (int k = MNFEAT; k < MFIN; k++) f[k] = to_elem<T>(0.f);
 }
 
 // The same features from per-visibility tables: the Fourier terms depend on
@@ -176,23 +184,24 @@ __device__ __forceinline__ void axis_table(float d, int t, int ksize, float *tab
     }
 }
 
+template <class T>
 __device__ __forceinline__ void tap_features_tab(float w, float du, float dv, int tx, int ty, int ksize,
-                                                 float inv_wmax, const float *ptab, const float *qtab, bf16 *f)
+                                                 float inv_wmax, const float *ptab, const float *qtab, T *f)
 {
     const float half = 0.5f * (float)ksize;
     const float p = (float)tx - half - du, q = (float)ty - half - dv;
-    f[0] = __float2bfloat16(w * inv_wmax);
-    f[1] = __float2bfloat16(2.f * du - 1.f);
-    f[2] = __float2bfloat16(2.f * dv - 1.f);
-    f[3] = __float2bfloat16(p / half);
-    f[4] = __float2bfloat16(q / half);
+    f[0] = to_elem<T>(w * inv_wmax);
+    f[1] = to_elem<T>(2.f * du - 1.f);
+    f[2] = to_elem<T>(2.f * dv - 1.f);
+    f[3] = to_elem<T>(p / half);
+    f[4] = to_elem<T>(q / half);
 #pragma unroll
     for (int j = 0; j < 8; j++) {
-        f[5 + j] = __float2bfloat16(ptab[tx * 8 + j]);
-        f[13 + j] = __float2bfloat16(qtab[ty * 8 + j]);
+        f[5 + j] = to_elem<T>(ptab[tx * 8 + j]);
+        f[13 + j] = to_elem<T>(qtab[ty * 8 + j]);
     }
 #pragma unroll
-    for (int k = MNFEAT; k < MFIN; k++) f[k] = __float2bfloat16(0.f);
+    for (int k = MNFEAT; k < MFIN; k++) f[k] = to_elem<T>(0.f);
 }
 
 // Epilogue of a 32x32 (per warp) hidden-layer tile: z = acc + b; Z (fp32,
@@ -422,12 +431,21 @@ __global__ void mlp_to_bf16_kernel(const float *__restrict__ P, bf16 *__restrict
 
 // ---------------------------------------------------------------------------
 // Inference on the 5th-generation tensor cores (tcgen05).  Rows (taps) go in
-// tiles of 128; each hidden layer is an M = 128, N = 128 BF16 x BF16 -> FP32
+// tiles of 128; each hidden layer is an M = 128, N = 128 FP16 x FP16 -> FP32
 // product issued as K = 16 steps by one thread from shared-memory operands
 // into an accumulator in tensor memory (TMEM), and its epilogue (bias, SiLU,
-// BF16 pack back into shared memory as the next layer's A operand) is done by
+// FP16 pack back into shared memory as the next layer's A operand) is done by
 // the tile's 128 threads, each owning one TMEM lane (row).  The 128 -> 2
 // output layer runs in FP32 in the last epilogue.
+//
+// Inference computes in FP16 where training used BF16.  The weights are the
+// BF16-rounded ones the training forward pass used (converted exactly): the
+// network was fitted through those, and the unrounded FP32 master weights are
+// a slightly different function whose error is systematic across taps.
+// Features and activations are FP16 (11-bit instead of 8-bit mantissas), and
+// the SiLU runs on packed pairs — one f32 -> f16x2 conversion and one
+// tanh.approx.f16x2 per two activations, half the transcendental-unit work of
+// the BF16 form.
 //
 // A CTA (one per SM) holds one copy of W1..W3 (72 KB) and runs TC_GROUPS
 // independent tile groups of four warps, each with its own feature / hidden
@@ -450,7 +468,7 @@ __host__ __device__ constexpr int core_off(int row, int k, int K)
 }
 
 struct TcSmem {
-    alignas(16) unsigned char W1[MH * MFIN * 2];  // B operands: W^T [out][in], K-major
+    alignas(16) unsigned char W1[MH * MFIN * 2];  // B operands: W^T [out][in], K-major, FP16
     alignas(16) unsigned char W2[MH * MH * 2];
     alignas(16) unsigned char W3[MH * MH * 2];
     alignas(16) unsigned char F[TC_GROUPS][IR * MFIN * 2];  // A of layer 1 (features)
@@ -475,17 +493,16 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint3
 }
 
 // Instruction descriptor, kind::f16: FP32 accumulator (bits 4-5 = 1), A and B
-// BF16 (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
-constexpr uint32_t kIdescBf16 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(MH >> 3) << 17) |
-                                ((uint32_t)(IR >> 4) << 24);
+// FP16 (bits 7-9, 10-12 = 0), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+constexpr uint32_t kIdescF16 = (1u << 4) | ((uint32_t)(MH >> 3) << 17) | ((uint32_t)(IR >> 4) << 24);
 
-__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate)
+__device__ __forceinline__ void umma_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate)
 {
     asm volatile(
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
         :
-        : "r"(d_tmem), "l"(a), "l"(b), "r"(kIdescBf16), "r"(accumulate));
+        : "r"(d_tmem), "l"(a), "l"(b), "r"(kIdescF16), "r"(accumulate));
 }
 
 __device__ __forceinline__ void umma_commit(uint32_t bar)
@@ -536,31 +553,42 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32])
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// SiLU from the half pre-activation hz = z / 2: z sigmoid(z) = hz (1 + tanh hz),
-// with the hardware tanh approximation (one MUFU op; its ~2^-11 relative error
-// is below the BF16 rounding of the activation it feeds).
-__device__ __forceinline__ float silu_half(float hz)
+// SiLU of a pair from the half pre-activations hz = z / 2:
+// z sigmoid(z) = hz (1 + tanh hz), in FP16 with the hardware tanh
+// approximation (relative error ~2^-11, the FP16 rounding of its result).
+__device__ __forceinline__ uint32_t silu2_half(float hz0, float hz1)
 {
-    float t;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(hz));
-    return fmaf(hz, t, hz);
+    const __half2 h = __floats2half2_rn(hz0, hz1);
+    uint32_t hu = *reinterpret_cast<const uint32_t *>(&h), t;
+    asm("tanh.approx.f16x2 %0, %1;" : "=r"(t) : "r"(hu));
+    const __half2 r = __hfma2(h, *reinterpret_cast<const __half2 *>(&t), h);
+    return *reinterpret_cast<const uint32_t *>(&r);
+}
+
+// One 16-byte core-matrix row of W^T in FP16: W^T[n][k0 .. k0+7] of the BF16
+// copy (transposed, K columns), converted exactly.
+__device__ __forceinline__ void stage_wt(unsigned char *dst, const bf16 *__restrict__ WT, int n, int k0, int K)
+{
+    const uint4 in = *reinterpret_cast<const uint4 *>(WT + n * K + k0);
+    const uint32_t w[4] = {in.x, in.y, in.z, in.w};
+    uint32_t q[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const __half2 h = __floats2half2_rn(__uint_as_float(w[j] << 16), __uint_as_float(w[j] & 0xFFFF0000u));
+        q[j] = *reinterpret_cast<const uint32_t *>(&h);
+    }
+    *reinterpret_cast<uint4 *>(dst + core_off(n, k0, K)) = make_uint4(q[0], q[1], q[2], q[3]);
 }
 
 // CTA prologue: weights into the core-matrix layout, biases, mbarriers and
 // TMEM columns (warp 0 allocates TC_GROUPS * 128 columns).
 __device__ __forceinline__ void tc_prologue(TcSmem &S, const float *__restrict__ P, const bf16 *__restrict__ PB)
 {
-    for (int c = threadIdx.x; c < MH * (MFIN / 8); c += blockDim.x) {
-        const int row = c / (MFIN / 8), kc = c % (MFIN / 8);
-        *reinterpret_cast<uint4 *>(S.W1 + core_off(row, kc * 8, MFIN)) =
-            *reinterpret_cast<const uint4 *>(PB + BOFF_W1T + row * MFIN + kc * 8);
-    }
+    for (int c = threadIdx.x; c < MH * (MFIN / 8); c += blockDim.x)
+        stage_wt(S.W1, PB + BOFF_W1T, c / (MFIN / 8), (c % (MFIN / 8)) * 8, MFIN);
     for (int c = threadIdx.x; c < MH * (MH / 8); c += blockDim.x) {
-        const int row = c / (MH / 8), kc = c % (MH / 8);
-        *reinterpret_cast<uint4 *>(S.W2 + core_off(row, kc * 8, MH)) =
-            *reinterpret_cast<const uint4 *>(PB + BOFF_W2T + row * MH + kc * 8);
-        *reinterpret_cast<uint4 *>(S.W3 + core_off(row, kc * 8, MH)) =
-            *reinterpret_cast<const uint4 *>(PB + BOFF_W3T + row * MH + kc * 8);
+        stage_wt(S.W2, PB + BOFF_W2T, c / (MH / 8), (c % (MH / 8)) * 8, MH);
+        stage_wt(S.W3, PB + BOFF_W3T, c / (MH / 8), (c % (MH / 8)) * 8, MH);
     }
     for (int n = threadIdx.x; n < MH; n += blockDim.x) {
         S.hb[0][n] = 0.5f * P[OFF_B1 + n];
@@ -600,17 +628,11 @@ __device__ __forceinline__ void tc_epilogue(TcSmem &S)
 }
 
 // Row r of a tile: features into the group's A buffer (core layout, K = 32).
-__device__ __forceinline__ void tc_store_features(unsigned char *F, int r, const bf16 (&f)[MFIN])
+__device__ __forceinline__ void tc_store_features(unsigned char *F, int r, const __half (&f)[MFIN])
 {
 #pragma unroll
-    for (int j = 0; j < MFIN / 8; j++) {
-        uint4 q;
-        q.x = pack_bf16(f[8 * j + 0], f[8 * j + 1]);
-        q.y = pack_bf16(f[8 * j + 2], f[8 * j + 3]);
-        q.z = pack_bf16(f[8 * j + 4], f[8 * j + 5]);
-        q.w = pack_bf16(f[8 * j + 6], f[8 * j + 7]);
-        *reinterpret_cast<uint4 *>(F + core_off(r, 8 * j, MFIN)) = q;
-    }
+    for (int j = 0; j < MFIN / 8; j++)
+        *reinterpret_cast<uint4 *>(F + core_off(r, 8 * j, MFIN)) = *reinterpret_cast<const uint4 *>(f + 8 * j);
 }
 
 // Issue one hidden layer (K / 16 MMA steps) and commit it to the group's
@@ -621,11 +643,11 @@ __device__ __forceinline__ void tc_issue_layer(uint32_t d_tmem, const unsigned c
     tc_fence_after();
     const uint32_t a = smem_u32(A), b = smem_u32(B);
     for (int s = 0; s < K / 16; s++)
-        umma_bf16(d_tmem, umma_desc(a + s * 256, 128, K * 16), umma_desc(b + s * 256, 128, K * 16), s > 0);
+        umma_f16(d_tmem, umma_desc(a + s * 256, 128, K * 16), umma_desc(b + s * 256, 128, K * 16), s > 0);
     umma_commit(bar);
 }
 
-// Hidden epilogue of row r: TMEM accumulator -> SiLU(z + b) as BF16 into H.
+// Hidden epilogue of row r: TMEM accumulator -> SiLU(z + b) as FP16 into H.
 __device__ __forceinline__ void tc_hidden_epilogue(uint32_t taddr, const float *__restrict__ hb, unsigned char *H,
                                                    int r)
 {
@@ -636,11 +658,9 @@ __device__ __forceinline__ void tc_hidden_epilogue(uint32_t taddr, const float *
         tmem_wait_ld();
         uint32_t pk[16];
 #pragma unroll
-        for (int j = 0; j < 16; j++) {
-            const float h0 = silu_half(fmaf(__uint_as_float(v[2 * j]), 0.5f, hb[c * 32 + 2 * j]));
-            const float h1 = silu_half(fmaf(__uint_as_float(v[2 * j + 1]), 0.5f, hb[c * 32 + 2 * j + 1]));
-            pk[j] = pack_bf16(__float2bfloat16(h0), __float2bfloat16(h1));
-        }
+        for (int j = 0; j < 16; j++)
+            pk[j] = silu2_half(fmaf(__uint_as_float(v[2 * j]), 0.5f, hb[c * 32 + 2 * j]),
+                               fmaf(__uint_as_float(v[2 * j + 1]), 0.5f, hb[c * 32 + 2 * j + 1]));
 #pragma unroll
         for (int j = 0; j < 4; j++)
             *reinterpret_cast<uint4 *>(H + core_off(r, c * 32 + 8 * j, MH)) =
@@ -648,7 +668,7 @@ __device__ __forceinline__ void tc_hidden_epilogue(uint32_t taddr, const float *
     }
 }
 
-// Output epilogue of row r: SiLU(z + b3) rounded to BF16, times W4, plus b4.
+// Output epilogue of row r: SiLU(z + b3) (FP16 pairs), times W4, plus b4.
 __device__ __forceinline__ float2 tc_output_epilogue(uint32_t taddr, const float *__restrict__ hb,
                                                      const float2 *__restrict__ w4, float2 b4)
 {
@@ -659,12 +679,13 @@ __device__ __forceinline__ float2 tc_output_epilogue(uint32_t taddr, const float
         tmem_ld32(taddr + c * 32, v);
         tmem_wait_ld();
 #pragma unroll
-        for (int j = 0; j < 32; j++) {
-            const float h = __bfloat162float(
-                __float2bfloat16(silu_half(fmaf(__uint_as_float(v[j]), 0.5f, hb[c * 32 + j]))));
-            const float2 wv = w4[c * 32 + j];
-            y0 = fmaf(h, wv.x, y0);
-            y1 = fmaf(h, wv.y, y1);
+        for (int j = 0; j < 16; j++) {
+            const uint32_t hp = silu2_half(fmaf(__uint_as_float(v[2 * j]), 0.5f, hb[c * 32 + 2 * j]),
+                                           fmaf(__uint_as_float(v[2 * j + 1]), 0.5f, hb[c * 32 + 2 * j + 1]));
+            const float2 h = __half22float2(*reinterpret_cast<const __half2 *>(&hp));
+            const float2 wa = w4[c * 32 + 2 * j], wb = w4[c * 32 + 2 * j + 1];
+            y0 = fmaf(h.x, wa.x, fmaf(h.y, wb.x, y0));
+            y1 = fmaf(h.x, wa.y, fmaf(h.y, wb.y, y1));
         }
     }
     return make_float2(y0, y1);
@@ -732,10 +753,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mlp_eval_kernel(const float *__
     bool ok = true;
     for (int base = (blockIdx.x * TC_GROUPS + g) * IR; base < n && ok; base += gridDim.x * TC_GROUPS * IR) {
         const int i = base + r;
-        bf16 f[MFIN];
+        __align__(16) __half f[MFIN];
         if (i < n) tap_features(in[i], in[n + i], in[2 * n + i], in[3 * n + i], in[4 * n + i], ksize, inv_wmax, f);
         else
-            for (int k = 0; k < MFIN; k++) f[k] = __float2bfloat16(0.f);
+            for (int k = 0; k < MFIN; k++) f[k] = __float2half_rn(0.f);
         tc_store_features(S.F[g], r, f);
         const float2 y = tc_tile(S, g, r, phase, b4, err, &ok);
         if (ok && i < n) out[i] = make_float2(y.x * scale, y.y * scale);
@@ -837,12 +858,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) learned_grid_kernel(Src src, in
         group_sync(g);
         for (int t0 = 0; t0 < taps && ok; t0 += IR) {
             const int t = t0 + r;
-            bf16 f[MFIN];
+            __align__(16) __half f[MFIN];
             if (t < taps)
                 tap_features_tab(o.wf, o.du, o.dv, t % ksize, t / ksize, ksize, inv_wmax, S.ftab[g][0],
                                  S.ftab[g][1], f);
             else
-                for (int k = 0; k < MFIN; k++) f[k] = __float2bfloat16(0.f);
+                for (int k = 0; k < MFIN; k++) f[k] = __float2half_rn(0.f);
             tc_store_features(S.F[g], r, f);
             const float2 y = tc_tile(S, g, r, phase, b4, err, &ok);
             const float kr = y.x * scale, ki = y.y * scale;

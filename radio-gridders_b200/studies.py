@@ -255,17 +255,27 @@ def baselines(ctx):
 
 def learned_small(ctx, stations=64, steps=2000):
     """A short learned W-towers run (a briefly trained network, 2048^2, S 512,
-    margin 16, winc 10, `stations` stations) for profiling the learned
-    gridding kernel; prints its time and the visibility count."""
+    margin 16, winc 10, `stations` stations, inputs and grid in HBM) for
+    profiling the learned gridding kernel: the whole call and its gridding
+    stage (CUDA events of the library's stage timers)."""
+    import torch
     obs = _sim.wtowers_plain(n_st=stations)
     u, v, w, vis = obs.flat()
     mlp, _ = _learned.train(ctx, wmax=6.0, theta=0.1, ksize=16, n_triples=512, steps=steps, batch=16384,
                             lr_max=4e-3)
-    g = np.zeros((2048, 2048), np.complex128)
-    V = _rg.Visibilities(u, v, w, vis)
-    ms = _events_ms(lambda: _rg.grid_wtowers_learned(ctx, mlp, g, 2048, 0.1, V, 512, 16, 10.0, flags=1),
-                    repeats=2)
-    return {"n_vis": len(u), "learned_ms": ms, "learned_vis_per_s": len(u) / (ms * 1e-3)}
+    dev = torch.device("cuda", 0)
+    ctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+    V = _rg.Visibilities(*(torch.from_numpy(a).to(dev) for a in (u, v, w)), torch.from_numpy(vis).to(dev))
+    g = torch.zeros((2048, 2048), dtype=torch.complex128, device=dev)
+    call = lambda: _rg.grid_wtowers_learned(ctx, mlp, g, 2048, 0.1, V, 512, 16, 10.0, flags=1)
+    ms = _events_ms(call, repeats=3)
+    ctx.set_profiling(True)
+    call()
+    stage = dict(ctx.last_timings())["learned_gridding"]
+    ctx.set_profiling(False)
+    ctx.set_stream(None)
+    return {"n_vis": len(u), "learned_ms": ms, "learned_vis_per_s": len(u) / (ms * 1e-3),
+            "gridding_stage_ms": stage, "gridding_stage_vis_per_s": len(u) / (stage * 1e-3)}
 
 
 def main(which):
