@@ -458,7 +458,7 @@ __global__ void mlp_to_bf16_kernel(const float *__restrict__ P, bf16 *__restrict
 // (stride byte offset).
 // ---------------------------------------------------------------------------
 constexpr int IR = 128;  // rows per tile
-constexpr int TC_GROUPS = 2;
+constexpr int TC_GROUPS = 4;
 constexpr int TC_THREADS = TC_GROUPS * IR;
 constexpr int TC_KMAX = 16;  // largest kernel support (feature tables)
 
@@ -471,8 +471,11 @@ struct TcSmem {
     alignas(16) unsigned char W1[MH * MFIN * 2];  // B operands: W^T [out][in], K-major, FP16
     alignas(16) unsigned char W2[MH * MH * 2];
     alignas(16) unsigned char W3[MH * MH * 2];
-    alignas(16) unsigned char F[TC_GROUPS][IR * MFIN * 2];  // A of layer 1 (features)
-    alignas(16) unsigned char H[TC_GROUPS][IR * MH * 2];    // A of layers 2, 3 (activations)
+    // A of layers 2, 3 (activations); its first IR * MFIN * 2 bytes are also
+    // layer 1's A (features): layer 1's MMA has completed before its epilogue
+    // writes activations, and the next tile's features are stored after the
+    // layer-3 MMA (the last reader of the activations) has completed.
+    alignas(16) unsigned char H[TC_GROUPS][IR * MH * 2];
     float hb[3][MH];                                         // b1..b3 / 2
     float2 w4[MH];
     float ftab[TC_GROUPS][2][TC_KMAX * 8];  // per-visibility Fourier terms
@@ -551,7 +554,40 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32])
           "=r"(v[30]), "=r"(v[31])
         : "r"(taddr));
 }
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// Wait for this thread's TMEM loads; v is tied to the wait so that no use of
+// the loaded registers is scheduled before it.
+__device__ __forceinline__ void tmem_wait_ld(uint32_t (&v)[32])
+{
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]),
+                   "+r"(v[7]), "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]),
+                   "+r"(v[14]), "+r"(v[15]), "+r"(v[16]), "+r"(v[17]), "+r"(v[18]), "+r"(v[19]), "+r"(v[20]),
+                   "+r"(v[21]), "+r"(v[22]), "+r"(v[23]), "+r"(v[24]), "+r"(v[25]), "+r"(v[26]), "+r"(v[27]),
+                   "+r"(v[28]), "+r"(v[29]), "+r"(v[30]), "+r"(v[31])
+                 :
+                 : "memory");
+}
+
+// The MH accumulator columns of this thread's TMEM lane in chunks of 32:
+// fn(c, v) for chunk c, with chunk c + 1 loading while chunk c is processed.
+template <class Fn>
+__device__ __forceinline__ void tmem_row_chunks(uint32_t taddr, Fn &&fn)
+{
+    static_assert(MH == 128, "four chunks of 32 columns");
+    uint32_t a[32], b[32];
+    tmem_ld32(taddr, a);
+    tmem_wait_ld(a);
+    tmem_ld32(taddr + 32, b);
+    fn(0, a);
+    tmem_wait_ld(b);
+    tmem_ld32(taddr + 64, a);
+    fn(1, b);
+    tmem_wait_ld(a);
+    tmem_ld32(taddr + 96, b);
+    fn(2, a);
+    tmem_wait_ld(b);
+    fn(3, b);
+}
 
 // SiLU of a pair from the half pre-activations hz = z / 2:
 // z sigmoid(z) = hz (1 + tanh hz), in FP16 with the hardware tanh
@@ -651,11 +687,7 @@ __device__ __forceinline__ void tc_issue_layer(uint32_t d_tmem, const unsigned c
 __device__ __forceinline__ void tc_hidden_epilogue(uint32_t taddr, const float *__restrict__ hb, unsigned char *H,
                                                    int r)
 {
-#pragma unroll 1
-    for (int c = 0; c < MH / 32; c++) {
-        uint32_t v[32];
-        tmem_ld32(taddr + c * 32, v);
-        tmem_wait_ld();
+    tmem_row_chunks(taddr, [&](int c, const uint32_t(&v)[32]) {
         uint32_t pk[16];
 #pragma unroll
         for (int j = 0; j < 16; j++)
@@ -665,7 +697,7 @@ __device__ __forceinline__ void tc_hidden_epilogue(uint32_t taddr, const float *
         for (int j = 0; j < 4; j++)
             *reinterpret_cast<uint4 *>(H + core_off(r, c * 32 + 8 * j, MH)) =
                 make_uint4(pk[4 * j], pk[4 * j + 1], pk[4 * j + 2], pk[4 * j + 3]);
-    }
+    });
 }
 
 // Output epilogue of row r: SiLU(z + b3) (FP16 pairs), times W4, plus b4.
@@ -673,11 +705,7 @@ __device__ __forceinline__ float2 tc_output_epilogue(uint32_t taddr, const float
                                                      const float2 *__restrict__ w4, float2 b4)
 {
     float y0 = b4.x, y1 = b4.y;
-#pragma unroll 1
-    for (int c = 0; c < MH / 32; c++) {
-        uint32_t v[32];
-        tmem_ld32(taddr + c * 32, v);
-        tmem_wait_ld();
+    tmem_row_chunks(taddr, [&](int c, const uint32_t(&v)[32]) {
 #pragma unroll
         for (int j = 0; j < 16; j++) {
             const uint32_t hp = silu2_half(fmaf(__uint_as_float(v[2 * j]), 0.5f, hb[c * 32 + 2 * j]),
@@ -687,11 +715,11 @@ __device__ __forceinline__ float2 tc_output_epilogue(uint32_t taddr, const float
             y0 = fmaf(h.x, wa.x, fmaf(h.y, wb.x, y0));
             y1 = fmaf(h.x, wa.y, fmaf(h.y, wb.y, y1));
         }
-    }
+    });
     return make_float2(y0, y1);
 }
 
-// The network on the 128 feature rows the group has just stored in S.F[g]:
+// The network on the 128 feature rows the group has just stored in S.H[g]:
 // returns row r's output (tap / out_scale).  All threads of group g.  On a
 // wait that timed out the error word gets DERR_TIMEOUT and *ok turns false
 // for the whole group (read after a group barrier).
@@ -712,7 +740,7 @@ __device__ __forceinline__ float2 tc_tile(TcSmem &S, int g, int r, uint32_t &pha
 #pragma unroll 1
     for (int layer = 0; layer < 3; layer++) {
         if (r == 0) {
-            if (layer == 0) tc_issue_layer(d_tmem, S.F[g], S.W1, MFIN, bar);
+            if (layer == 0) tc_issue_layer(d_tmem, S.H[g], S.W1, MFIN, bar);
             else tc_issue_layer(d_tmem, S.H[g], layer == 1 ? S.W2 : S.W3, MH, bar);
         }
         if (!mbar_wait(bar, phase)) {
@@ -757,7 +785,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mlp_eval_kernel(const float *__
         if (i < n) tap_features(in[i], in[n + i], in[2 * n + i], in[3 * n + i], in[4 * n + i], ksize, inv_wmax, f);
         else
             for (int k = 0; k < MFIN; k++) f[k] = __float2half_rn(0.f);
-        tc_store_features(S.F[g], r, f);
+        tc_store_features(S.H[g], r, f);
         const float2 y = tc_tile(S, g, r, phase, b4, err, &ok);
         if (ok && i < n) out[i] = make_float2(y.x * scale, y.y * scale);
     }
@@ -864,7 +892,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) learned_grid_kernel(Src src, in
                                  S.ftab[g][1], f);
             else
                 for (int k = 0; k < MFIN; k++) f[k] = __float2half_rn(0.f);
-            tc_store_features(S.F[g], r, f);
+            tc_store_features(S.H[g], r, f);
             const float2 y = tc_tile(S, g, r, phase, b4, err, &ok);
             const float kr = y.x * scale, ki = y.y * scale;
             const int64_t idx = o.goff + (int64_t)(t / ksize) * o.ld + (t % ksize);
