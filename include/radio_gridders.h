@@ -265,10 +265,13 @@ rg_status rg_hdf5_attr_f64(const char *path, const char *object, const char *nam
  * and tap (tx, ty), in place of the quantised oversampled table.  No
  * counterpart in the reference (whose kernels come from crocodile table files,
  * src/common/hdf5.c:1362-1509).  Network: 21 features -> 128 -> 128 -> 128
- * (SiLU) -> complex tap / out_scale; BF16 tensor-core layers with FP32
- * accumulation; trained by the library's own forward/backward kernels with
- * Adam.  Samples are [5][n] float arrays (w, du, dv, tx, ty), taps complex
- * float interleaved.  A network belongs to the context's device. */
+ * (SiLU) -> complex tap / out_scale; tensor-core layers with FP32
+ * accumulation (FP16 tcgen05 MMAs with TMEM accumulators in evaluation and
+ * gridding, BF16 in training); trained by the library's own forward/backward
+ * kernels with Adam.  Samples are [5][n] float arrays (w, du, dv, tx, ty),
+ * taps complex float interleaved.  A network belongs to the context's device.
+ * The tensor-core waits are bounded: a wait that runs out returns RG_ERR_CUDA
+ * ("timed out") with the context still usable. */
 typedef struct rg_mlp rg_mlp;
 int rg_mlp_param_count(void);
 rg_status rg_mlp_create(rg_context *ctx, int ksize, double wmax, double out_scale, uint64_t seed,
@@ -298,6 +301,11 @@ rg_status rg_grid_wprojection_learned(rg_context *ctx, rg_mlp *mlp, double *uvgr
 rg_status rg_grid_wtowers_learned(rg_context *ctx, rg_mlp *mlp, double *uvgrid, int grid_size, double theta,
                                   const rg_vis *vis, int subgrid_size, int subgrid_margin, double wincrement,
                                   int flags);
+
+/* Self-test of the bounded tensor-core wait: one CTA waits ~2 ms on an
+ * mbarrier that nothing arrives on.  Returns RG_ERR_CUDA with a "timed out"
+ * message when the timeout path works (RG_OK would mean it does not). */
+rg_status rg_selftest_wait_timeout(rg_context *ctx);
 
 #ifdef __cplusplus
 }

@@ -44,7 +44,7 @@ EXPORTS = [
     "rg_mlp_set_params", "rg_mlp_get_params", "rg_mlp_gradient", "rg_mlp_train", "rg_mlp_eval",
     "rg_grid_wprojection_learned", "rg_grid_wtowers_learned", "rg_grid_wtowers_batch", "rg_read_vis_hdf5", "rg_free_vis_data", "rg_read_wkern_hdf5",
     "rg_free_wkern_data", "rg_write_vis_hdf5", "rg_write_vis_flat_hdf5", "rg_write_wkern_hdf5", "rg_hdf5_read_f64",
-    "rg_hdf5_attr_f64",
+    "rg_hdf5_attr_f64", "rg_selftest_wait_timeout",
 ]
 
 
@@ -134,6 +134,7 @@ def lib():
         L.rg_write_vis_flat_hdf5.argtypes = [ct.c_char_p, i, i, vp, vp, vp, vp, vp, vp]
         L.rg_hdf5_read_f64.argtypes = [ct.c_char_p, ct.c_char_p, vp, i64, ct.POINTER(i64), ct.POINTER(i)]
         L.rg_hdf5_attr_f64.argtypes = [ct.c_char_p, ct.c_char_p, ct.c_char_p, ct.POINTER(d)]
+        L.rg_selftest_wait_timeout.argtypes = [vp]
         for name in EXPORTS:
             getattr(L, name)  # raises AttributeError if a declared symbol is missing
         _lib = L
@@ -225,6 +226,12 @@ class Context:
 
     def set_profiling(self, enabled=True):
         _check(lib().rg_context_set_profiling(self._h, 1 if enabled else 0))
+
+    def selftest_wait_timeout(self):
+        """Run the bounded tensor-core wait against an mbarrier nothing arrives
+        on (rg_selftest_wait_timeout); raises RGError when the timeout path
+        reports, as it should."""
+        _check(lib().rg_selftest_wait_timeout(self._h))
 
     def last_timings(self):
         """[(stage, ms)] of the last call when profiling is enabled."""

@@ -523,8 +523,9 @@ __device__ __forceinline__ void group_sync(int g)
 }
 
 // Bounded wait for the completion of the mbarrier phase with this parity
-// (about two seconds of SM clock); false when it did not complete.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+// (by default 2^32 SM clocks, about two seconds); false when it did not
+// complete.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit = 1ll << 32)
 {
     const long long t0 = clock64();
     for (;;) {
@@ -536,7 +537,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
             : "r"(bar), "r"(parity)
             : "memory");
         if (done) return true;
-        if (clock64() - t0 > (1ll << 32)) return false;
+        if (clock64() - t0 > limit) return false;
     }
 }
 
@@ -904,6 +905,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) learned_grid_kernel(Src src, in
     tc_epilogue(S);
 }
 
+// Self-test of the bounded wait: one CTA waits on an mbarrier that nothing
+// arrives on, for `limit` SM clocks, and reports DERR_TIMEOUT like the
+// inference kernels do.
+__global__ void mbar_timeout_probe_kernel(unsigned *err, long long limit)
+{
+    __shared__ unsigned long long bar;
+    if (threadIdx.x == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar)) : "memory");
+    __syncthreads();
+    if (!mbar_wait(smem_u32(&bar), 0, limit)) atomicOr(err, DERR_TIMEOUT);
+}
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
@@ -926,6 +938,11 @@ void launch_mlp_adam(cudaStream_t s, float *P, void *PB, float *grad, float *m, 
 void launch_mlp_to_bf16(cudaStream_t s, const float *P, void *PB)
 {
     mlp_to_bf16_kernel<<<(MLP_NPARAM + 255) / 256, 256, 0, s>>>(P, (bf16 *)PB);
+}
+
+void launch_mbar_timeout_probe(cudaStream_t s, unsigned *err, long long limit)
+{
+    mbar_timeout_probe_kernel<<<1, 64, 0, s>>>(err, limit);
 }
 
 static int tc_blocks(int64_t groups_of_work, int sm_count)

@@ -270,6 +270,7 @@ void launch_mlp_adam(cudaStream_t s, float *P, void *PB, float *grad, float *m, 
 void launch_mlp_to_bf16(cudaStream_t s, const float *P, void *PB);
 void launch_mlp_eval(cudaStream_t s, const float *P, const void *PB, const float *in, int n, int ksize,
                      float inv_wmax, float scale, float2 *out, int sm_count, unsigned *err);
+void launch_mbar_timeout_probe(cudaStream_t s, unsigned *err, long long limit);
 void launch_learned_wproj(cudaStream_t s, const double *u, const double *v, const double *w,
                           const double2 *vis, int64_t n, int N, double theta, const float *P, const void *PB,
                           int ksize, float inv_wmax, float scale, float2 *grid, int sm_count, unsigned *err);

@@ -230,6 +230,18 @@ rg_status rg_mlp_eval(rg_context *ctx, rg_mlp *mlp, const float *samples, int64_
     return RG_OK;
 }
 
+rg_status rg_selftest_wait_timeout(rg_context *ctx)
+{
+    if (!ctx) return fail(RG_ERR_INVALID_ARGUMENT, "ctx must be non-NULL");
+    RG_CUDA(cudaSetDevice(ctx->device));
+    unsigned *err;
+    RG_CHECK(tc_err_begin(ctx, &err));
+    launch_mbar_timeout_probe(ctx->stream, err, 1ll << 22);  // ~2 ms of SM clock
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "wait self-test");
+    return tc_err_end(ctx, err);
+}
+
 rg_status rg_grid_wprojection_learned(rg_context *ctx, rg_mlp *mlp, double *uvgrid, int grid_size, double theta,
                                       const rg_vis *vis, int flags)
 {

@@ -130,3 +130,16 @@ def test_learned_wtowers_equals_table_wtowers_on_the_lattice(rg, ctx, MO):
     assert np.linalg.norm(g_learned - g_table) / np.linalg.norm(g_table) < 1e-5
     with pytest.raises(rg.RGError):  # network w range narrower than winc / 2
         rg.grid_wtowers_learned(ctx, mlp, g_learned, n, th, V, S, M, 10.0)
+
+
+def test_bounded_wait_times_out_and_context_survives(rg, ctx):
+    """The tensor-core kernels' waits are bounded: a wait on an mbarrier that
+    nothing arrives on gives up, the error reaches the host as RG_ERR_CUDA
+    ("timed out"), and the context keeps working afterwards."""
+    with pytest.raises(rg.RGError) as e:
+        ctx.selftest_wait_timeout()
+    assert e.value.status == 2 and "timed out" in str(e.value)
+    mlp = rg.LearnedKernel(ctx, 16, 10.0, 0.05)
+    taps = mlp.eval(rg.LearnedKernel.samples(np.zeros(4), np.full(4, 0.5), np.full(4, 0.5), np.arange(4.0),
+                                            np.arange(4.0)))
+    assert np.all(np.isfinite(taps))
