@@ -974,8 +974,11 @@ rg_status grid_wtowers_batch_impl(rg_context *ctx, int count, double *const *uvg
         const rg_vis &v = vis[i];
         const void *src[4] = {v.u, v.v, v.w, v.vis};
         const void *dev[4];
-        if (used[b]) RG_CUDA(cudaStreamWaitEvent(ctx->copy_in, ctx->ev_used[b], 0));  // step i-2 done with set b
-        if (out_pending[b]) RG_CUDA(cudaStreamWaitEvent(ctx->copy_in, ctx->ev_out[b], 0));  // its grid copied out
+        // Input staging set b was last read by step i-2's pass.  Its output
+        // staging buffer is only rewritten by this step's pass, so the wait for
+        // step i-2's grid copy-out goes on the pass, not on these copies: the
+        // uploads of step i overlap the download of step i-2.
+        if (used[b]) RG_CUDA(cudaStreamWaitEvent(ctx->copy_in, ctx->ev_used[b], 0));
         for (int f = 0; f < 4; f++) {
             if (n == 0 || is_device_pointer(src[f])) {
                 dev[f] = src[f];
@@ -993,10 +996,15 @@ rg_status grid_wtowers_batch_impl(rg_context *ctx, int count, double *const *uvg
         dv.n = n;
         const bool host_out = !is_device_pointer(uvgrids[i]);
         double *out_dev = host_out ? (double *)outb[b] : uvgrids[i];
-        if (host_out && !(flags & RG_GRID_OVERWRITE))
+        if (host_out && !(flags & RG_GRID_OVERWRITE)) {
+            // accumulating into a host grid: its upload rewrites the output staging buffer
+            if (out_pending[b]) RG_CUDA(cudaStreamWaitEvent(ctx->copy_in, ctx->ev_out[b], 0));
             RG_CUDA(cudaMemcpyAsync(out_dev, uvgrids[i], grid_bytes, cudaMemcpyHostToDevice, ctx->copy_in));
+        }
         RG_CUDA(cudaEventRecord(ctx->ev_in[b], ctx->copy_in));
         RG_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev_in[b], 0));
+        if (host_out && out_pending[b])  // step i-2's grid has left the output staging buffer
+            RG_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev_out[b], 0));
         RG_CHECK(wtowers_enqueue(ctx, dv, (const float2 *)taps, wkern, nullptr, out_dev, N, theta, S, M, winc, flags,
                                  pl, (char *)ctx->pinned_steps + (size_t)i * 64, (int *)poison));
         RG_CUDA(cudaEventRecord(ctx->ev_used[b], ctx->stream));
