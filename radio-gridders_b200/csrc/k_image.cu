@@ -39,9 +39,32 @@ __global__ void convert_table_dup_kernel(const double2 *__restrict__ src, float2
     }
 }
 
+// The same for a power-of-two slice length (every supported kernel size): one
+// thread per two source taps (two 16-byte loads), each converted pair stored
+// twice as one 16-byte store; shifts instead of 64-bit divisions.
+__global__ void convert_table_dup_pow2_kernel(const double2 *__restrict__ src, float4 *__restrict__ dst,
+                                              int64_t n_pairs, int kk_lg)
+{
+    const int64_t half = (int64_t)1 << (kk_lg - 1);  // pairs per slice
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_pairs;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 a = src[2 * i], b = src[2 * i + 1];
+        const float4 f = make_float4((float)a.x, (float)a.y, (float)b.x, (float)b.y);
+        const int64_t slice = i >> (kk_lg - 1), t = i & (half - 1);
+        float4 *d = dst + (slice << kk_lg) + t;
+        d[0] = f;
+        d[half] = f;
+    }
+}
+
 void launch_convert_table_dup(cudaStream_t s, const double2 *src, float2 *dst, int64_t n, int kk)
 {
-    convert_table_dup_kernel<<<blocks_for(2 * n), 256, 0, s>>>(src, dst, 2 * n, kk);
+    int lg = 0;
+    while ((1 << lg) < kk) lg++;
+    if ((1 << lg) == kk && lg >= 1)
+        convert_table_dup_pow2_kernel<<<blocks_for(n / 2), 256, 0, s>>>(src, (float4 *)dst, n / 2, lg);
+    else
+        convert_table_dup_kernel<<<blocks_for(2 * n), 256, 0, s>>>(src, dst, 2 * n, kk);
 }
 
 // make_hermitian, src/reference/grid.c:639-662: the pointer walk pairs linear
