@@ -327,8 +327,9 @@ __global__ void __launch_bounds__(kSparseColThreads) sparse_cols_kernel(
 // ph(l, m)) with ph = winc (1 - sqrt(1 - l^2 - m^2)) — the reference's
 // wtransfer^(-wp), grid.c:304-319 and :473-496, which also covers the w = 0
 // transfer — accumulated in registers; the strip sum goes to the group's
-// partial buffer.  Phase products are formed and reduced modulo 1 in FP64;
-// sin/cos of the reduced phase in FP32.
+// partial buffer.  The phase -wp * ph is formed modulo one turn as an integer
+// product with the 32-bit fixed-point table (fresnel_table_kernel); sin/cos of
+// its top 24 bits in FP32.
 //
 // tower_rows_finish_kernel: CTA = (tower, strip of R rows).  Sums the tower's
 // group partials in group order (deterministic) and applies the forward row
@@ -401,7 +402,7 @@ template <int N1>
 __global__ void __launch_bounds__(kRowThreads) tower_rows_kernel(
     float2 *__restrict__ slots, const unsigned *__restrict__ masks, const int *__restrict__ bin_of_slot,
     const int *__restrict__ group_begin, const int *__restrict__ group_end, const int *__restrict__ range,
-    const int *__restrict__ counts, int slot_cap, const double *__restrict__ ph, float2 *__restrict__ partial,
+    const int *__restrict__ counts, int slot_cap, const uint32_t *__restrict__ phq, float2 *__restrict__ partial,
     const float2 *__restrict__ tw)
 {
     using G = RowGeom<N1>;
@@ -409,7 +410,7 @@ __global__ void __launch_bounds__(kRowThreads) tower_rows_kernel(
     extern __shared__ float2 smem[];
     float2 *T = smem;                                // [R][N1][kPad]
     float2 *W = smem + G::T_ELEMS;                   // [N]
-    double *P = reinterpret_cast<double *>(W + N);   // [R][N] Fresnel phase of the strip
+    uint32_t *P = reinterpret_cast<uint32_t *>(W + N);  // [R][N] Fresnel phase of the strip (turns, 2^-32)
     __shared__ unsigned smask[G::WORDS];
     const int rstrips = N / R;
     const int group = blockIdx.x / rstrips, row0 = (blockIdx.x % rstrips) * R;
@@ -418,7 +419,7 @@ __global__ void __launch_bounds__(kRowThreads) tower_rows_kernel(
     const int begin = group_begin[group];
     const int end = group_end[group] < slot_cap ? group_end[group] : slot_cap;
     load_twiddles<N1>(W, tw);
-    for (int e = threadIdx.x; e < R * N; e += blockDim.x) P[e] = ph[(int64_t)row0 * N + e];
+    for (int e = threadIdx.x; e < R * N; e += blockDim.x) P[e] = phq[(int64_t)row0 * N + e];
 
     float2 acc[G::PER][N1];
 #pragma unroll
@@ -427,7 +428,7 @@ __global__ void __launch_bounds__(kRowThreads) tower_rows_kernel(
         for (int j = 0; j < N1; j++) acc[q][j] = make_float2(0.f, 0.f);
 
     for (int slot = begin; slot < end; slot++) {
-        const double mwp = -(double)(wp_min + bin_of_slot[slot] % nfloor);
+        const uint32_t mwp = (uint32_t)(-(wp_min + bin_of_slot[slot] % nfloor));  // two's complement
         if (threadIdx.x < G::WORDS) smask[threadIdx.x] = masks[(int64_t)slot * G::WORDS + threadIdx.x];
         __syncthreads();  // masks visible; the previous floor's step 2 is done with T
         // the slot's strip mask in two 64-bit registers (at most 128 strips)
@@ -480,11 +481,16 @@ __global__ void __launch_bounds__(kRowThreads) tower_rows_kernel(
 #pragma unroll
                 for (int j = 0; j < N1; j++) {
                     const int col = k2 + 32 * bitrevc(j, G::LB);
-                    double phase = mwp * P[r * N + col];
-                    phase -= rint(phase);  // |phase| <= 1/2 after the FP64 reduction
+                    // -wp ph modulo one turn as a signed 32-bit fraction, rounded to
+                    // its top 24 bits (k, |k| <= 2^22), converted exactly by the
+                    // 1.5 * 2^23 magic number
+                    const int k = (int)(mwp * P[r * N + col] + 256u) >> 9;
+                    const float turns = __int_as_float(0x4B400000 + k) - 12582912.f;
                     float sn, cs;
-                    __sincosf(6.28318530717958647f * (float)phase, &sn, &cs);
-                    acc[q][j] = caddf(acc[q][j], cmulf(b[j], make_float2(cs, sn)));
+                    __sincosf(turns * (6.28318530717958647f / 8388608.f), &sn, &cs);
+                    // acc += b * (cs + i sn), two fused multiply-adds per component
+                    acc[q][j].x = fmaf(b[j].x, cs, fmaf(-b[j].y, sn, acc[q][j].x));
+                    acc[q][j].y = fmaf(b[j].x, sn, fmaf(b[j].y, cs, acc[q][j].y));
                 }
             }
         }
@@ -562,7 +568,7 @@ static size_t sparse_cols_smem() { return sizeof(float2) * (StripGeom<N1>::T_ELE
 template <int N1>
 static size_t tower_rows_smem()
 {
-    return sizeof(float2) * (RowGeom<N1>::T_ELEMS + N1 * 32) + sizeof(double) * RowGeom<N1>::R * N1 * 32;
+    return sizeof(float2) * (RowGeom<N1>::T_ELEMS + N1 * 32) + sizeof(uint32_t) * RowGeom<N1>::R * N1 * 32;
 }
 template <int N1>
 static size_t tower_finish_smem() { return sizeof(float2) * (RowGeom<N1>::T_ELEMS + N1 * 32); }
@@ -613,7 +619,7 @@ static void sparse_cols_impl(cudaStream_t s, float2 *slots, const unsigned *mask
 template <int N1>
 static void tower_rows_impl(cudaStream_t s, float2 *slots, const unsigned *masks, const int *bin_of_slot,
                             const int *group_begin, const int *group_end, const int *range, const int *counts,
-                            int slot_cap, int group_cap, const double *ph, float2 *partial, const float2 *tw)
+                            int slot_cap, int group_cap, const uint32_t *ph, float2 *partial, const float2 *tw)
 {
     const int rstrips = RowGeom<N1>::N / RowGeom<N1>::R;
     const size_t sm1 = tower_rows_smem<N1>();
@@ -670,7 +676,7 @@ void launch_sparse_cols(cudaStream_t s, float2 *slots, const unsigned *masks, co
 
 void launch_tower_rows(cudaStream_t s, float2 *slots, const unsigned *masks, const int *bin_of_slot,
                        const int *group_begin, const int *group_end, const int *range, const int *counts,
-                       int slot_cap, int group_cap, const double *ph, float2 *partial, int subgrid,
+                       int slot_cap, int group_cap, const uint32_t *ph, float2 *partial, int subgrid,
                        const float2 *tw)
 {
 #define CALL(N1) tower_rows_impl<N1>(s, slots, masks, bin_of_slot, group_begin, group_end, range, counts, \

@@ -4,12 +4,15 @@
 
 namespace rg {
 
-// ph[y*S + x] = winc (1 - sqrt(1 - l^2 - m^2)) for the fft-shifted pixel (y, x),
-// i.e. the reference's transfer pattern phase before cexp, at centred
-// coordinates ((x + S/2) mod S, (y + S/2) mod S) (src/reference/grid.c:304-319
-// followed by fft_shift); the column stage raises exp(2 pi i ph) to the power
-// -wp by multiplying the phase.  Round-to-nearest intrinsics: no contraction.
-__global__ void fresnel_table_kernel(double *__restrict__ ph, int S, double theta, double winc)
+// ph = winc (1 - sqrt(1 - l^2 - m^2)) for the fft-shifted pixel (y, x), i.e.
+// the reference's transfer pattern phase before cexp, at centred coordinates
+// ((x + S/2) mod S, (y + S/2) mod S) (src/reference/grid.c:304-319 followed by
+// fft_shift), computed in FP64 with round-to-nearest intrinsics (no
+// contraction) and stored as its fraction of a turn in 32-bit fixed point:
+// phq[y*S + x] = round(frac(ph) 2^32) mod 2^32.  The row stage raises
+// exp(2 pi i ph) to the power -wp as the integer product -wp * phq mod 2^32,
+// exact to |wp| 2^-33 turns.
+__global__ void fresnel_table_kernel(uint32_t *__restrict__ phq, int S, double theta, double winc)
 {
     const int64_t total = (int64_t)S * S;
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total;
@@ -19,16 +22,18 @@ __global__ void fresnel_table_kernel(double *__restrict__ ph, int S, double thet
         const double l = __ddiv_rn(__dmul_rn(theta, (double)(xc - S / 2)), (double)S);
         const double m = __ddiv_rn(__dmul_rn(theta, (double)(yc - S / 2)), (double)S);
         const double r = __dsqrt_rn(__dsub_rn(__dsub_rn(1.0, __dmul_rn(l, l)), __dmul_rn(m, m)));
-        ph[k] = __dmul_rn(winc, __dsub_rn(1.0, r));
+        const double ph = __dmul_rn(winc, __dsub_rn(1.0, r));
+        const double frac = __dsub_rn(ph, floor(ph));  // [0, 1), exact
+        phq[k] = (uint32_t)__double2ull_rn(ldexp(frac, 32));  // 2^32 wraps to 0
     }
 }
 
-void launch_fresnel_table(cudaStream_t s, double *ph, int subgrid, double theta, double winc)
+void launch_fresnel_table(cudaStream_t s, uint32_t *phq, int subgrid, double theta, double winc)
 {
     const int64_t total = (int64_t)subgrid * subgrid;
     int blocks = (int)((total + 255) / 256);
     if (blocks > 4096) blocks = 4096;
-    fresnel_table_kernel<<<blocks, 256, 0, s>>>(ph, subgrid, theta, winc);
+    fresnel_table_kernel<<<blocks, 256, 0, s>>>(phq, subgrid, theta, winc);
 }
 
 // a / d for 0 <= a < 2^24, d > 0: float reciprocal estimate, corrected to the

@@ -523,11 +523,11 @@ static rg_status wtowers_enqueue(rg_context *ctx, const DevVis &dv, const float2
     RG_CHECK(get_twiddles32(ctx, S, &tw));
     {
         char key[160];
-        std::snprintf(key, sizeof(key), "ph_%d_%.17g_%.17g", S, theta, winc);
+        std::snprintf(key, sizeof(key), "phq_%d_%.17g_%.17g", S, theta, winc);
         bool fresh = ctx->scratch.find(key) == ctx->scratch.end();
-        RG_CHECK(scratch(ctx, key, sizeof(double) * (size_t)sub_cells, &ph));
+        RG_CHECK(scratch(ctx, key, sizeof(uint32_t) * (size_t)sub_cells, &ph));
         if (fresh) {
-            launch_fresnel_table(st, (double *)ph, S, theta, winc);
+            launch_fresnel_table(st, (uint32_t *)ph, S, theta, winc);
             ctx->launches++;
         }
     }
@@ -597,7 +597,7 @@ static rg_status wtowers_enqueue(rg_context *ctx, const DevVis &dv, const float2
     end_stage(ctx);
     begin_stage(ctx, "tower_rows");
     launch_tower_rows(st, (float2 *)slots, (const unsigned *)masks, (const int *)bin_of_slot, (const int *)gbegin,
-                      (const int *)gend, range, counts, pl.slots_cap, pl.groups_cap, (const double *)ph,
+                      (const int *)gend, range, counts, pl.slots_cap, pl.groups_cap, (const uint32_t *)ph,
                       (float2 *)partial, S, tw);
     end_stage(ctx);
     begin_stage(ctx, "tower_finish");
