@@ -152,10 +152,27 @@ __global__ void prepare_towers_kernel(const double *__restrict__ u, const double
     __syncthreads();
     // first guesses only (the exact half-open tests below decide)
     const double inv_chunk = 1.0 / (double)g.chunk, inv_winc = 1.0 / g.winc;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const double uu = u[i], vv = v[i], ww = w[i];
-        const double2 vz = vis[i];
+    // The next visibility's inputs are loaded before this one is processed,
+    // so each thread has one set of loads in flight while it computes.
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    double nu = 0.0, nv = 0.0, nw = 0.0;
+    double2 nvz = make_double2(0.0, 0.0);
+    if (i < n) {
+        nu = u[i];
+        nv = v[i];
+        nw = w[i];
+        nvz = vis[i];
+    }
+    for (; i < n; i += stride) {
+        const double uu = nu, vv = nv, ww = nw;
+        const double2 vz = nvz;
+        if (i + stride < n) {
+            nu = u[i + stride];
+            nv = v[i + stride];
+            nw = w[i + stride];
+            nvz = vis[i + stride];
+        }
         visf[i] = make_float2((float)vz.x, (float)vz.y);
         int4 r = make_int4(-1, 0, 0, 0);
         if (!finite3(uu, vv, ww)) {
