@@ -75,7 +75,9 @@ __global__ void add_back_kernel(const float2 *__restrict__ subimg, const int *__
     if (cy_hi >= nchunk) cy_hi = nchunk - 1;
     const int64_t at = (int64_t)gy * N + gx;
     double2 acc = overwrite ? make_double2(0.0, 0.0) : master[at];
-    const double norm = (double)(S * S);
+    // S is a power of two, so 1 / S^2 is exact and multiplying by it gives
+    // the quotient the division would, bit for bit
+    const double inv_norm = 1.0 / (double)(S * S);
     for (int cy = cy_lo; cy <= cy_hi; cy++) {
         const int sy = ay - chunk * cy;
         if (sy < 0 || sy >= S) continue;
@@ -85,8 +87,8 @@ __global__ void add_back_kernel(const float2 *__restrict__ subimg, const int *__
             const int t = cy * nchunk + cx;
             if (tower_count[t] == 0) continue;
             const float2 z = subimg[(int64_t)t * S * S + (int64_t)sy * S + sx];
-            acc.x += (double)z.x / norm;
-            acc.y += (double)z.y / norm;
+            acc.x += (double)z.x * inv_norm;
+            acc.y += (double)z.y * inv_norm;
         }
     }
     master[at] = acc;
