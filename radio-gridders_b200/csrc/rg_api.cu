@@ -329,7 +329,7 @@ rg_status rg_context_destroy(rg_context *ctx)
     cudaStreamSynchronize(ctx->stream);
     for (auto &kv : ctx->tower_plans)
         if (kv.second.graph_exec) cudaGraphExecDestroy(kv.second.graph_exec);
-    for (int b = 0; b < 2; b++)
+    for (int b = 0; b < rg_context::kBatchSets; b++)
         for (cudaEvent_t e : {ctx->ev_in[b], ctx->ev_used[b], ctx->ev_done[b], ctx->ev_out[b]})
             if (e) cudaEventDestroy(e);
     if (ctx->copy_in) {
@@ -877,9 +877,9 @@ rg_status grid_wtowers_impl(rg_context *ctx, double *uvgrid, int grid_size, doub
 }
 
 // Several observations of one shape in one call, pipelined over three
-// streams: the inputs of step k+1 are copied in (copy_in) and the grid of step
-// k-1 copied out (copy_out) while step k's pass runs (ctx->stream), with two
-// sets of staging buffers.  Step 0 runs as an ordinary call (it sizes the plan,
+// streams: the inputs of later steps are copied in (copy_in) and the grids of
+// earlier steps copied out (copy_out) while step k's pass runs (ctx->stream),
+// with three sets of staging buffers.  Step 0 runs as an ordinary call (it sizes the plan,
 // tunes and stages the kernel table, which the later steps reuse) unless an
 // earlier call already sized and tuned the shape.  Each
 // pass's diagnostics land in their own pinned slot; after the last step they
@@ -890,7 +890,7 @@ static rg_status batch_streams(rg_context *ctx)
 {
     if (!ctx->copy_in) RG_CUDA(cudaStreamCreateWithFlags(&ctx->copy_in, cudaStreamNonBlocking));
     if (!ctx->copy_out) RG_CUDA(cudaStreamCreateWithFlags(&ctx->copy_out, cudaStreamNonBlocking));
-    for (int b = 0; b < 2; b++)
+    for (int b = 0; b < rg_context::kBatchSets; b++)
         for (cudaEvent_t *e : {&ctx->ev_in[b], &ctx->ev_used[b], &ctx->ev_done[b], &ctx->ev_out[b]})
             if (!*e) RG_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     return RG_OK;
@@ -946,13 +946,21 @@ rg_status grid_wtowers_batch_impl(rg_context *ctx, int count, double *const *uvg
         RG_CUDA(cudaMallocHost(&ctx->pinned_steps, (size_t)count * 64));
         ctx->pinned_steps_bytes = (size_t)count * 64;
     }
-    // two staging sets for inputs in host memory and for grids in host memory
-    void *in[2][4], *outb[2];
-    static const char *in_names[2][4] = {{"batch_u0", "batch_v0", "batch_w0", "batch_vis0"},
-                                         {"batch_u1", "batch_v1", "batch_w1", "batch_vis1"}};
-    for (int b = 0; b < 2; b++) {
-        for (int f = 0; f < 4; f++) RG_CHECK(scratch(ctx, in_names[b][f], f == 3 ? 2 * vb : vb, &in[b][f]));
-        RG_CHECK(scratch(ctx, b ? "batch_out1" : "batch_out0", grid_bytes, &outb[b]));
+    // Staging sets (kBatchSets) for inputs in host memory and for grids in
+    // host memory.  With three, the upload of step i may start as soon as the
+    // pass of step i-3 is done: two passes of slack for a copy that takes about
+    // as long as one pass.
+    constexpr int SETS = rg_context::kBatchSets;
+    void *in[SETS][4], *outb[SETS];
+    static const char *field[4] = {"u", "v", "w", "vis"};
+    for (int b = 0; b < SETS; b++) {
+        char name[32];
+        for (int f = 0; f < 4; f++) {
+            std::snprintf(name, sizeof(name), "batch_%s%d", field[f], b);
+            RG_CHECK(scratch(ctx, name, f == 3 ? 2 * vb : vb, &in[b][f]));
+        }
+        std::snprintf(name, sizeof(name), "batch_out%d", b);
+        RG_CHECK(scratch(ctx, name, grid_bytes, &outb[b]));
     }
     // the copy streams start after everything already on the context stream
     RG_CUDA(cudaEventRecord(ctx->ev_done[0], ctx->stream));
@@ -968,16 +976,16 @@ rg_status grid_wtowers_batch_impl(rg_context *ctx, int count, double *const *uvg
             cudaStreamSynchronize(c->copy_out);
         }
     } quiesce{ctx};
-    bool used[2] = {false, false}, out_pending[2] = {false, false};
+    bool used[SETS] = {}, out_pending[SETS] = {};
     for (int i = first; i < count; i++) {
-        const int b = i & 1;
+        const int b = i % SETS;
         const rg_vis &v = vis[i];
         const void *src[4] = {v.u, v.v, v.w, v.vis};
         const void *dev[4];
-        // Input staging set b was last read by step i-2's pass.  Its output
-        // staging buffer is only rewritten by this step's pass, so the wait for
-        // step i-2's grid copy-out goes on the pass, not on these copies: the
-        // uploads of step i overlap the download of step i-2.
+        // Input staging set b was last read by the pass of step i-SETS.  Its
+        // output staging buffer is only rewritten by this step's pass, so the
+        // wait for that step's grid copy-out goes on the pass, not on these
+        // copies: uploads never queue behind downloads.
         if (used[b]) RG_CUDA(cudaStreamWaitEvent(ctx->copy_in, ctx->ev_used[b], 0));
         for (int f = 0; f < 4; f++) {
             if (n == 0 || is_device_pointer(src[f])) {
@@ -1003,7 +1011,7 @@ rg_status grid_wtowers_batch_impl(rg_context *ctx, int count, double *const *uvg
         }
         RG_CUDA(cudaEventRecord(ctx->ev_in[b], ctx->copy_in));
         RG_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev_in[b], 0));
-        if (host_out && out_pending[b])  // step i-2's grid has left the output staging buffer
+        if (host_out && out_pending[b])  // step i-SETS has left the output staging buffer
             RG_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev_out[b], 0));
         RG_CHECK(wtowers_enqueue(ctx, dv, (const float2 *)taps, wkern, nullptr, out_dev, N, theta, S, M, winc, flags,
                                  pl, (char *)ctx->pinned_steps + (size_t)i * 64, (int *)poison));

@@ -104,8 +104,9 @@ struct rg_context {
     uint64_t scratch_gen = 0;  // bumped on every scratch (re)allocation: captured graphs go stale
     // batched W-towers calls: copy streams, their events, per-step diagnostics
     cudaStream_t copy_in = nullptr, copy_out = nullptr;
-    cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_used[2] = {nullptr, nullptr};
-    cudaEvent_t ev_done[2] = {nullptr, nullptr}, ev_out[2] = {nullptr, nullptr};
+    static constexpr int kBatchSets = 3;  // staging sets of a batch call
+    cudaEvent_t ev_in[kBatchSets] = {}, ev_used[kBatchSets] = {};
+    cudaEvent_t ev_done[kBatchSets] = {}, ev_out[kBatchSets] = {};
     void *pinned_steps = nullptr;
     size_t pinned_steps_bytes = 0;
     void *pinned = nullptr;  // small pinned host buffer (diagnostics read-back)
