@@ -161,9 +161,10 @@ rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double
 
 /* count observations of one shape (same visibility count) with one kernel
  * table: the same result as count rg_grid_wtowers calls in order (grid i from
- * vis[i] into uvgrids[i]), with the host-to-device copies of the next
- * observation and the device-to-host copy of the previous grid overlapping each
- * pass (two staging sets, three streams).  For streams of snapshots imaged
+ * vis[i] into uvgrids[i]), with the host-to-device copies of later
+ * observations and the device-to-host copies of earlier grids overlapping each
+ * pass (three staging sets of inputs and grid in device memory, three
+ * streams).  For streams of snapshots imaged
  * with one set of kernels; no counterpart in the reference.  Inputs and grids
  * in pinned host memory overlap fully; device buffers are used in place.
  * Returns the first error; the grids of the steps before it are complete. */
