@@ -95,7 +95,7 @@ def towers_image_error(ctx, oversampling=8, w_step=1.0):
             "region": "central half of each axis", "dft_s": time.time() - t0}
 
 
-def learned_towers(ctx, config="C1", steps=60000, n_triples=8192):
+def learned_towers(ctx, config="C1", steps=120000, n_triples=16384):
     """Learned-kernel W-towers against the table W-towers on the same
     workload: a network trained on the GPU (own forward/backward kernels) on
     generator kernels over the residual w range |w - w_mid| <= winc/2, then
