@@ -29,15 +29,21 @@ __global__ void minmax_w_kernel(const double *__restrict__ u, const double *__re
 {
     double lo = 0.0, hi = 0.0;
     bool bad = false;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const double ww = w[i];
-        if (!isfinite(ww)) {  // u and v are checked by the binning kernel
-            bad = true;
-            continue;
+    // four independent loads in flight per thread per round
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i0 < n; i0 += 4 * stride) {
+        double ww[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) ww[k] = i0 + k * stride < n ? w[i0 + k * stride] : 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (!isfinite(ww[k])) {  // u and v are checked by the binning kernel
+                bad = true;
+                continue;
+            }
+            lo = fmin(lo, ww[k]);
+            hi = fmax(hi, ww[k]);
         }
-        lo = fmin(lo, ww);
-        hi = fmax(hi, ww);
     }
     for (int o = 16; o > 0; o >>= 1) {
         lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
@@ -71,8 +77,10 @@ void launch_minmax_w(cudaStream_t s, const double *u, const double *v, const dou
     // compares above zero as an unsigned integer.  A device memset keeps the
     // sequence free of host copies (it is replayed from a captured graph).
     cudaMemsetAsync(out2, 0, 2 * sizeof(double), s);
-    int blocks = (int)((n + 255) / 256);
-    if (blocks > 4096) blocks = 4096;
+    // few CTAs: each ends with two atomics on the same two words, which
+    // serialise in L2
+    int blocks = (int)((n + 1023) / 1024);
+    if (blocks > 512) blocks = 512;
     if (blocks < 1) blocks = 1;
     minmax_w_kernel<<<blocks, 256, 0, s>>>(u, v, w, n, (unsigned long long *)out2, err);
 }
