@@ -208,6 +208,39 @@ rg_status rg_fft2d(rg_context *ctx, void *data, int batch, int ny, int nx, int s
 rg_status rg_dft_image(rg_context *ctx, double *image_out, int grid_size, double theta,
                        const rg_vis *vis, int precision, double factor);
 
+/* ---- file-level drop-ins for the reference's host wrappers --------------- */
+
+/* Same arguments as the reference's wrappers, so grid.cpp / dft.cpp change
+ * only the function name: read the crocodile HDF5 files (the rg_read_*_hdf5
+ * readers below: visibilities to wavelengths, baselines with first-sample
+ * length in [bl_min, bl_max) metres, w-kernels of group wkern/<theta %g>),
+ * grid or transform, and leave the dirty image in the caller's grid_size^2
+ * complex-double buffers as real part (imaginary part 0): the device buffer
+ * (which also holds the uv grid on the way) and, when non-NULL, the host
+ * one.  The image is the reference CPU pipeline's (src/reference/main.c:
+ * 258-294, hermitian then FFT); the reference's GPU wrappers leave half of it
+ * mirrored (no hermitian step, inverse FFT).  lambda, threads_per_block,
+ * blocks and threads_block are accepted and unused (the caller derives
+ * grid_size from lambda; launch shapes are the library's own).  Runs on the
+ * calling thread's current device with a context of its own; returns a status
+ * instead of exiting.
+ *
+ * Replaces wtowers_CUDA_flat (src/grid/grid_common.cuh:49-52,
+ * src/grid/grid_cuda.cu:522-744). */
+rg_status rg_wtowers_cuda_flat(const char *visfile, const char *wkernfile, double *grid, double *gridh,
+                               int grid_size, double theta, double lambda, double bl_min, double bl_max,
+                               int subgrid_size, int subgrid_margin, double winc);
+/* Replaces wproj_CUDA_flat (src/grid/grid_common.cuh:59-62). */
+rg_status rg_wproj_cuda_flat(const char *visfile, const char *wkernfile, double *grid, double *gridh,
+                             int grid_size, double theta, double lambda, double bl_min, double bl_max,
+                             int threads_per_block);
+/* Replaces image_dft_host_flat (src/dft/dft_common.cuh:16-18): the direct DFT
+ * image (FP64-reduced phase, the reference dft.out's scale) into grid_host
+ * and/or grid_dev. */
+rg_status rg_image_dft_host_flat(const char *visfile, double *grid_host, double *grid_dev, int grid_size,
+                                 double theta, double lambda, double bl_min, double bl_max, int blocks,
+                                 int threads_block);
+
 /* ---- crocodile HDF5 files ------------------------------------------------- */
 
 /* Flat visibilities read from a file; arrays owned by the struct, released

@@ -44,7 +44,8 @@ EXPORTS = [
     "rg_mlp_set_params", "rg_mlp_get_params", "rg_mlp_gradient", "rg_mlp_train", "rg_mlp_eval",
     "rg_grid_wprojection_learned", "rg_grid_wtowers_learned", "rg_grid_wtowers_batch", "rg_read_vis_hdf5", "rg_free_vis_data", "rg_read_wkern_hdf5",
     "rg_free_wkern_data", "rg_write_vis_hdf5", "rg_write_vis_flat_hdf5", "rg_write_wkern_hdf5", "rg_hdf5_read_f64",
-    "rg_hdf5_attr_f64", "rg_selftest_wait_timeout",
+    "rg_hdf5_attr_f64", "rg_selftest_wait_timeout", "rg_wtowers_cuda_flat", "rg_wproj_cuda_flat",
+    "rg_image_dft_host_flat",
 ]
 
 
@@ -135,6 +136,10 @@ def lib():
         L.rg_hdf5_read_f64.argtypes = [ct.c_char_p, ct.c_char_p, vp, i64, ct.POINTER(i64), ct.POINTER(i)]
         L.rg_hdf5_attr_f64.argtypes = [ct.c_char_p, ct.c_char_p, ct.c_char_p, ct.POINTER(d)]
         L.rg_selftest_wait_timeout.argtypes = [vp]
+        cp = ct.c_char_p
+        L.rg_wtowers_cuda_flat.argtypes = [cp, cp, vp, vp, i, d, d, d, d, i, i, d]
+        L.rg_wproj_cuda_flat.argtypes = [cp, cp, vp, vp, i, d, d, d, d, i]
+        L.rg_image_dft_host_flat.argtypes = [cp, vp, vp, i, d, d, d, d, i, i]
         for name in EXPORTS:
             getattr(L, name)  # raises AttributeError if a declared symbol is missing
         _lib = L

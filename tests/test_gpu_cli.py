@@ -67,3 +67,42 @@ def test_dft_out(oracle, files, precision, tol):
         f"-precision={precision}")
     ref = oracle.dft_image(n, th, u, v, w, vis, factor=2.0)
     assert rel_rms(_load(f"{d}/dft.img", n), ref) < tol
+
+
+def test_reference_wrapper_entry_points(rg, oracle, files):
+    """rg_wtowers_cuda_flat / rg_wproj_cuda_flat / rg_image_dft_host_flat take
+    the reference wrappers' argument lists (files, device grid, host grid,
+    grid_size, theta, lambda, bl_min, bl_max, ...) and leave the dirty image
+    as the real part of both complex buffers."""
+    import ctypes as ct
+
+    import torch
+    d, obs, (u, v, w, vis), wk = files
+    n, th, lam = obs.meta["grid_size"], obs.meta["theta"], obs.meta["lam"]
+    L = rg.lib()
+    for mode in ("wproj", "wtowers"):
+        dev = torch.zeros((n, n), dtype=torch.complex128, device="cuda")
+        host = np.zeros((n, n), np.complex128)
+        args = [f"{d}/vis.h5".encode(), f"{d}/wk.h5".encode(), ct.c_void_p(dev.data_ptr()),
+                host.ctypes.data_as(ct.c_void_p), n, th, lam, 0.0, 1e30]
+        if mode == "wproj":
+            st = L.rg_wproj_cuda_flat(*args, 256)
+            ref = oracle.grid_wprojection(n, th, u, v, w, vis, wk)
+        else:
+            st = L.rg_wtowers_cuda_flat(*args, 128, 16, 10.0)
+            ref = oracle.grid_wtowers(n, th, u, v, w, vis, wk, 128, 16, 10.0)
+        assert st == 0, rg.lib().rg_last_error()
+        img_ref = oracle.image_from_grid(ref.copy())
+        assert rel_rms(host.real, img_ref) < 1e-5
+        assert np.all(host.imag == 0)
+        assert np.array_equal(dev.cpu().numpy(), host)
+    lam_dft = 640.0
+    m = int(np.floor(lam_dft * th + 0.5))
+    host = np.zeros((m, m), np.complex128)
+    st = L.rg_image_dft_host_flat(f"{d}/vis.h5".encode(), host.ctypes.data_as(ct.c_void_p), None, m, th,
+                                  lam_dft, 0.0, 1e30, 64, 256)
+    assert st == 0, rg.lib().rg_last_error()
+    assert rel_rms(host.real, oracle.dft_image(m, th, u, v, w, vis, factor=1.0)) < 2e-5
+    # errors come back as a status, not an exit
+    assert L.rg_wtowers_cuda_flat(b"/nonexistent.h5", f"{d}/wk.h5".encode(), ct.c_void_p(dev.data_ptr()), None,
+                                  n, th, lam, 0.0, 1e30, 128, 16, 10.0) != 0
