@@ -7,6 +7,7 @@
 // (src/reference/main.c:258-294: hermitian, shift, FFT, shift); the
 // reference's GPU wrappers give half of it mirrored (no hermitian step, an
 // inverse FFT).  Errors come back as rg_status, never exit().
+#include <algorithm>
 #include <vector>
 
 #include "rg_internal.h"
