@@ -35,7 +35,7 @@ def test_forward_matches_oracle(rg, ctx, MO):
     y, _ = MO.forward(P, MO.features(*b, 16, 2000.0))
     ref = (y[:, 0] + 1j * y[:, 1]) * 0.05
     got = mlp.eval(rg.LearnedKernel.samples(*b))
-    # BF16 operands, FP32 accumulation
+    # BF16-rounded weights, FP16 activations (tcgen05), FP32 accumulation
     assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 2e-2
 
 
