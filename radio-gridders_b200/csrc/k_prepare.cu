@@ -130,6 +130,29 @@ __device__ __forceinline__ void frac_axis(double coord, double mid, double theta
     frac = (int)floor(__dadd_rn(__dmul_rn(__dsub_rn(x, (double)cell), (double)ov), 0.5));
 }
 
+// cp.async (shared <- global) of 8 or 16 bytes, its commit and bounded-depth wait
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+constexpr int kPrepTile = 256;  // = the kernel's block size
+constexpr int kPrepStages = 4;
+
 __global__ void prepare_towers_kernel(const double *__restrict__ u, const double *__restrict__ v,
                                       const double *__restrict__ w, const double2 *__restrict__ vis,
                                       int64_t n, TowerGeom g, const int *__restrict__ range,
@@ -154,39 +177,23 @@ __global__ void prepare_towers_kernel(const double *__restrict__ u, const double
     // divisions each) when they fit; the per-visibility search reads them
     constexpr int kBoundsCache = 256;
     __shared__ Bounds sb[kBoundsCache];
+    __shared__ __align__(16) double s_u[kPrepStages][kPrepTile], s_v[kPrepStages][kPrepTile],
+        s_w[kPrepStages][kPrepTile];
+    __shared__ __align__(16) double2 s_vz[kPrepStages][kPrepTile];
     const bool cached = g.nchunk <= kBoundsCache;
     if (cached)
         for (int c = threadIdx.x; c < g.nchunk; c += blockDim.x) sb[c] = tower_axis(c, g.chunk, g.grid_size, g.theta);
     __syncthreads();
     // first guesses only (the exact half-open tests below decide)
     const double inv_chunk = 1.0 / (double)g.chunk, inv_winc = 1.0 / g.winc;
-    // The next visibility's inputs are loaded before this one is processed,
-    // so each thread has one set of loads in flight while it computes.
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    double nu = 0.0, nv = 0.0, nw = 0.0;
-    double2 nvz = make_double2(0.0, 0.0);
-    if (i < n) {
-        nu = u[i];
-        nv = v[i];
-        nw = w[i];
-        nvz = vis[i];
-    }
-    for (; i < n; i += stride) {
-        const double uu = nu, vv = nv, ww = nw;
-        const double2 vz = nvz;
-        if (i + stride < n) {
-            nu = u[i + stride];
-            nv = v[i + stride];
-            nw = w[i + stride];
-            nvz = vis[i + stride];
-        }
+    // one visibility: the binning, coordinates and marks below
+    auto one = [&](int64_t i, double uu, double vv, double ww, double2 vz) {
         visf[i] = make_float2((float)vz.x, (float)vz.y);
         int4 r = make_int4(-1, 0, 0, 0);
         if (!finite3(uu, vv, ww)) {
             local_err |= DERR_NONFINITE;
             rec[i] = r;
-            continue;
+            return;
         }
         const double half_n = (double)(g.grid_size / 2);
         const int cxc = (int)floor((uu * g.theta + 0.5 + half_n) * inv_chunk);
@@ -220,7 +227,7 @@ __global__ void prepare_towers_kernel(const double *__restrict__ u, const double
         if (found_cx < 0 || found_cy < 0 || !have_wp) {
             dropped++;
             rec[i] = r;
-            continue;
+            return;
         }
         int cell_x, frac_x, cell_y, frac_y;
         const double wmid = __dmul_rn((double)found_wp, g.winc);
@@ -242,7 +249,7 @@ __global__ void prepare_towers_kernel(const double *__restrict__ u, const double
             if (plane < 0 || plane >= g.planes || tap < 0 || tap + ks2 > taps_total) {
                 local_err |= DERR_PLANE_RANGE;
                 rec[i] = r;
-                continue;
+                return;
             }
         }
         const int col0 = cell_x + g.subgrid / 2 - g.ksize / 2;
@@ -262,7 +269,33 @@ __global__ void prepare_towers_kernel(const double *__restrict__ u, const double
         for (int c = col0; c < col0 + g.ksize; c += kStripCols) mk[(c & (g.subgrid - 1)) / kStripCols] = 1;
         mk[((col0 + g.ksize - 1) & (g.subgrid - 1)) / kStripCols] = 1;
         gridded++;
+    };
+    // Inputs in tiles of kPrepTile visibilities staged through shared memory by
+    // cp.async, kPrepStages deep: each thread copies and then reads only its
+    // own elements, so the wait on its copy groups is the only ordering needed
+    // and kPrepStages - 1 tiles stay in flight while one is processed.
+    const int tid = threadIdx.x;
+    const int64_t ntiles = (n + kPrepTile - 1) / kPrepTile;
+    auto fetch = [&](int64_t tile, int stage) {
+        const int64_t i = tile * kPrepTile + tid;
+        if (tile < ntiles && i < n) {
+            cp_async8(&s_u[stage][tid], u + i);
+            cp_async8(&s_v[stage][tid], v + i);
+            cp_async8(&s_w[stage][tid], w + i);
+            cp_async16(&s_vz[stage][tid], vis + i);
+        }
+        cp_async_commit();  // possibly empty: keeps the group count per tile
+    };
+    for (int s = 0; s < kPrepStages - 1; s++) fetch(blockIdx.x + (int64_t)s * gridDim.x, s);
+    int k = 0;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, k++) {
+        fetch(tile + (int64_t)(kPrepStages - 1) * gridDim.x, (k + kPrepStages - 1) % kPrepStages);
+        cp_async_wait<kPrepStages - 1>();
+        const int stage = k % kPrepStages;
+        const int64_t i = tile * kPrepTile + tid;
+        if (i < n) one(i, s_u[stage][tid], s_v[stage][tid], s_w[stage][tid], s_vz[stage][tid]);
     }
+    cp_async_wait<0>();
     if (local_err) atomicOr(err, local_err);
     // warp-aggregated counters
     for (int o = 16; o > 0; o >>= 1) {
