@@ -45,3 +45,16 @@ def test_no_device_is_reported_not_faked(rg):
     with pytest.raises(rg.RGError) as e:
         rg.Context(0)
     assert e.value.status == 6
+
+
+def test_reference_wrapper_entries_reject_null_arguments():
+    """The file-level entries with the reference wrappers' argument lists
+    check their pointers before touching CUDA or the files, and report
+    RG_ERR_INVALID_ARGUMENT instead of exiting."""
+    import importlib
+    rg = importlib.import_module("radio-gridders_b200")
+    L = rg.lib()
+    assert L.rg_wtowers_cuda_flat(None, b"wk.h5", None, None, 64, 0.1, 640.0, 0.0, 1e30, 32, 8, 10.0) == 1
+    assert L.rg_wproj_cuda_flat(b"vis.h5", None, ct.c_void_p(1), None, 64, 0.1, 640.0, 0.0, 1e30, 256) == 1
+    assert L.rg_image_dft_host_flat(b"vis.h5", None, None, 64, 0.1, 640.0, 0.0, 1e30, 1, 1) == 1
+    assert b"NULL" in L.rg_last_error() or b"buffer" in L.rg_last_error()
