@@ -152,16 +152,18 @@ __device__ __forceinline__ void col_step1(const float2 *__restrict__ src, int ld
 
 template <int N1, int SIGN>
 __global__ void __launch_bounds__(256) fft32_cols_kernel(float2 *__restrict__ data,
-                                                         const float2 *__restrict__ tw)
+                                                         const float2 *__restrict__ tw,
+                                                         const int *__restrict__ live)
 {
     using G = ColGeom<N1>;
     constexpr int N = G::N;
     extern __shared__ float2 smem[];
     float2 *T = smem;
     float2 *W = smem + G::T_ELEMS;
-    load_twiddles<N1>(W, tw);
     const int strip = blockIdx.x % (N / G::C);
     const int64_t arr = blockIdx.x / (N / G::C);
+    if (live && live[arr] == 0) return;  // an array nobody reads (a tower without data)
+    load_twiddles<N1>(W, tw);
     float2 *base = data + arr * N * N + strip * G::C;
     __syncthreads();
     col_step1<N1, SIGN>(base, N, T, W);
@@ -590,16 +592,16 @@ static void rows_impl(cudaStream_t s, float2 *data, int64_t rows, int sign, cons
 }
 
 template <int N1>
-static void cols_impl(cudaStream_t s, float2 *data, int batch, int sign, const float2 *tw)
+static void cols_impl(cudaStream_t s, float2 *data, int batch, int sign, const float2 *tw, const int *live)
 {
     const size_t sm = cols_smem<N1>();
     const unsigned blocks = (unsigned)batch * (N1 * 32 / ColGeom<N1>::C);
     if (sign < 0) {
         cudaFuncSetAttribute(fft32_cols_kernel<N1, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        fft32_cols_kernel<N1, -1><<<blocks, 256, sm, s>>>(data, tw);
+        fft32_cols_kernel<N1, -1><<<blocks, 256, sm, s>>>(data, tw, live);
     } else {
         cudaFuncSetAttribute(fft32_cols_kernel<N1, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        fft32_cols_kernel<N1, +1><<<blocks, 256, sm, s>>>(data, tw);
+        fft32_cols_kernel<N1, +1><<<blocks, 256, sm, s>>>(data, tw, live);
     }
 }
 
@@ -659,9 +661,9 @@ void launch_fft32_rows(cudaStream_t s, float2 *data, int64_t rows, int n, int si
 #undef CALL
 }
 
-void launch_fft32_cols(cudaStream_t s, float2 *data, int batch, int n, int sign, const float2 *tw)
+void launch_fft32_cols(cudaStream_t s, float2 *data, int batch, int n, int sign, const float2 *tw, const int *live)
 {
-#define CALL(N1) cols_impl<N1>(s, data, batch, sign, tw)
+#define CALL(N1) cols_impl<N1>(s, data, batch, sign, tw, live)
     RG_DISPATCH_N1(n, CALL)
 #undef CALL
 }

@@ -605,7 +605,7 @@ static rg_status wtowers_enqueue(rg_context *ctx, const DevVis &dv, const float2
                         (const float2 *)partial, (float2 *)subimg, S, tw);
     end_stage(ctx);
     begin_stage(ctx, "fft_cols_forward");
-    launch_fft32_cols(st, (float2 *)subimg, ntowers, S, -1, tw);
+    launch_fft32_cols(st, (float2 *)subimg, ntowers, S, -1, tw, (const int *)tcount);  // towers with data only
     end_stage(ctx);
     begin_stage(ctx, "add_back");
     launch_add_back(st, (const float2 *)subimg, (const int *)tcount, (double2 *)out_dev, N, S, M, chunk, nchunk,

@@ -161,9 +161,10 @@ void fft32_init_twiddles(cudaStream_t s, float2 *tw, int n);  // tw: n entries
 // batched row transforms: rows = count of rows of length n (contiguous)
 void launch_fft32_rows(cudaStream_t s, float2 *data, int64_t rows, int n, int sign,
                        const float2 *tw, const int *count_dev = nullptr);
-// column transforms of `batch` n x n arrays
+// column transforms of `batch` n x n arrays; arrays b with live[b] == 0 are
+// left as they are (live may be NULL: all)
 void launch_fft32_cols(cudaStream_t s, float2 *data, int batch, int n, int sign,
-                       const float2 *tw);
+                       const float2 *tw, const int *live = nullptr);
 // FP64 transforms for image formation (n power of two, <= 4096)
 bool fft64_supported(int n);
 void launch_fft64_2d(cudaStream_t s, double2 *data, double2 *tmp, int batch, int ny, int nx,
