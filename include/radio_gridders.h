@@ -146,7 +146,11 @@ rg_status rg_grid_wprojection(rg_context *ctx, double *uvgrid, int grid_size, do
  * device resolves the array's address (cudaGetSymbolAddress); make that first
  * call before any stream capture.  Calls share the array: calls that overlap
  * on the GPU (other streams, other host threads) race.  Runs on the calling
- * thread's current device and returns after the grid is written. */
+ * thread's current device.  The call synchronises with `cuda_stream` twice:
+ * it reads the error word back before it touches uvgrid (a call rejected for
+ * its data, e.g. w outside the table, leaves uvgrid as it was), and it returns
+ * after the grid is written.  A CUDA error already pending when the call
+ * starts is returned as RG_ERR_CUDA with a message that says so. */
 rg_status rg_grid_wprojection_noalloc(double *uvgrid, int grid_size, double theta,
                                       const rg_vis *vis, const rg_wkern *wkern, int flags,
                                       void *cuda_stream);

@@ -27,17 +27,21 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
 REF = os.path.join(HERE, "_ref")
-REFERENCE_SRC = "/root/reference/src/reference"
+# Directory of the reference's src/reference sources (read in place); set by
+# the caller, no default.
+REFERENCE_SRC = os.environ.get("RG_REFERENCE_SRC")
 
 _c_double_p = ct.POINTER(ct.c_double)
 
 
-def build(reference: bool = True) -> None:
-    """Compile the restatement (always) and the reference build (when the
-    reference sources are present on this machine)."""
+def build(reference: bool = True, reference_src: str | None = None) -> None:
+    """Compile the restatement (always) and the reference build from the
+    reference's src/reference directory (``reference_src``, else the
+    RG_REFERENCE_SRC environment variable) when one is given and present."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    if reference and os.path.isdir(REFERENCE_SRC):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    src = reference_src or REFERENCE_SRC
+    if reference and src and os.path.isdir(src):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_SRC={src}"], check=True)
 
 
 def _ptr(a):
@@ -73,6 +77,7 @@ def lib():
         L.rgo_fft_shift.argtypes = [vp, i]
         L.rgo_image_from_grid.argtypes = [vp, i, vp]
         L.rgo_dft_image.argtypes = [vp, i, d, i64, vp, vp, vp, vp, d]
+        L.rgo_dft_pixels.argtypes = [vp, i, vp, vp, i, d, i64, vp, vp, vp, vp, d]
         L.rgo_frac_coord.argtypes = [i, i, i, d, d, d, d, d, ct.POINTER(i), ct.POINTER(i)]
         _lib = L
     return _lib
@@ -142,6 +147,17 @@ def dft_image(grid_size, theta, u, v, w, vis, factor=2.0):
     lib().rgo_dft_image(_ptr(img), grid_size, theta, len(u), _ptr(u), _ptr(v), _ptr(w),
                         _ptr(vis), factor)
     return img
+
+
+def dft_pixels(grid_size, theta, u, v, w, vis, px, py, factor=2.0):
+    """The FP64 DFT oracle at pixels (px[k], py[k]) (column, row) only."""
+    u, v, w, vis = _flat(u, v, w, vis)
+    px = np.ascontiguousarray(px, np.int32)
+    py = np.ascontiguousarray(py, np.int32)
+    out = np.zeros(len(px), np.float64)
+    lib().rgo_dft_pixels(_ptr(out), len(px), _ptr(px), _ptr(py), grid_size, theta, len(u), _ptr(u), _ptr(v),
+                         _ptr(w), _ptr(vis), factor)
+    return out
 
 
 def frac_coord(grid_size, ksize, ov, theta, u, v, du=0.0, dv=0.0):

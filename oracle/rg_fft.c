@@ -42,12 +42,22 @@ void rgo_fft1d(double complex *x, int n, int stride, int sign)
         for (int b = 0; b < bits; b++) { r = (r << 1) | (v & 1u); v >>= 1; }
         a[r] = x[(size_t)i * stride];
     }
-    /* twiddle table w[k] = exp(sign*2*pi*i*k/n), k < n/2 */
-    double complex *w = (double complex *)malloc(sizeof(double complex) * (size_t)(n / 2));
-    for (int k = 0; k < n / 2; k++) {
-        double ang = sign * 2.0 * M_PI * (double)k / (double)n;
-        w[k] = cos(ang) + I * sin(ang);
+    /* twiddle table w[k] = exp(sign*2*pi*i*k/n), k < n/2: computed once per
+     * thread, length and sign and kept (the same values every call, so the
+     * results are unchanged; a plan's precomputed table, as FFTW keeps one) */
+    static __thread double complex *tw_cache = NULL;
+    static __thread int tw_n = 0, tw_sign = 0;
+    if (tw_n != n || tw_sign != sign) {
+        free(tw_cache);
+        tw_cache = (double complex *)malloc(sizeof(double complex) * (size_t)(n / 2));
+        for (int k = 0; k < n / 2; k++) {
+            double ang = sign * 2.0 * M_PI * (double)k / (double)n;
+            tw_cache[k] = cos(ang) + I * sin(ang);
+        }
+        tw_n = n;
+        tw_sign = sign;
     }
+    const double complex *w = tw_cache;
     for (int len = 2; len <= n; len <<= 1) {
         int half = len >> 1, step = n / len;
         for (int s = 0; s < n; s += len) {
@@ -60,7 +70,6 @@ void rgo_fft1d(double complex *x, int n, int stride, int sign)
         }
     }
     for (int i = 0; i < n; i++) x[(size_t)i * stride] = a[i];
-    free(w);
     free(a);
 }
 

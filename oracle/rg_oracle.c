@@ -97,7 +97,7 @@ static void tower_bounds(int c, int chunk_size, int grid_size, double theta,
     *mid = (double)(*x_min + chunk_size / 2) / theta;
 }
 
-/* grid.c:295-555 (serial).  The reference scans every baseline of a tower's bin
+/* grid.c:295-555 (its serial build).  The reference scans every baseline of a tower's bin
  * once per w-floor and grids the visibilities passing the half-open (u,v,w)
  * cut in baseline/time/frequency order.  Here the same cut is applied once per
  * visibility (testing the neighbouring towers/floors with the reference's exact
@@ -184,13 +184,22 @@ uint64_t rgo_grid_wtowers(double complex *uvgrid, int grid_size, double theta,
     free(fill);
     if (gridded_count) memset(gridded_count, 0, sizeof(int32_t) * (size_t)nvis);
 
-    double complex *subgrid = (double complex *)calloc((size_t)S * S, sizeof(double complex));
-    double complex *subimg = (double complex *)calloc((size_t)S * S, sizeof(double complex));
     uint64_t flops = 0;
     const int sg_norm = S * S;
     double complex *uvgrid_mid = uvgrid + (grid_size + 1) * grid_size / 2;
+    /* Towers are independent until the add-back: each is computed on its own
+     * thread into its own sub-image, and the sub-images are then added to the
+     * grid one after another in tower order, so the result does not depend on
+     * the thread count. */
+    const int ntowers = nchunk * nchunk;
+    double complex **finished = (double complex **)calloc((size_t)ntowers, sizeof(double complex *));
 
-    for (int c = 0; c < nchunk * nchunk; c++) {
+#pragma omp parallel reduction(+ : flops)
+    {
+    double complex *subgrid = (double complex *)calloc((size_t)S * S, sizeof(double complex));
+    double complex *subimg = (double complex *)calloc((size_t)S * S, sizeof(double complex));
+#pragma omp for schedule(dynamic, 1)
+    for (int c = 0; c < ntowers; c++) {
         int cx = c % nchunk, cy = c / nchunk;
         int x_min, y_min;
         double ulo, uhi, umid, vlo, vhi, vmid;
@@ -208,7 +217,10 @@ uint64_t rgo_grid_wtowers(double complex *uvgrid, int grid_size, double theta,
                 int64_t i = order[p];
                 flops += w_project_one(subgrid, S, theta, u[i], v[i], w[i], vis[i],
                                        umid, vmid, w_mid, wk);
-                if (gridded_count) gridded_count[i]++;
+                if (gridded_count) {
+#pragma omp atomic
+                    gridded_count[i]++;
+                }
             }
             have_vis = 1;
             /* back to the image plane, step the accumulated sub-image to this
@@ -226,6 +238,21 @@ uint64_t rgo_grid_wtowers(double complex *uvgrid, int grid_size, double theta,
         if (last_wp != 0)
             for (int k = 0; k < S * S; k++) subimg[k] /= int_power(wtransfer[k], last_wp);
         rgo_fft2d(subimg, subimg, S, S, -1);
+        finished[c] = subimg;
+        subimg = (double complex *)calloc((size_t)S * S, sizeof(double complex));
+    }
+    free(subgrid);
+    free(subimg);
+    }
+
+    for (int c = 0; c < ntowers; c++) {
+        if (!finished[c]) continue;
+        const double complex *subimg = finished[c];
+        int cx = c % nchunk, cy = c / nchunk;
+        int x_min, y_min;
+        double ulo, uhi, umid, vlo, vhi, vmid;
+        tower_bounds(cx, chunk, grid_size, theta, &x_min, &ulo, &uhi, &umid);
+        tower_bounds(cy, chunk, grid_size, theta, &y_min, &vlo, &vhi, &vmid);
         /* add the sub-grid, margins included, clipped to the grid (grid.c:503-516) */
         int x0 = x_min - M / 2, x1 = x0 + S;
         int y0 = y_min - M / 2, y1 = y0 + S;
@@ -237,9 +264,10 @@ uint64_t rgo_grid_wtowers(double complex *uvgrid, int grid_size, double theta,
             for (int x = x0; x < x1; x++)
                 uvgrid_mid[x + y * grid_size] +=
                     (subimg[(x - x_min + M / 2) + (y - y_min + M / 2) * S] / sg_norm);
+        free(finished[c]);
     }
 
-    free(subgrid); free(subimg); free(order); free(start);
+    free(finished); free(order); free(start);
     free(pair_bin); free(pair_vis); free(wtransfer);
     return flops;
 }
@@ -304,29 +332,45 @@ void rgo_image_from_grid(double complex *uvgrid, int grid_size, double *image)
     for (long long k = 0; k < (long long)grid_size * grid_size; k++) image[k] = creal(uvgrid[k]);
 }
 
+/* One pixel of the FP64 DFT oracle: factor * sum_k Re(V_k exp(2 pi i ph_k)),
+ * ph = u l + v m + w (1 - n) reduced to [-1/2, 1/2] turns in FP64 before the
+ * FP64 sin/cos, summed with Neumaier compensation. */
+static double dft_pixel(int x, int y, int N, double theta, int64_t nvis, const double *u,
+                        const double *v, const double *w, const double complex *vis, double factor)
+{
+    double m = theta * (double)(y - N / 2) / N;
+    double l = theta * (double)(x - N / 2) / N;
+    double one_minus_n = 1.0 - sqrt(1.0 - l * l - m * m);
+    double sum = 0.0, comp = 0.0;
+    for (int64_t k = 0; k < nvis; k++) {
+        double ph = u[k] * l + v[k] * m + w[k] * one_minus_n;
+        ph -= nearbyint(ph);
+        double a = 2.0 * M_PI * ph;
+        double term = creal(vis[k]) * cos(a) + cimag(vis[k]) * sin(a);
+        double t = sum + term; /* Neumaier compensated sum */
+        if (fabs(sum) >= fabs(term)) comp += (sum - t) + term;
+        else comp += (term - t) + sum;
+        sum = t;
+    }
+    return factor * (sum + comp);
+}
+
 void rgo_dft_image(double *image, int grid_size, double theta, int64_t nvis,
                    const double *u, const double *v, const double *w,
                    const double complex *vis, double factor)
 {
     const int N = grid_size;
 #pragma omp parallel for schedule(dynamic, 1)
-    for (int y = 0; y < N; y++) {
-        double m = theta * (double)(y - N / 2) / N;
-        for (int x = 0; x < N; x++) {
-            double l = theta * (double)(x - N / 2) / N;
-            double one_minus_n = 1.0 - sqrt(1.0 - l * l - m * m);
-            double sum = 0.0, comp = 0.0;
-            for (int64_t k = 0; k < nvis; k++) {
-                double ph = u[k] * l + v[k] * m + w[k] * one_minus_n;
-                ph -= nearbyint(ph);
-                double a = 2.0 * M_PI * ph;
-                double term = creal(vis[k]) * cos(a) + cimag(vis[k]) * sin(a);
-                double t = sum + term; /* Neumaier compensated sum */
-                if (fabs(sum) >= fabs(term)) comp += (sum - t) + term;
-                else comp += (term - t) + sum;
-                sum = t;
-            }
-            image[(size_t)y * N + x] = factor * (sum + comp);
-        }
-    }
+    for (int y = 0; y < N; y++)
+        for (int x = 0; x < N; x++)
+            image[(size_t)y * N + x] = dft_pixel(x, y, N, theta, nvis, u, v, w, vis, factor);
+}
+
+void rgo_dft_pixels(double *out, int npix, const int *px, const int *py, int grid_size, double theta,
+                    int64_t nvis, const double *u, const double *v, const double *w,
+                    const double complex *vis, double factor)
+{
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int k = 0; k < npix; k++)
+        out[k] = dft_pixel(px[k], py[k], grid_size, theta, nvis, u, v, w, vis, factor);
 }

@@ -79,6 +79,10 @@ void rgo_image_from_grid(double complex *uvgrid, int grid_size, double *image);
 void rgo_dft_image(double *image, int grid_size, double theta, int64_t nvis,
                    const double *u, const double *v, const double *w,
                    const double complex *vis, double factor);
+/* The same DFT at the npix pixels (px[k], py[k]) only (column x, row y). */
+void rgo_dft_pixels(double *out, int npix, const int *px, const int *py, int grid_size, double theta,
+                    int64_t nvis, const double *u, const double *v, const double *w,
+                    const double complex *vis, double factor);
 
 #ifdef __cplusplus
 }

@@ -797,17 +797,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mlp_eval_kernel(const float *__
 // Gridding with learned taps.  A visibility's K x K taps are K*K / 128 tiles
 // (one half-filled tile for K = 8); tap t = ty * K + tx of the tile row is
 // scattered as grid[goff + ty * ld + tx] += vis * conj(tap) where that index
-// lies in [0, limit).  The groups of a CTA take visibilities in turn.
+// lies in [0, limit) — or, when axes is set, where column col0 + tx and row
+// row0 + ty both lie in [0, ld).  The groups of a CTA take visibilities in
+// turn.
 // ---------------------------------------------------------------------------
 struct LearnedVis {
     float wf, du, dv, vr, vi;
     float2 *grid;
     int64_t goff, ld, limit;
+    int col0, row0;
+    bool axes;
 };
 
 // W-projection: x = theta u, cell = floor(x), du = x - cell (continuous — no
-// oversampling quantisation); footprint column cell - K/2 + tx; the
-// reference's linear index rule (dropped outside [0, N^2)).
+// oversampling quantisation); footprint column cell - K/2 + tx; taps whose
+// column or row leaves the grid are dropped (the reference GPU gridder's
+// per-axis check, src/grid/grid_cuda.cu:25-41).
 struct WprojVisSource {
     const double *u, *v, *w;
     const double2 *vis;
@@ -828,6 +833,9 @@ struct WprojVisSource {
         o.grid = grid;
         o.ld = N;
         o.limit = (int64_t)N * N;
+        o.col0 = (int)cx - ksize / 2 + N / 2;
+        o.row0 = (int)cy - ksize / 2 + N / 2;
+        o.axes = true;
         return true;
     }
 };
@@ -860,6 +868,8 @@ struct TowersVisSource {
         o.goff = r.y;
         o.ld = sub;
         o.limit = (int64_t)sub * sub;
+        o.col0 = o.row0 = 0;
+        o.axes = false;
         return true;
     }
 };
@@ -897,7 +907,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) learned_grid_kernel(Src src, in
             const float2 y = tc_tile(S, g, r, phase, b4, err, &ok);
             const float kr = y.x * scale, ki = y.y * scale;
             const int64_t idx = o.goff + (int64_t)(t / ksize) * o.ld + (t % ksize);
-            if (ok && t < taps && idx >= 0 && idx < o.limit)
+            const bool inside = o.axes ? ((unsigned)(o.col0 + t % ksize) < (unsigned)o.ld &&
+                                          (unsigned)(o.row0 + t / ksize) < (unsigned)o.ld)
+                                       : (idx >= 0 && idx < o.limit);
+            if (ok && t < taps && inside)
                 atomicAdd(o.grid + (strip_lg ? (int64_t)strip_addr((int)idx, strip_lg) : idx),
                           make_float2(o.vr * kr + o.vi * ki, o.vi * kr - o.vr * ki));
         }

@@ -362,7 +362,7 @@ __global__ void prepare_wproj_kernel(const double *__restrict__ u, const double 
         r.x = 0;
         r.y = row0 * grid_size + col0;
         r.z = (int)tap;
-        r.w = ((row0 & 63) << 8) | (col0 & 63);
+        r.w = ((row0 + 64) << 16) | (col0 + 64);  // the origin itself: Romein checks each axis
         rec[i] = r;
     }
     if (local_err) atomicOr(err, local_err);

@@ -11,14 +11,18 @@
 // registers.  Per tap: sum += vis * conj(tap), the reference's
 // grid += v * conj(wk) (src/reference/grid.c:177-182).
 //
-// The linear index grid_offset + cv * side + cu is the reference's
-// grid_offset + y*size + x (mapped to the strip-major sub-grid layout when
-// strip_lg is set: the W-towers sub-grids, whose kernel table then holds every
-// slice twice); points outside [0, side^2) are dropped (the
-// reference does not check, grid.c:177-182; its GPU gridder drops them,
-// src/grid/grid_cuda.cu:25-41).  The record carries grid_offset and the
-// footprint origin's residues modulo 64, so a thread's tap (cu, cv) is two
-// subtractions and masks.
+// Sub-grids of the W-towers pass (STRIP): the linear index grid_offset + cv *
+// side + cu is the reference's grid_offset + y*size + x (grid.c:177-182),
+// mapped to the strip-major layout (whose kernel table holds every slice
+// twice); points outside [0, side^2) are dropped.  The record carries
+// grid_offset and the footprint origin's residues modulo 64.
+// The W-projection grid (not STRIP): each tap's column and row are checked
+// separately and taps outside [0, side) on either axis are dropped, as the
+// reference GPU gridder does (src/grid/grid_cuda.cu:25-41; the CPU grid.c
+// checks nothing, so a footprint crossing the left or right edge would wrap
+// into the neighbouring row).  The record carries the origin itself,
+// r.w = (row0 + 64) << 16 | (col0 + 64).  Either way a thread's tap (cu, cv)
+// is two subtractions and masks (K divides 64).
 //
 // Visibilities are staged through shared memory in batches (coalesced 16-byte
 // record and 8-byte visibility loads); taps are read through the read-only
@@ -79,7 +83,8 @@ __global__ void __launch_bounds__(K *K / P, (RomeinBounds<K, P>::min_ctas)) rome
                 const int4 r = srec[j];
                 if (r.x < 0) continue;
                 const int cu = (myU - (r.w & 0xff)) & (K - 1);
-                const int cv0 = (myV0 - (r.w >> 8)) & (K - 1);  // slice row of the thread's first point
+                // slice row of the thread's first point
+                const int cv0 = (myV0 - (STRIP ? (r.w >> 8) : (r.w >> 16))) & (K - 1);
                 float2 t[P];
                 if (STRIP) {
                     // duplicated slices (2K rows): rows cv0 + p*RS need no wrap, so the
@@ -104,8 +109,20 @@ __global__ void __launch_bounds__(K *K / P, (RomeinBounds<K, P>::min_ctas)) rome
                 cur_goff = r.y;
                 cur_res = r.w;
                 int idx[P];
+                if (STRIP) {
 #pragma unroll
-                for (int p = 0; p < P; p++) idx[p] = r.y + ((cv0 + p * RS) & (K - 1)) * side + cu;
+                    for (int p = 0; p < P; p++) idx[p] = r.y + ((cv0 + p * RS) & (K - 1)) * side + cu;
+                } else {
+                    // per-axis check; -1 (never flushed) for a tap off the grid
+                    const int col = (r.w & 0xffff) - 64 + cu;
+                    const int row0 = (r.w >> 16) - 64;
+#pragma unroll
+                    for (int p = 0; p < P; p++) {
+                        const int row = row0 + ((cv0 + p * RS) & (K - 1));
+                        idx[p] = ((unsigned)col < (unsigned)side && (unsigned)row < (unsigned)side) ? row * side + col
+                                                                                                  : -1;
+                    }
+                }
                 if (r.x != cur_bin) {
 #pragma unroll
                     for (int p = 0; p < P; p++) {

@@ -154,7 +154,7 @@ static rg_status diag_end(rg_context *ctx, const Diag &d, unsigned long long *co
     return RG_OK;
 }
 
-static rg_status check_vis(const rg_vis *vis)
+rg_status check_vis(const rg_vis *vis)
 {
     if (!vis) return fail(RG_ERR_INVALID_ARGUMENT, "vis is NULL");
     if (vis->n < 0) return fail(RG_ERR_INVALID_ARGUMENT, "vis->n is negative");
@@ -164,7 +164,7 @@ static rg_status check_vis(const rg_vis *vis)
     return RG_OK;
 }
 
-static rg_status check_wkern(const rg_wkern *wk)
+rg_status check_wkern(const rg_wkern *wk)
 {
     if (!wk || !wk->data) return fail(RG_ERR_INVALID_ARGUMENT, "w-kernel table is NULL");
     if (wk->size != 4 && wk->size != 8 && wk->size != 16 && wk->size != 32)

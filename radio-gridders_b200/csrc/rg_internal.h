@@ -125,6 +125,12 @@ void begin_stage(rg_context *ctx, const char *name);
 void end_stage(rg_context *ctx);
 void collect_timings(rg_context *ctx);
 
+// Argument checks shared by the entry points: the visibility arrays (NULL
+// pointers, negative or > 2^31 counts) and the w-kernel table description
+// (support, oversampling, plane count, finite w_min and positive w_step).
+rg_status check_vis(const rg_vis *vis);
+rg_status check_wkern(const rg_wkern *wk);
+
 // Device scratch that persists in the context and grows on demand.
 rg_status scratch(rg_context *ctx, const char *name, size_t bytes, void **out);
 

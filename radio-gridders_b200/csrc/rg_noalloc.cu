@@ -14,6 +14,7 @@
 // taps (e.g. 16x16 taps x 8x8 oversampling x 32 planes); any number of
 // visibilities (they are processed in batches of 65,536).  Every GPU that loads
 // the library holds the array (about 13.5 MiB) until the process exits.
+#include <cmath>
 #include <cstring>
 #include <mutex>
 
@@ -97,19 +98,15 @@ extern "C" rg_status rg_grid_wprojection_noalloc(double *uvgrid, int grid_size, 
                                                  const rg_vis *vis, const rg_wkern *wkern,
                                                  int flags, void *cuda_stream)
 {
-    if (!uvgrid || !vis || !wkern || !wkern->data)
-        return fail(RG_ERR_INVALID_ARGUMENT, "uvgrid, vis and wkern must be non-NULL");
+    if (!uvgrid) return fail(RG_ERR_INVALID_ARGUMENT, "uvgrid must be non-NULL");
     if (grid_size < 2 || grid_size > kMaxGrid)
         return fail(RG_ERR_UNSUPPORTED, "rg_grid_wprojection_noalloc: grid_size must be in [2, 1024] "
                                         "(its fixed scratch holds a 1024 x 1024 FP32 grid)");
-    if (!(theta > 0.0)) return fail(RG_ERR_INVALID_ARGUMENT, "theta must be > 0");
-    if (vis->n < 0 || vis->n > (int64_t)1 << 31) return fail(RG_ERR_INVALID_ARGUMENT, "bad visibility count");
+    if (!(theta > 0.0) || !std::isfinite(theta)) return fail(RG_ERR_INVALID_ARGUMENT, "theta must be > 0");
+    // the checks rg_grid_wprojection makes (finite w_min, positive w_step, ...)
+    RG_CHECK(check_vis(vis));
+    RG_CHECK(check_wkern(wkern));
     const int K = wkern->size;
-    if (K != 4 && K != 8 && K != 16 && K != 32)
-        return fail(RG_ERR_UNSUPPORTED, "kernel support must be 4, 8, 16 or 32 cells");
-    if (wkern->oversampling < 1 || wkern->oversampling > 64 || wkern->plane_count < 1 ||
-        !(wkern->w_step > 0.0))
-        return fail(RG_ERR_INVALID_ARGUMENT, "bad w-kernel table description");
     const int64_t ntaps = (int64_t)wkern->plane_count * wkern->oversampling * wkern->oversampling * K * K;
     if (ntaps > kMaxTaps)
         return fail(RG_ERR_UNSUPPORTED, "rg_grid_wprojection_noalloc: the w-kernel table must hold at "
@@ -121,6 +118,11 @@ extern "C" rg_status rg_grid_wprojection_noalloc(double *uvgrid, int grid_size, 
         return fail(RG_ERR_INVALID_ARGUMENT,
                     "rg_grid_wprojection_noalloc takes device pointers only (no staging memory)");
 
+    // an error left pending by the caller's earlier work is reported as such,
+    // not as a failure of the launches below
+    const cudaError_t pending = cudaGetLastError();
+    if (pending != cudaSuccess)
+        return cuda_fail(pending, "a CUDA error was already pending before rg_grid_wprojection_noalloc");
     unsigned char *base = nullptr;
     int sms = 148;
     RG_CHECK(scratch_for_current_device(&base, &sms));
@@ -145,9 +147,10 @@ extern "C" rg_status rg_grid_wprojection_noalloc(double *uvgrid, int grid_size, 
                              wkern->plane_count, wkern->w_min, wkern->w_step, rec, visf, err);
         launch_romein(st, rec, visf, cnt, taps32, grid32, slot, 0, N, K, sms);
     }
-    launch_add_f32_to_f64(st, grid32, (double2 *)uvgrid, cells, (flags & RG_GRID_OVERWRITE) ? 1 : 0);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "rg_grid_wprojection_noalloc launch");
+    // the error word is read before the caller's grid is touched: a rejected
+    // call leaves it as it was
     unsigned herr = 0;
     RG_CUDA(cudaMemcpyAsync(&herr, err, sizeof(herr), cudaMemcpyDeviceToHost, st));
     RG_CUDA(cudaStreamSynchronize(st));
@@ -156,5 +159,9 @@ extern "C" rg_status rg_grid_wprojection_noalloc(double *uvgrid, int grid_size, 
         return fail(RG_ERR_INVALID_ARGUMENT, "a visibility's w (or sub-cell index) falls outside the w-kernel table");
     if (herr & DERR_GRID_RANGE)
         return fail(RG_ERR_INVALID_ARGUMENT, "a visibility's kernel footprint lies outside the grid");
+    launch_add_f32_to_f64(st, grid32, (double2 *)uvgrid, cells, (flags & RG_GRID_OVERWRITE) ? 1 : 0);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "rg_grid_wprojection_noalloc launch");
+    RG_CUDA(cudaStreamSynchronize(st));
     return RG_OK;
 }

@@ -12,7 +12,8 @@ import numpy as np
 import pytest
 
 C_LIGHT = 299792458.0
-REF = os.environ.get("RG_REFERENCE_DIR", "/root/reference")
+# the reference checkout (its root directory), when the caller provides one
+REF = os.environ.get("RG_REFERENCE_ROOT")
 
 
 @pytest.fixture(scope="module")
@@ -110,9 +111,11 @@ def test_reads_libhdf5_written_files(rg, rel, shape):
     """Separable-kernel files written by libhdf5 (read by
     src/common/hdf5.c:372-500: dataset sepkern/kern, root attributes du, dw,
     x0)."""
+    if not REF:
+        pytest.skip("set RG_REFERENCE_ROOT to the reference checkout to read its libhdf5-written files")
     path = os.path.join(REF, rel)
     if not os.path.exists(path):
-        pytest.skip("reference tree not present")
+        pytest.skip(f"{rel} not found under RG_REFERENCE_ROOT")
     kern = rg.hdf5_read(path, "sepkern/kern")
     assert kern.shape == shape
     assert np.isfinite(kern).all() and np.abs(kern).max() > 0
