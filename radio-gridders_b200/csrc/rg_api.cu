@@ -525,9 +525,10 @@ static rg_status wtowers_enqueue(rg_context *ctx, const DevVis &dv, const float2
         char key[160];
         std::snprintf(key, sizeof(key), "phq_%d_%.17g_%.17g", S, theta, winc);
         bool fresh = ctx->scratch.find(key) == ctx->scratch.end();
-        RG_CHECK(scratch(ctx, key, sizeof(uint32_t) * (size_t)sub_cells, &ph));
+        // the fixed-point phase table, then exp(2 pi i ph) in FP32
+        RG_CHECK(scratch(ctx, key, (sizeof(uint32_t) + sizeof(float2)) * (size_t)sub_cells, &ph));
         if (fresh) {
-            launch_fresnel_table(st, (uint32_t *)ph, S, theta, winc);
+            launch_fresnel_table(st, (uint32_t *)ph, (float2 *)((uint32_t *)ph + sub_cells), S, theta, winc);
             ctx->launches++;
         }
     }
@@ -598,7 +599,7 @@ static rg_status wtowers_enqueue(rg_context *ctx, const DevVis &dv, const float2
     begin_stage(ctx, "tower_rows");
     launch_tower_rows(st, (float2 *)slots, (const unsigned *)masks, (const int *)bin_of_slot, (const int *)gbegin,
                       (const int *)gend, range, counts, pl.slots_cap, pl.groups_cap, (const uint32_t *)ph,
-                      (float2 *)partial, S, tw);
+                      (const float2 *)((const uint32_t *)ph + sub_cells), (float2 *)partial, S, tw);
     end_stage(ctx);
     begin_stage(ctx, "tower_finish");
     launch_tower_finish(st, pl.groups_cap, (const int *)tgfirst, (const int *)tgcount, ntowers,

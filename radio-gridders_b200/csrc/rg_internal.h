@@ -229,7 +229,9 @@ void launch_romein(cudaStream_t s, const int4 *rec, const float2 *visf, int64_t 
                    int points = 0, int strip_lg = 0);
 
 // k_towers.cu
-void launch_fresnel_table(cudaStream_t s, uint32_t *phq, int subgrid, double theta, double winc);
+// phq: the Fresnel phase as a 32-bit fraction of a turn; gtab (optional):
+// exp(2 pi i ph) rounded from FP64 to FP32.
+void launch_fresnel_table(cudaStream_t s, uint32_t *phq, float2 *gtab, int subgrid, double theta, double winc);
 // Sparse sub-grid transforms and the W-towers row stage.  Group g covers
 // active slots [group_begin[g], group_end[g]) of one tower; partial holds one
 // sub-grid per group; tower t's groups are [tower_group_first[t],
@@ -251,7 +253,7 @@ void launch_sparse_cols(cudaStream_t s, float2 *slots, const unsigned *masks, co
 void launch_tower_rows(cudaStream_t s, float2 *slots, const unsigned *masks, const int *bin_of_slot,
                        const int *group_begin, const int *group_end, const int *range,
                        const int *counts, int slot_cap, int group_cap, const uint32_t *phq,
-                       float2 *partial, int subgrid, const float2 *tw);
+                       const float2 *gtab, float2 *partial, int subgrid, const float2 *tw);
 // Per tower: the sum of its groups' partials (in group order) and the forward
 // row transform into subimg.  The forward column transform of subimg follows
 // (launch_fft32_cols).
