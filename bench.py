@@ -16,9 +16,11 @@ lambda 20480), 512-cell sub-grids with 16-cell margins, w-increment 10,
 SKA-Low-like 256 stations (32,640 baselines x 16 dumps x 4 channels =
 2,088,960 visibilities), 16 x 16 taps at 32x oversampling (11 w-planes,
 |dw| <= 5), which keeps the image within 1e-4 RMS of the FP64 DFT.  Synthetic, seeded.
-With --gpus N each rank grids its own 32-minute snapshot (hour angles offset
-by rank) and the FP64 master grids are summed onto rank 0 with one NCCL
-reduce: per-GPU work is fixed (weak scaling).
+With --gpus N the towers of the one observation are split over the ranks
+(rg_wtowers_tower_loads + rg_wtowers_partition: balanced by visibilities and
+active w-floors), each rank grids its share into its own FP64 master grid
+(rg_grid_wtowers_part) and one NCCL reduce sums the master grids onto rank 0:
+total work fixed (strong scaling).
 
 ``--impl reference`` times the reference's own CPU grid_wtowers
 (src/reference/grid.c, compiled from its sources into oracle/_ref with its
@@ -65,12 +67,19 @@ def parse():
     return p.parse_args()
 
 
-def workload(rank: int, stations: int = 256):
-    """Rank r observes the r-th consecutive 32-minute snapshot of the same field."""
+def workload(stations: int = 256):
+    """The observation every rank grids a share of (seeded)."""
     sim = importlib.import_module("radio-gridders_b200.simulate")
-    obs = sim.wtowers_plain(seed=1, n_st=stations, ha_offset_hours=rank * 32.0 / 60.0)
+    obs = sim.wtowers_plain(seed=1, n_st=stations)
     wk = sim.generate_wkernel(THETA, np.arange(-5, 6, 1.0), KSIZE, OVER)
     return obs, wk
+
+
+def tower_parts(vis_per_tower, floors_per_tower, world):
+    """Part (rank) of each tower: the library's deterministic balance of
+    visibilities and active w-floors, the same on every rank."""
+    rg = importlib.import_module("radio-gridders_b200")
+    return rg.partition_towers(vis_per_tower, floors_per_tower, world)
 
 
 def reduce_master(grid, world):
@@ -221,7 +230,7 @@ def run_reference(args, rank, world):
     if rank != 0:
         return 0
     import oracle
-    obs, wk = workload(0)
+    obs, wk = workload()
     cores = len(os.sched_getaffinity(0))
     if not oracle.reference_available(omp=True):
         kind = "port"
@@ -239,7 +248,7 @@ def run_reference(args, rank, world):
     value = nvis / per
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "vis/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
             "config": {"workload": "wtowers_plain", "grid_size": GRID, "theta": THETA,
                        "subgrid": SUBGRID, "margin": MARGIN, "winc": WINC},
@@ -303,7 +312,7 @@ def run_b200(args, rank, world, local_rank):
     rg = importlib.import_module("radio-gridders_b200")
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    obs, wk = workload(rank, args.stations)
+    obs, wk = workload(args.stations)
     u, v, w, vis = obs.flat()
     nvis = len(u)
 
@@ -321,9 +330,18 @@ def run_b200(args, rank, world, local_rank):
     V = rg.Visibilities(du, dv, dw, dvis)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
+    parts = None
+    if world > 1:  # this rank's towers (planning, outside the timed steps)
+        nv, nf = ctx.tower_loads(GRID, THETA, V, SUBGRID, MARGIN, WINC)
+        parts = tower_parts(nv, nf, world)
+
     def step():
-        ctx.grid_wtowers(grid, GRID, THETA, V, wk, SUBGRID, MARGIN, WINC,
-                         flags=rg.RG_GRID_OVERWRITE, wkern_data=dwk)
+        if parts is None:
+            ctx.grid_wtowers(grid, GRID, THETA, V, wk, SUBGRID, MARGIN, WINC,
+                             flags=rg.RG_GRID_OVERWRITE, wkern_data=dwk)
+        else:
+            ctx.grid_wtowers_part(grid, GRID, THETA, V, wk, SUBGRID, MARGIN, WINC, parts, rank,
+                                  flags=rg.RG_GRID_OVERWRITE, wkern_data=dwk)
         reduce_master(grid, world)
 
     for _ in range(max(args.warmup, 3)):
@@ -367,54 +385,83 @@ def run_b200(args, rank, world, local_rank):
     if world > 1:
         dist.all_reduce(total, op=dist.ReduceOp.MAX)
     ms_per_step = total.item() / args.steps
-    value = nvis * world / (ms_per_step * 1e-3)
+    value = nvis / (ms_per_step * 1e-3)  # one observation per step, over all ranks
 
     # end to end through the C ABI with pinned host buffers
-    hu = torch.from_numpy(u).pin_memory().numpy()
-    hv = torch.from_numpy(v).pin_memory().numpy()
-    hw = torch.from_numpy(w).pin_memory().numpy()
-    hvis = torch.from_numpy(vis).pin_memory().numpy()
+    hu = torch.from_numpy(u).pin_memory()
+    hv = torch.from_numpy(v).pin_memory()
+    hw = torch.from_numpy(w).pin_memory()
+    hvis = torch.from_numpy(vis).pin_memory()
     hwk = torch.from_numpy(np.ascontiguousarray(wk.data)).pin_memory().numpy()
-    hgrid = torch.zeros((GRID, GRID), dtype=torch.complex128).pin_memory().numpy()
-    HV = rg.Visibilities(hu, hv, hw, hvis)
-    for _ in range(2):
-        ctx.grid_wtowers(hgrid, GRID, THETA, HV, wk, SUBGRID, MARGIN, WINC,
-                         flags=rg.RG_GRID_OVERWRITE, wkern_data=hwk)
-    torch.cuda.synchronize()
-    # (a) one call per step
-    e2e_single = []
-    for _ in range(args.steps):
+    hgrid_t = torch.zeros((GRID, GRID), dtype=torch.complex128).pin_memory()
+    hgrid = hgrid_t.numpy()
+    if world == 1:
+        HV = rg.Visibilities(hu.numpy(), hv.numpy(), hw.numpy(), hvis.numpy())
+        for _ in range(2):
+            ctx.grid_wtowers(hgrid, GRID, THETA, HV, wk, SUBGRID, MARGIN, WINC,
+                             flags=rg.RG_GRID_OVERWRITE, wkern_data=hwk)
+        torch.cuda.synchronize()
+        # (a) one call per step
+        e2e_single = []
+        for _ in range(args.steps):
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            ctx.grid_wtowers(hgrid, GRID, THETA, HV, wk, SUBGRID, MARGIN, WINC,
+                             flags=rg.RG_GRID_OVERWRITE, wkern_data=hwk)
+            t1.record(stream)
+            t1.synchronize()
+            e2e_single.append(t0.elapsed_time(t1))
+        # (b) the steps as one batch call: each step's inputs copied in and grid
+        # copied out, overlapping the neighbouring steps' passes
+        hgrids = [hgrid] * args.steps
+        HVs = [HV] * args.steps
+        ctx.grid_wtowers_batch(hgrids[:2], GRID, THETA, HVs[:2], wk, SUBGRID, MARGIN, WINC,
+                               flags=rg.RG_GRID_OVERWRITE, wkern_data=hwk)
+        torch.cuda.synchronize()
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record(stream)
-        ctx.grid_wtowers(hgrid, GRID, THETA, HV, wk, SUBGRID, MARGIN, WINC,
-                         flags=rg.RG_GRID_OVERWRITE, wkern_data=hwk)
+        ctx.grid_wtowers_batch(hgrids, GRID, THETA, HVs, wk, SUBGRID, MARGIN, WINC,
+                               flags=rg.RG_GRID_OVERWRITE, wkern_data=hwk)
         t1.record(stream)
         t1.synchronize()
-        e2e_single.append(t0.elapsed_time(t1))
-    # (b) the steps as one batch call: each step's inputs copied in and grid
-    # copied out, overlapping the neighbouring steps' passes
-    hgrids = [hgrid] * args.steps
-    HVs = [HV] * args.steps
-    ctx.grid_wtowers_batch(hgrids[:2], GRID, THETA, HVs[:2], wk, SUBGRID, MARGIN, WINC,
-                           flags=rg.RG_GRID_OVERWRITE, wkern_data=hwk)
-    torch.cuda.synchronize()
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    t0.record(stream)
-    ctx.grid_wtowers_batch(hgrids, GRID, THETA, HVs, wk, SUBGRID, MARGIN, WINC,
-                           flags=rg.RG_GRID_OVERWRITE, wkern_data=hwk)
-    t1.record(stream)
-    t1.synchronize()
-    e2e_ms = [t0.elapsed_time(t1) / args.steps]
+        e2e_ms = [t0.elapsed_time(t1) / args.steps]
+        e2e_call = f"rg_grid_wtowers_batch over {args.steps} steps (pinned host buffers)"
+        h2d = 8 * 3 * nvis + 16 * nvis + 16 * wk.data.size / args.steps
+    else:
+        # per step: every rank copies the observation in from pinned host
+        # memory, grids its towers, the master grids are reduced onto rank 0,
+        # which copies the grid out
+        def e2e_step():
+            for dst, src in ((du, hu), (dv, hv), (dw, hw), (dvis, hvis)):
+                dst.copy_(src, non_blocking=True)
+            step()
+            if rank == 0:
+                hgrid_t.copy_(grid, non_blocking=True)
+
+        for _ in range(2):
+            e2e_step()
+        torch.cuda.synchronize()
+        dist.barrier()
+        e2e_ms = []
+        for _ in range(args.steps):
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            e2e_step()
+            t1.record(stream)
+            t1.synchronize()
+            e2e_ms.append(t0.elapsed_time(t1))
+        e2e_single = e2e_ms
+        e2e_call = "per step: H2D of the observation on every rank, rg_grid_wtowers_part, NCCL reduce, D2H on rank 0"
+        h2d = world * (8 * 3 * nvis + 16 * nvis)
     e2e_t = torch.tensor([sum(e2e_ms) / len(e2e_ms)], dtype=torch.float64, device=dev)
     single_t = torch.tensor([sum(e2e_single) / len(e2e_single)], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
         dist.all_reduce(single_t, op=dist.ReduceOp.MAX)
-    e2e_value = nvis * world / (e2e_t.item() * 1e-3)
-    # the kernel table crosses once per batch call; visibilities and grid every step
-    h2d = 8 * 3 * nvis + 16 * nvis + 16 * wk.data.size / args.steps
+    e2e_value = nvis / (e2e_t.item() * 1e-3)
     d2h = 16 * GRID * GRID
 
     if rank != 0:
@@ -447,7 +494,7 @@ def run_b200(args, rank, world, local_rank):
     line = {
         "impl": "b200", "metric": METRIC, "value": value, "unit": "vis/s", "n_gpus": world,
         "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded Earth-rotation synthesis, power-law point sources)",
         "config": {"workload": "wtowers_plain: 2048x2048 grid (theta 0.1, lambda 20480), subgrid 512, "
                                f"margin 16, winc 10, {nvis:,} vis ({args.stations} stations, 16 dumps x 4 ch), "
@@ -455,7 +502,8 @@ def run_b200(args, rank, world, local_rank):
                    "grid_size": GRID, "subgrid": SUBGRID, "margin": MARGIN, "winc": WINC,
                    "vis_per_gpu": nvis, "active_subgrids": stats["active_subgrids"],
                    "towers_with_data": stats["towers_with_data"], "floors": stats["floors"],
-                   "parallelism": f"{world} rank(s), one snapshot each, master grids reduced over NCCL",
+                   "parallelism": (f"{world} ranks, the observation's towers split by load, FP64 master grids "
+                                   "reduced over NCCL") if world > 1 else "1 GPU",
                    "l2": "256 MiB buffer written between steps, outside each step's event pair",
                    "precision": "FP32 sub-grids and transforms; FP64 coordinates, Fresnel phase and master grid",
                    "schedule": {"romein_points_per_thread": stats["romein_points"],
@@ -480,9 +528,9 @@ def run_b200(args, rank, world, local_rank):
         "stage_ms": {k: round(statistics.mean(v), 4) for k, v in stage_ms.items()},
         "e2e": {"value": e2e_value, "unit": "vis/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_t.item(),
-                "call": f"rg_grid_wtowers_batch over {args.steps} steps (pinned host buffers)",
+                "call": e2e_call,
                 "single_call_ms_per_step": single_t.item(),
-                "single_call_vis_per_s": nvis * world / (single_t.item() * 1e-3)},
+                "single_call_vis_per_s": nvis / (single_t.item() * 1e-3)},
         "gpu_launches": int(launches),
         "clocks": clk,
     }

@@ -163,6 +163,39 @@ rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double
                           const rg_vis *vis, const rg_wkern *wkern, int subgrid_size,
                           int subgrid_margin, double wincrement, int flags);
 
+/* ---- one observation's towers over several GPUs ------------------------
+ * No counterpart in the reference, which grids every tower on one device
+ * (src/grid/grid.cpp:161-165, src/grid/grid_cuda.cu:644-655); its work unit
+ * is the tower (src/reference/grid.c:413-416).  Towers are independent until
+ * the add-back, so rank r of R grids the towers of part r into its own FP64
+ * master grid (rg_grid_wtowers_part) and one sum of the R master grids (an
+ * NCCL reduce or reduce-scatter) gives rg_grid_wtowers' grid, up to the order
+ * of the FP64 additions of overlapping towers.  Every rank needs the
+ * visibilities of its own towers only; a rank given all of them skips the
+ * others' after binning. */
+
+/* Towers of a W-towers shape: (grid_size / (subgrid - margin) + 1)^2, ordered
+ * row-major (cy * n + cx). */
+int rg_wtowers_tower_count(int grid_size, int subgrid_size, int subgrid_margin);
+/* Load of each tower: visibilities (vis_per_tower) and active w-floors
+ * (floors_per_tower) under the gridder's binning cuts.  ntowers must equal
+ * rg_wtowers_tower_count. */
+rg_status rg_wtowers_tower_loads(rg_context *ctx, int grid_size, double theta, const rg_vis *vis,
+                                 int subgrid_size, int subgrid_margin, double wincrement, int64_t *vis_per_tower,
+                                 int32_t *floors_per_tower, int ntowers);
+/* Host only: towers into nparts parts balanced by vis + vis_per_floor *
+ * floors (0: the default 2400, the measured cost ratio of a sub-grid's
+ * transforms to one visibility's gridding on B200), largest first to the
+ * least loaded part.  Deterministic: every rank computes the same parts. */
+rg_status rg_wtowers_partition(const int64_t *vis_per_tower, const int32_t *floors_per_tower, int ntowers,
+                               int nparts, double vis_per_floor, int32_t *part_of_tower);
+/* rg_grid_wtowers restricted to the towers t with part_of_tower[t] == part;
+ * other towers' visibilities are skipped (last_stats counts only this
+ * part's gridded visibilities). */
+rg_status rg_grid_wtowers_part(rg_context *ctx, double *uvgrid, int grid_size, double theta, const rg_vis *vis,
+                               const rg_wkern *wkern, int subgrid_size, int subgrid_margin, double wincrement,
+                               int flags, const int32_t *part_of_tower, int part);
+
 /* count observations of one shape (same visibility count) with one kernel
  * table: the same result as count rg_grid_wtowers calls in order (grid i from
  * vis[i] into uvgrids[i]), with the host-to-device copies of later
@@ -296,6 +329,27 @@ rg_status rg_write_vis_flat_hdf5(const char *path, int n_rows, int n_freq, const
 rg_status rg_hdf5_read_f64(const char *path, const char *dataset, double *out, int64_t capacity,
                            int64_t *dims, int *ndims);
 rg_status rg_hdf5_attr_f64(const char *path, const char *object, const char *name, double *out);
+
+/* ---- w-kernel generator --------------------------------------------------- */
+
+/* An oversampled w-kernel table (rg_wkern layout: plane_count * ov * ov * size
+ * * size complex float64, interleaved) for the given w planes:
+ *   tap[plane][yf][xf][ty][tx] = K_w(tx - size/2 - xf/ov, ty - size/2 - yf/ov),
+ *   K_w(p, q) = 1/M^2 sum_ij A(l_i) A(m_j) exp(2 pi i w (1 - n_ij))
+ *               exp(-2 pi i (p l_i + q m_j) / theta),
+ * on an M x M screen (screen_pixels; <= 0: 128), l_i = theta (i - M/2) / M,
+ * A(l) = psi_0(c, 2 l / theta) (c <= 0: pi (size - 2) / 2).  The reference
+ * has no generator (its kernels come from the crocodile scripts as files,
+ * README.md:25-26, loaded by src/common/hdf5.c:1362-1509); this produces the
+ * tables its load_wkern would return (src/reference/hdf5.c:321-413), for
+ * rg_grid_* or rg_write_wkern_hdf5.  data_out: host or device pointer.  FP64
+ * throughout; the screen and the sums run on the device. */
+rg_status rg_wkern_generate(rg_context *ctx, double theta, const double *w_planes, int plane_count, int size,
+                            int oversampling, double c, int screen_pixels, double *data_out);
+/* Host only: the zeroth prolate spheroidal wave function psi_0(c, x),
+ * normalised to psi_0(c, 0) = 1, at n points x in [-1, 1] (the generator's
+ * taper and the image-plane grid correction). */
+rg_status rg_pswf0(double c, const double *x, int64_t n, double *out);
 
 /* ---- learned w-kernel ---------------------------------------------------- */
 

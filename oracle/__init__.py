@@ -70,7 +70,8 @@ def lib():
         i64, vp, d, i = ct.c_int64, ct.c_void_p, ct.c_double, ct.c_int
         L.rgo_grid_wprojection.argtypes = [vp, i, d, i64, vp, vp, vp, vp, ct.POINTER(_Wk)]
         L.rgo_grid_wprojection.restype = ct.c_uint64
-        L.rgo_grid_wtowers.argtypes = [vp, i, d, i64, vp, vp, vp, vp, ct.POINTER(_Wk), i, i, d, vp]
+        L.rgo_grid_wtowers.argtypes = [vp, i, d, i64, vp, vp, vp, vp, ct.POINTER(_Wk), i, i, d, vp, vp]
+        L.rgo_wtowers_census.argtypes = [i, d, i64, vp, vp, vp, i, i, d, vp, vp]
         L.rgo_grid_wtowers.restype = ct.c_uint64
         L.rgo_weight.argtypes = [i, d, i64, vp, vp, vp]
         L.rgo_make_hermitian.argtypes = [vp, i]
@@ -104,15 +105,29 @@ def grid_wprojection(grid_size, theta, u, v, w, vis, wk):
 
 
 def grid_wtowers(grid_size, theta, u, v, w, vis, wk, subgrid, margin, winc,
-                 return_counts=False):
+                 return_counts=False, towers=None):
+    """towers: optional boolean array over the towers (row-major): grid only
+    those (one share of a tower-partitioned observation)."""
     u, v, w, vis = _flat(u, v, w, vis)
     grid = np.zeros((grid_size, grid_size), np.complex128)
     s, keep = _wk_struct(wk)
     counts = np.zeros(len(u), np.int32)
+    sel = None if towers is None else np.ascontiguousarray(towers, np.uint8)
     lib().rgo_grid_wtowers(_ptr(grid), grid_size, theta, len(u), _ptr(u), _ptr(v),
                            _ptr(w), _ptr(vis), ct.byref(s), subgrid, margin, winc,
-                           _ptr(counts))
+                           _ptr(counts), None if sel is None else _ptr(sel))
     return (grid, counts) if return_counts else grid
+
+
+def wtowers_census(grid_size, theta, u, v, w, subgrid, margin, winc):
+    """(visibilities per tower int64, active w-floors per tower int32)."""
+    u, v, w, _ = _flat(u, v, w, np.zeros(0))
+    nc = grid_size // (subgrid - margin) + 1
+    nv = np.zeros(nc * nc, np.int64)
+    nf = np.zeros(nc * nc, np.int32)
+    lib().rgo_wtowers_census(grid_size, theta, len(u), _ptr(u), _ptr(v), _ptr(w), subgrid, margin, winc,
+                             _ptr(nv), _ptr(nf))
+    return nv, nf
 
 
 def weight(grid_size, theta, u, v, vis):

@@ -107,7 +107,8 @@ uint64_t rgo_grid_wtowers(double complex *uvgrid, int grid_size, double theta,
                           int64_t nvis, const double *u, const double *v,
                           const double *w, const double complex *vis,
                           const rgo_wkern *wk, int subgrid_size, int subgrid_margin,
-                          double wincrement, int32_t *gridded_count)
+                          double wincrement, int32_t *gridded_count,
+                          const unsigned char *tower_sel)
 {
     const int S = subgrid_size, M = subgrid_margin;
     assert(M >= wk->size);
@@ -200,6 +201,7 @@ uint64_t rgo_grid_wtowers(double complex *uvgrid, int grid_size, double theta,
     double complex *subimg = (double complex *)calloc((size_t)S * S, sizeof(double complex));
 #pragma omp for schedule(dynamic, 1)
     for (int c = 0; c < ntowers; c++) {
+        if (tower_sel && !tower_sel[c]) continue; /* another share's tower */
         int cx = c % nchunk, cy = c / nchunk;
         int x_min, y_min;
         double ulo, uhi, umid, vlo, vhi, vmid;
@@ -270,6 +272,56 @@ uint64_t rgo_grid_wtowers(double complex *uvgrid, int grid_size, double theta,
     free(finished); free(order); free(start);
     free(pair_bin); free(pair_vis); free(wtransfer);
     return flops;
+}
+
+/* Tower loads under the binning cuts of rgo_grid_wtowers (grid.c:357-367,
+ * 425-458, 244-254): visibilities per tower and w-floors with data per tower
+ * (towers row-major, cy * nchunk + cx). */
+void rgo_wtowers_census(int grid_size, double theta, int64_t nvis, const double *u, const double *v,
+                        const double *w, int subgrid_size, int subgrid_margin, double wincrement,
+                        int64_t *vis_per_tower, int32_t *floors_per_tower)
+{
+    const int chunk = subgrid_size - subgrid_margin;
+    const int nchunk = grid_size / chunk + 1;
+    double wlo = 0, whi = 0;
+    for (int64_t i = 0; i < nvis; i++) {
+        if (w[i] < wlo) wlo = w[i];
+        if (w[i] > whi) whi = w[i];
+    }
+    const int wp_min = (int)floor(wlo / wincrement + 0.5);
+    const int wp_max = (int)floor(whi / wincrement + 0.5);
+    const int nfloor = wp_max - wp_min + 1;
+    unsigned char *active = (unsigned char *)calloc((size_t)nchunk * nchunk * nfloor, 1);
+    memset(vis_per_tower, 0, sizeof(int64_t) * (size_t)nchunk * nchunk);
+    for (int64_t i = 0; i < nvis; i++) {
+        int cxc = (int)floor((u[i] * theta + 0.5 + grid_size / 2) / chunk);
+        int cyc = (int)floor((v[i] * theta + 0.5 + grid_size / 2) / chunk);
+        int wpc = (int)floor(w[i] / wincrement + 0.5);
+        for (int cy = cyc - 1; cy <= cyc + 1; cy++) {
+            if (cy < 0 || cy >= nchunk) continue;
+            int y_min; double vlo, vhi, vmid;
+            tower_bounds(cy, chunk, grid_size, theta, &y_min, &vlo, &vhi, &vmid);
+            if (v[i] < vlo || v[i] >= vhi) continue;
+            for (int cx = cxc - 1; cx <= cxc + 1; cx++) {
+                if (cx < 0 || cx >= nchunk) continue;
+                int x_min; double ulo, uhi, umid;
+                tower_bounds(cx, chunk, grid_size, theta, &x_min, &ulo, &uhi, &umid);
+                if (u[i] < ulo || u[i] >= uhi) continue;
+                for (int wp = wpc - 1; wp <= wpc + 1; wp++) {
+                    if (wp < wp_min || wp > wp_max) continue;
+                    if (w[i] < ((double)wp - 0.5) * wincrement || w[i] >= ((double)wp + 0.5) * wincrement) continue;
+                    vis_per_tower[cy * nchunk + cx]++;
+                    active[((size_t)cy * nchunk + cx) * nfloor + (wp - wp_min)] = 1;
+                }
+            }
+        }
+    }
+    for (int t = 0; t < nchunk * nchunk; t++) {
+        int c = 0;
+        for (int f = 0; f < nfloor; f++) c += active[(size_t)t * nfloor + f];
+        floors_per_tower[t] = c;
+    }
+    free(active);
 }
 
 /* grid.c:27-35 */

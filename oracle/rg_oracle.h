@@ -51,12 +51,19 @@ uint64_t rgo_grid_wprojection(double complex *uvgrid, int grid_size, double thet
 
 /* grid.c:295-555 (serial build, i.e. without OMP_TOWERS).  If gridded_count is
  * non-NULL it receives, per visibility, how many times it was gridded (the
- * reference checks this is exactly once, grid.c:519-530).  Returns flops. */
+ * reference checks this is exactly once, grid.c:519-530).  If tower_sel is
+ * non-NULL, only the towers t (row-major) with tower_sel[t] != 0 are gridded.
+ * Returns flops. */
 uint64_t rgo_grid_wtowers(double complex *uvgrid, int grid_size, double theta,
                           int64_t nvis, const double *u, const double *v,
                           const double *w, const double complex *vis,
                           const rgo_wkern *wk, int subgrid_size, int subgrid_margin,
-                          double wincrement, int32_t *gridded_count);
+                          double wincrement, int32_t *gridded_count,
+                          const unsigned char *tower_sel);
+/* Visibilities and active w-floors per tower under the same binning. */
+void rgo_wtowers_census(int grid_size, double theta, int64_t nvis, const double *u, const double *v,
+                        const double *w, int subgrid_size, int subgrid_margin, double wincrement,
+                        int64_t *vis_per_tower, int32_t *floors_per_tower);
 
 /* grid.c:59-81: uniform weighting, vis[i] /= count of visibilities in its cell. */
 void rgo_weight(int grid_size, double theta, int64_t nvis, const double *u,

@@ -45,7 +45,8 @@ EXPORTS = [
     "rg_grid_wprojection_learned", "rg_grid_wtowers_learned", "rg_grid_wtowers_batch", "rg_read_vis_hdf5", "rg_free_vis_data", "rg_read_wkern_hdf5",
     "rg_free_wkern_data", "rg_write_vis_hdf5", "rg_write_vis_flat_hdf5", "rg_write_wkern_hdf5", "rg_hdf5_read_f64",
     "rg_hdf5_attr_f64", "rg_selftest_wait_timeout", "rg_wtowers_cuda_flat", "rg_wproj_cuda_flat",
-    "rg_image_dft_host_flat",
+    "rg_image_dft_host_flat", "rg_wtowers_tower_count", "rg_wtowers_tower_loads", "rg_wtowers_partition",
+    "rg_grid_wtowers_part", "rg_wkern_generate", "rg_pswf0",
 ]
 
 
@@ -105,6 +106,13 @@ def lib():
         L.rg_last_timings.restype = i
         L.rg_grid_wprojection.argtypes = [vp, vp, i, d, ct.POINTER(_Vis), ct.POINTER(_WKern), i]
         L.rg_grid_wtowers.argtypes = [vp, vp, i, d, ct.POINTER(_Vis), ct.POINTER(_WKern), i, i, d, i]
+        L.rg_wtowers_tower_count.argtypes = [i, i, i]
+        L.rg_wtowers_tower_count.restype = i
+        L.rg_wtowers_tower_loads.argtypes = [vp, i, d, ct.POINTER(_Vis), i, i, d, vp, vp, i]
+        L.rg_wtowers_partition.argtypes = [vp, vp, i, i, d, vp]
+        L.rg_grid_wtowers_part.argtypes = [vp, vp, i, d, ct.POINTER(_Vis), ct.POINTER(_WKern), i, i, d, i, vp, i]
+        L.rg_wkern_generate.argtypes = [vp, d, vp, i, i, i, d, i, vp]
+        L.rg_pswf0.argtypes = [d, vp, i64, vp]
         L.rg_grid_wtowers_batch.argtypes = [vp, i, ct.POINTER(vp), i, d, ct.POINTER(_Vis), ct.POINTER(_WKern),
                                             i, i, d, i]
         L.rg_weight.argtypes = [vp, i, d, ct.POINTER(_Vis), vp]
@@ -270,6 +278,40 @@ class Context:
                                      int(subgrid_margin), float(wincrement), int(flags)))
         return uvgrid
 
+    def wkern_generate(self, theta, w_planes, size=16, oversampling=8, c=0.0, screen_pixels=128, out=None):
+        """rg_wkern_generate: complex128 [planes, ov, ov, size, size] table
+        (a numpy array, or `out`, which may be a device tensor)."""
+        wp = np.ascontiguousarray(w_planes, np.float64)
+        if out is None:
+            out = np.empty((wp.size, oversampling, oversampling, size, size), np.complex128)
+        _check(lib().rg_wkern_generate(self._h, float(theta), _ptr(wp), int(wp.size), int(size), int(oversampling),
+                                       float(c), int(screen_pixels), _ptr(out)))
+        return out
+
+    # ---- one observation's towers over several GPUs ----
+    def tower_loads(self, grid_size, theta, vis: Visibilities, subgrid_size, subgrid_margin, wincrement):
+        """rg_wtowers_tower_loads: (visibilities, active w-floors) per tower."""
+        nt = tower_count(grid_size, subgrid_size, subgrid_margin)
+        nv = np.zeros(nt, np.int64)
+        nf = np.zeros(nt, np.int32)
+        vs = vis.struct()
+        _check(lib().rg_wtowers_tower_loads(self._h, int(grid_size), float(theta), ct.byref(vs), int(subgrid_size),
+                                            int(subgrid_margin), float(wincrement), _ptr(nv), _ptr(nf), nt))
+        return nv, nf
+
+    def grid_wtowers_part(self, uvgrid, grid_size, theta, vis: Visibilities, wkern, subgrid_size, subgrid_margin,
+                          wincrement, part_of_tower, part, flags=RG_GRID_ACCUMULATE, wkern_data=None):
+        """rg_grid_wtowers_part: the towers t with part_of_tower[t] == part."""
+        s, keep = _wkern_struct(wkern, wkern_data)
+        vs = vis.struct()
+        pt = np.ascontiguousarray(part_of_tower, np.int32)
+        if pt.size != tower_count(grid_size, subgrid_size, subgrid_margin):
+            raise ValueError("part_of_tower needs one entry per tower")
+        _check(lib().rg_grid_wtowers_part(self._h, _ptr(uvgrid), int(grid_size), float(theta), ct.byref(vs),
+                                          ct.byref(s), int(subgrid_size), int(subgrid_margin), float(wincrement),
+                                          int(flags), _ptr(pt), int(part)))
+        return uvgrid
+
     def grid_wtowers_batch(self, uvgrids, grid_size, theta, vis_list, wkern, subgrid_size, subgrid_margin,
                            wincrement, flags=RG_GRID_ACCUMULATE, wkern_data=None):
         """rg_grid_wtowers_batch: one grid per Visibilities of vis_list, with
@@ -427,6 +469,30 @@ def grid_wprojection(uvgrid, grid_size, theta, vis, wkern):
 def grid_wtowers(uvgrid, grid_size, theta, vis, wkern, subgrid_size, subgrid_margin, wincrement):
     return default_context().grid_wtowers(uvgrid, grid_size, theta, vis, wkern, subgrid_size,
                                           subgrid_margin, wincrement)
+
+
+def pswf0(c, x):
+    """rg_pswf0 (host only): psi_0(c, x) / psi_0(c, 0) for x in [-1, 1]."""
+    xa = np.ascontiguousarray(x, np.float64)
+    out = np.empty_like(xa)
+    _check(lib().rg_pswf0(float(c), _ptr(xa), int(xa.size), _ptr(out)))
+    return out
+
+
+def tower_count(grid_size, subgrid_size, subgrid_margin):
+    """rg_wtowers_tower_count: towers of a W-towers shape (row-major)."""
+    return int(lib().rg_wtowers_tower_count(int(grid_size), int(subgrid_size), int(subgrid_margin)))
+
+
+def partition_towers(vis_per_tower, floors_per_tower, nparts, vis_per_floor=0.0):
+    """rg_wtowers_partition (host only): part index per tower, balanced by
+    visibilities + vis_per_floor * active floors, largest first."""
+    nv = np.ascontiguousarray(vis_per_tower, np.int64)
+    nf = np.ascontiguousarray(floors_per_tower, np.int32)
+    out = np.zeros(nv.size, np.int32)
+    _check(lib().rg_wtowers_partition(_ptr(nv), _ptr(nf), int(nv.size), int(nparts), float(vis_per_floor),
+                                      _ptr(out)))
+    return out
 
 
 def weight(grid_size, theta, vis):

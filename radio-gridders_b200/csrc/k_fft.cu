@@ -9,8 +9,9 @@
 // src/reference/grid.c:467-499 with the per-floor row transforms done by the
 // row kernel beforehand.
 //
-// FP64 (image formation, power-of-two n <= 4096): radix-2 Stockham rows in
-// shared memory plus tiled transposes; not on the timed path.
+// FP64 (image formation, any n <= 4096): radix-2 Stockham rows in shared
+// memory for powers of two, Bluestein's algorithm (k_bluestein.cu) for other
+// lengths, plus tiled transposes; not on the timed path.
 #include <cmath>
 #include <vector>
 
@@ -325,17 +326,13 @@ __global__ void __launch_bounds__(kSparseColThreads) sparse_cols_kernel(
 //
 // tower_rows_kernel: CTA = (floor group, strip of R rows).  For each floor of
 // the group: backward row transform of the column-transformed sub-grid (only
-// the slot's marked strips are read, then zeroed), and the floor's image is
-// folded into the group's sum by the reference's own recurrence (grid.c:
-// 473-483): subimg = wtransfer^(wp - last_wp) * subimg + image, with
-// wtransfer = exp(2 pi i ph), ph = winc (1 - sqrt(1 - l^2 - m^2)) (grid.c:
-// 304-319) — one complex multiply-add per element and floor with the FP32
-// table of exp(2 pi i ph) (FP64-evaluated) for the usual one-floor step; a
-// step over skipped floors forms exp(2 pi i (wp - last_wp) ph) from the
-// 32-bit fixed-point phase table (integer product modulo one turn).  At the
-// end of the group the sum is taken to w = 0, times exp(-2 pi i wp_last ph)
-// (grid.c:490-496, the w = 0 transfer), and written to the group's partial
-// buffer.
+// the slot's marked strips are read, then zeroed), times exp(-2 pi i wp
+// ph(l, m)) with ph = winc (1 - sqrt(1 - l^2 - m^2)) — the reference's
+// wtransfer^(-wp), grid.c:304-319 and :473-496, which also covers the w = 0
+// transfer — accumulated in registers; the strip sum goes to the group's
+// partial buffer.  The phase -wp * ph is formed modulo one turn as an integer
+// product with the 32-bit fixed-point table (fresnel_table_kernel); sin/cos of
+// its top 24 bits in FP32.
 //
 // tower_rows_finish_kernel: CTA = (tower, strip of R rows).  Sums the tower's
 // group partials in group order (deterministic) and applies the forward row
@@ -404,32 +401,19 @@ __device__ __forceinline__ void ld_if(float2 &a, const float2 *p, bool on)
         : "memory");
 }
 
-// exp(2 pi i t / 2^32) for a 32-bit fraction of a turn t: the signed fraction
-// rounded to its top 24 bits (|k| <= 2^22, converted exactly by the 1.5 * 2^23
-// magic number), then sincospif — FP32-accurate, used once per group and for
-// steps over skipped floors, not in the per-floor recurrence.
-__device__ __forceinline__ float2 turn_phasor(uint32_t t)
-{
-    const int k = (int)(t + 256u) >> 9;
-    const float half_turns = (__int_as_float(0x4B400000 + k) - 12582912.f) * (1.f / 4194304.f);  // 2 t / 2^32
-    float sn, cs;
-    sincospif(half_turns, &sn, &cs);
-    return make_float2(cs, sn);
-}
-
 template <int N1>
 __global__ void __launch_bounds__(kRowThreads) tower_rows_kernel(
     float2 *__restrict__ slots, const unsigned *__restrict__ masks, const int *__restrict__ bin_of_slot,
     const int *__restrict__ group_begin, const int *__restrict__ group_end, const int *__restrict__ range,
-    const int *__restrict__ counts, int slot_cap, const uint32_t *__restrict__ phq,
-    const float2 *__restrict__ gtab, float2 *__restrict__ partial, const float2 *__restrict__ tw)
+    const int *__restrict__ counts, int slot_cap, const uint32_t *__restrict__ phq, float2 *__restrict__ partial,
+    const float2 *__restrict__ tw)
 {
     using G = RowGeom<N1>;
     constexpr int N = G::N, R = G::R;
     extern __shared__ float2 smem[];
-    float2 *T = smem;                 // [R][N1][kPad]
-    float2 *W = smem + G::T_ELEMS;    // [N]
-    float2 *F = W + N;                // [R][N] exp(2 pi i ph) of the strip's rows
+    float2 *T = smem;                                // [R][N1][kPad]
+    float2 *W = smem + G::T_ELEMS;                   // [N]
+    uint32_t *P = reinterpret_cast<uint32_t *>(W + N);  // [R][N] Fresnel phase of the strip (turns, 2^-32)
     __shared__ unsigned smask[G::WORDS];
     const int rstrips = N / R;
     const int group = blockIdx.x / rstrips, row0 = (blockIdx.x % rstrips) * R;
@@ -438,7 +422,7 @@ __global__ void __launch_bounds__(kRowThreads) tower_rows_kernel(
     const int begin = group_begin[group];
     const int end = group_end[group] < slot_cap ? group_end[group] : slot_cap;
     load_twiddles<N1>(W, tw);
-    for (int e = threadIdx.x; e < R * N; e += blockDim.x) F[e] = gtab[(int64_t)row0 * N + e];
+    for (int e = threadIdx.x; e < R * N; e += blockDim.x) P[e] = phq[(int64_t)row0 * N + e];
 
     float2 acc[G::PER][N1];
 #pragma unroll
@@ -446,12 +430,8 @@ __global__ void __launch_bounds__(kRowThreads) tower_rows_kernel(
 #pragma unroll
         for (int j = 0; j < N1; j++) acc[q][j] = make_float2(0.f, 0.f);
 
-    // the first floor's step multiplies the zero sum: any step will do
-    int last_wp = begin < end ? wp_min + bin_of_slot[begin] % nfloor - 1 : 0;
     for (int slot = begin; slot < end; slot++) {
-        const int wp = wp_min + bin_of_slot[slot] % nfloor;
-        const uint32_t dwp = (uint32_t)(wp - last_wp);  // >= 1: slots ascend in floor
-        last_wp = wp;
+        const uint32_t mwp = (uint32_t)(-(wp_min + bin_of_slot[slot] % nfloor));  // two's complement
         if (threadIdx.x < G::WORDS) smask[threadIdx.x] = masks[(int64_t)slot * G::WORDS + threadIdx.x];
         __syncthreads();  // masks visible; the previous floor's step 2 is done with T
         // the slot's strip mask in two 64-bit registers (at most 128 strips)
@@ -501,30 +481,23 @@ __global__ void __launch_bounds__(kRowThreads) tower_rows_kernel(
 #pragma unroll
                 for (int n1 = 0; n1 < N1; n1++) b[n1] = T[(r * N1 + n1) * kPad + k2];
                 reg_fft<N1, +1>(b);
-                if (dwp == 1u) {  // uniform: the next floor
 #pragma unroll
-                    for (int j = 0; j < N1; j++) {
-                        const int col = k2 + 32 * bitrevc(j, G::LB);
-                        const float2 g = F[r * N + col];
-                        const float2 h = acc[q][j];
-                        acc[q][j].x = fmaf(h.x, g.x, fmaf(-h.y, g.y, b[j].x));
-                        acc[q][j].y = fmaf(h.x, g.y, fmaf(h.y, g.x, b[j].y));
-                    }
-                } else {  // floors skipped: exp(2 pi i dwp ph), exact product modulo one turn
-#pragma unroll
-                    for (int j = 0; j < N1; j++) {
-                        const int col = k2 + 32 * bitrevc(j, G::LB);
-                        const float2 g = turn_phasor(dwp * __ldg(phq + (int64_t)(row0 + r) * N + col));
-                        const float2 h = acc[q][j];
-                        acc[q][j].x = fmaf(h.x, g.x, fmaf(-h.y, g.y, b[j].x));
-                        acc[q][j].y = fmaf(h.x, g.y, fmaf(h.y, g.x, b[j].y));
-                    }
+                for (int j = 0; j < N1; j++) {
+                    const int col = k2 + 32 * bitrevc(j, G::LB);
+                    // -wp ph modulo one turn as a signed 32-bit fraction, rounded to
+                    // its top 24 bits (k, |k| <= 2^22), converted exactly by the
+                    // 1.5 * 2^23 magic number
+                    const int k = (int)(mwp * P[r * N + col] + 256u) >> 9;
+                    const float turns = __int_as_float(0x4B400000 + k) - 12582912.f;
+                    float sn, cs;
+                    __sincosf(turns * (6.28318530717958647f / 8388608.f), &sn, &cs);
+                    // acc += b * (cs + i sn), two fused multiply-adds per component
+                    acc[q][j].x = fmaf(b[j].x, cs, fmaf(-b[j].y, sn, acc[q][j].x));
+                    acc[q][j].y = fmaf(b[j].x, sn, fmaf(b[j].y, cs, acc[q][j].y));
                 }
             }
         }
     }
-    // to w = 0: times exp(-2 pi i wp_last ph)
-    const uint32_t mwp = (uint32_t)(-last_wp);  // two's complement
     float2 *out = partial + ((int64_t)group * N + row0) * N;
 #pragma unroll
     for (int q = 0; q < G::PER; q++) {
@@ -532,12 +505,7 @@ __global__ void __launch_bounds__(kRowThreads) tower_rows_kernel(
         if (it < G::ITEMS2) {
             const int k2 = it % 32, r = it / 32;
 #pragma unroll
-            for (int j = 0; j < N1; j++) {
-                const int col = k2 + 32 * bitrevc(j, G::LB);
-                const float2 g = turn_phasor(mwp * __ldg(phq + (int64_t)(row0 + r) * N + col));
-                const float2 h = acc[q][j];
-                out[(int64_t)r * N + col] = make_float2(fmaf(h.x, g.x, -h.y * g.y), fmaf(h.x, g.y, h.y * g.x));
-            }
+            for (int j = 0; j < N1; j++) out[(int64_t)r * N + k2 + 32 * bitrevc(j, G::LB)] = acc[q][j];
         }
     }
 }
@@ -603,7 +571,7 @@ static size_t sparse_cols_smem() { return sizeof(float2) * (StripGeom<N1>::T_ELE
 template <int N1>
 static size_t tower_rows_smem()
 {
-    return sizeof(float2) * (RowGeom<N1>::T_ELEMS + N1 * 32 + RowGeom<N1>::R * N1 * 32);
+    return sizeof(float2) * (RowGeom<N1>::T_ELEMS + N1 * 32) + sizeof(uint32_t) * RowGeom<N1>::R * N1 * 32;
 }
 template <int N1>
 static size_t tower_finish_smem() { return sizeof(float2) * (RowGeom<N1>::T_ELEMS + N1 * 32); }
@@ -654,15 +622,14 @@ static void sparse_cols_impl(cudaStream_t s, float2 *slots, const unsigned *mask
 template <int N1>
 static void tower_rows_impl(cudaStream_t s, float2 *slots, const unsigned *masks, const int *bin_of_slot,
                             const int *group_begin, const int *group_end, const int *range, const int *counts,
-                            int slot_cap, int group_cap, const uint32_t *ph, const float2 *gtab, float2 *partial,
-                            const float2 *tw)
+                            int slot_cap, int group_cap, const uint32_t *ph, float2 *partial, const float2 *tw)
 {
     const int rstrips = RowGeom<N1>::N / RowGeom<N1>::R;
     const size_t sm1 = tower_rows_smem<N1>();
     cudaFuncSetAttribute(tower_rows_kernel<N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
     if (group_cap > 0)
         tower_rows_kernel<N1><<<(unsigned)group_cap * rstrips, kRowThreads, sm1, s>>>(
-            slots, masks, bin_of_slot, group_begin, group_end, range, counts, slot_cap, ph, gtab, partial, tw);
+            slots, masks, bin_of_slot, group_begin, group_end, range, counts, slot_cap, ph, partial, tw);
 }
 
 template <int N1>
@@ -712,11 +679,11 @@ void launch_sparse_cols(cudaStream_t s, float2 *slots, const unsigned *masks, co
 
 void launch_tower_rows(cudaStream_t s, float2 *slots, const unsigned *masks, const int *bin_of_slot,
                        const int *group_begin, const int *group_end, const int *range, const int *counts,
-                       int slot_cap, int group_cap, const uint32_t *ph, const float2 *gtab, float2 *partial,
-                       int subgrid, const float2 *tw)
+                       int slot_cap, int group_cap, const uint32_t *ph, float2 *partial, int subgrid,
+                       const float2 *tw)
 {
 #define CALL(N1) tower_rows_impl<N1>(s, slots, masks, bin_of_slot, group_begin, group_end, range, counts, \
-                                     slot_cap, group_cap, ph, gtab, partial, tw)
+                                     slot_cap, group_cap, ph, partial, tw)
     RG_DISPATCH_N1(subgrid, CALL)
 #undef CALL
 }
@@ -799,6 +766,8 @@ static double2 *twiddles64(cudaStream_t s, int n)
     return d;
 }
 
+const double2 *fft64_twiddles(cudaStream_t s, int n) { return twiddles64(s, n); }
+
 static void rows64(cudaStream_t s, double2 *data, int64_t rows, int n, int sign)
 {
     const size_t sm = sizeof(double2) * 2 * n;
@@ -807,13 +776,19 @@ static void rows64(cudaStream_t s, double2 *data, int64_t rows, int n, int sign)
     fft64_rows_kernel<<<(unsigned)rows, threads, sm, s>>>(data, n, sign, twiddles64(s, n));
 }
 
-void launch_fft64_2d(cudaStream_t s, double2 *data, double2 *tmp, int batch, int ny, int nx, int sign)
+void launch_fft64_pow2_rows(cudaStream_t s, double2 *data, int64_t rows, int n, int sign)
 {
-    rows64(s, data, (int64_t)batch * ny, nx, sign);
+    rows64(s, data, rows, n, sign);
+}
+
+void launch_fft64_2d(cudaStream_t s, double2 *data, double2 *tmp, int batch, int ny, int nx, int sign,
+                     double2 *work)
+{
+    launch_fft64_any_rows(s, data, (int64_t)batch * ny, nx, sign, work);
     dim3 blk(32, 8);
     dim3 g1((nx + 31) / 32, (ny + 31) / 32, batch);
     transpose64_kernel<<<g1, blk, 0, s>>>(data, tmp, ny, nx);
-    rows64(s, tmp, (int64_t)batch * nx, ny, sign);
+    launch_fft64_any_rows(s, tmp, (int64_t)batch * nx, ny, sign, work);
     dim3 g2((ny + 31) / 32, (nx + 31) / 32, batch);
     transpose64_kernel<<<g2, blk, 0, s>>>(tmp, data, nx, ny);
 }

@@ -150,6 +150,51 @@ __device__ __forceinline__ void cp_async_wait()
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// The (tower, w-floor) bin of a visibility with the reference's half-open
+// cuts (grid.c:425-458 for the towers, :244-254 for the floors): the nearest
+// chunk and floor are first guesses, the exact comparisons decide among their
+// neighbours.  sb caches the per-chunk bounds when `cached`.
+struct BinHit {
+    int cx, cy, wp;
+    Bounds bx, by;
+};
+__device__ __forceinline__ bool locate_bin(double uu, double vv, double ww, const TowerGeom &g, const Bounds *sb,
+                                           bool cached, int wp_min, int wp_max, double inv_chunk, double inv_winc,
+                                           BinHit &h)
+{
+    const double half_n = (double)(g.grid_size / 2);
+    const int cxc = (int)floor((uu * g.theta + 0.5 + half_n) * inv_chunk);
+    const int cyc = (int)floor((vv * g.theta + 0.5 + half_n) * inv_chunk);
+    const int wpc = (int)floor(ww * inv_winc + 0.5);
+    int found_cx = -1, found_cy = -1;
+    for (int cy = cyc - 1; cy <= cyc + 1 && found_cy < 0; cy++) {
+        if (cy < 0 || cy >= g.nchunk) continue;
+        const Bounds t = cached ? sb[cy] : tower_axis(cy, g.chunk, g.grid_size, g.theta);
+        if (vv < t.lo || vv >= t.hi) continue;
+        found_cy = cy;
+        h.by = t;
+    }
+    for (int cx = cxc - 1; cx <= cxc + 1 && found_cx < 0; cx++) {
+        if (cx < 0 || cx >= g.nchunk) continue;
+        const Bounds t = cached ? sb[cx] : tower_axis(cx, g.chunk, g.grid_size, g.theta);
+        if (uu < t.lo || uu >= t.hi) continue;
+        found_cx = cx;
+        h.bx = t;
+    }
+    bool have_wp = false;
+    for (int wp = wpc - 1; wp <= wpc + 1 && !have_wp; wp++) {
+        if (wp < wp_min || wp > wp_max) continue;
+        const double wlo = __dmul_rn(__dsub_rn((double)wp, 0.5), g.winc);
+        const double whi = __dmul_rn(__dadd_rn((double)wp, 0.5), g.winc);
+        if (ww < wlo || ww >= whi) continue;
+        have_wp = true;
+        h.wp = wp;
+    }
+    h.cx = found_cx;
+    h.cy = found_cy;
+    return found_cx >= 0 && found_cy >= 0 && have_wp;
+}
+
 constexpr int kPrepTile = 256;  // = the kernel's block size
 constexpr int kPrepStages = 4;
 
@@ -195,40 +240,19 @@ __global__ void prepare_towers_kernel(const double *__restrict__ u, const double
             rec[i] = r;
             return;
         }
-        const double half_n = (double)(g.grid_size / 2);
-        const int cxc = (int)floor((uu * g.theta + 0.5 + half_n) * inv_chunk);
-        const int cyc = (int)floor((vv * g.theta + 0.5 + half_n) * inv_chunk);
-        const int wpc = (int)floor(ww * inv_winc + 0.5);
-        int found_cx = -1, found_cy = -1, found_wp = 0;
-        Bounds bx, by;
-        for (int cy = cyc - 1; cy <= cyc + 1 && found_cy < 0; cy++) {
-            if (cy < 0 || cy >= g.nchunk) continue;
-            const Bounds t = cached ? sb[cy] : tower_axis(cy, g.chunk, g.grid_size, g.theta);
-            if (vv < t.lo || vv >= t.hi) continue;
-            found_cy = cy;
-            by = t;
-        }
-        for (int cx = cxc - 1; cx <= cxc + 1 && found_cx < 0; cx++) {
-            if (cx < 0 || cx >= g.nchunk) continue;
-            const Bounds t = cached ? sb[cx] : tower_axis(cx, g.chunk, g.grid_size, g.theta);
-            if (uu < t.lo || uu >= t.hi) continue;
-            found_cx = cx;
-            bx = t;
-        }
-        bool have_wp = false;
-        for (int wp = wpc - 1; wp <= wpc + 1 && !have_wp; wp++) {
-            if (wp < wp_min || wp > wp_max) continue;
-            const double wlo = __dmul_rn(__dsub_rn((double)wp, 0.5), g.winc);
-            const double whi = __dmul_rn(__dadd_rn((double)wp, 0.5), g.winc);
-            if (ww < wlo || ww >= whi) continue;
-            have_wp = true;
-            found_wp = wp;
-        }
-        if (found_cx < 0 || found_cy < 0 || !have_wp) {
+        BinHit h;
+        if (!locate_bin(uu, vv, ww, g, sb, cached, wp_min, wp_max, inv_chunk, inv_winc, h)) {
             dropped++;
             rec[i] = r;
             return;
         }
+        const int tower = h.cy * g.nchunk + h.cx;
+        if (g.tower_sel && !g.tower_sel[tower]) {  // another share's tower
+            rec[i] = r;
+            return;
+        }
+        const int found_wp = h.wp;
+        const Bounds &bx = h.bx, &by = h.by;
         int cell_x, frac_x, cell_y, frac_y;
         const double wmid = __dmul_rn((double)found_wp, g.winc);
         const double wr = __dsub_rn(ww, wmid);
@@ -254,7 +278,6 @@ __global__ void prepare_towers_kernel(const double *__restrict__ u, const double
         }
         const int col0 = cell_x + g.subgrid / 2 - g.ksize / 2;
         const int row0 = cell_y + g.subgrid / 2 - g.ksize / 2;
-        const int tower = found_cy * g.nchunk + found_cx;
         const int bin = tower * nfloor + (found_wp - wp_min);
         r.x = bin;
         r.y = row0 * g.subgrid + col0;
@@ -318,6 +341,71 @@ void launch_prepare_towers(cudaStream_t s, const double *u, const double *v, con
     if (blocks < 1) blocks = 1;
     prepare_towers_kernel<<<blocks, 256, 0, s>>>(u, v, w, vis, n, g, range, rec, visf, active, marks, err,
                                                  counters, feat);
+}
+
+// Tower census: visibilities per tower (shared-memory histogram when the
+// towers fit, else global atomics) and the active (tower, floor) bins.
+__global__ void tower_census_kernel(const double *__restrict__ u, const double *__restrict__ v,
+                                    const double *__restrict__ w, int64_t n, TowerGeom g,
+                                    const int *__restrict__ range, unsigned long long *__restrict__ vis_count,
+                                    int *__restrict__ active, int ntowers, unsigned *err)
+{
+    if (!range[2]) return;  // more floors than the capacity: reported by the w-floors kernel
+    const int wp_min = range[0], nfloor = range[1];
+    const int wp_max = wp_min + nfloor - 1;
+    constexpr int kBoundsCache = 256, kHist = 2048;
+    __shared__ Bounds sb[kBoundsCache];
+    __shared__ unsigned hist[kHist];
+    const bool cached = g.nchunk <= kBoundsCache;
+    const bool local = ntowers <= kHist;
+    if (cached)
+        for (int c = threadIdx.x; c < g.nchunk; c += blockDim.x) sb[c] = tower_axis(c, g.chunk, g.grid_size, g.theta);
+    if (local)
+        for (int t = threadIdx.x; t < ntowers; t += blockDim.x) hist[t] = 0;
+    __syncthreads();
+    const double inv_chunk = 1.0 / (double)g.chunk, inv_winc = 1.0 / g.winc;
+    bool bad = false;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double uu = u[i], vv = v[i], ww = w[i];
+        if (!finite3(uu, vv, ww)) {
+            bad = true;
+            continue;
+        }
+        BinHit h;
+        if (!locate_bin(uu, vv, ww, g, sb, cached, wp_min, wp_max, inv_chunk, inv_winc, h)) continue;
+        const int tower = h.cy * g.nchunk + h.cx;
+        active[(int64_t)tower * nfloor + (h.wp - wp_min)] = 1;
+        if (local) atomicAdd(&hist[tower], 1u);
+        else atomicAdd(vis_count + tower, 1ull);
+    }
+    if (bad) atomicOr(err, DERR_NONFINITE);
+    __syncthreads();
+    if (local)
+        for (int t = threadIdx.x; t < ntowers; t += blockDim.x)
+            if (hist[t]) atomicAdd(vis_count + t, (unsigned long long)hist[t]);
+}
+
+__global__ void tower_floors_kernel(const int *__restrict__ active, const int *__restrict__ range, int ntowers,
+                                    int *__restrict__ floors)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntowers) return;
+    int c = 0;
+    if (range[2])
+        for (int f = 0; f < range[1]; f++) c += active[(int64_t)t * range[1] + f] != 0;
+    floors[t] = c;
+}
+
+void launch_tower_census(cudaStream_t s, const double *u, const double *v, const double *w, int64_t n,
+                         TowerGeom g, const int *range, unsigned long long *vis_count, int *active, int *floors,
+                         int ntowers, int floors_cap, unsigned *err)
+{
+    (void)floors_cap;
+    int blocks = (int)((n + 255) / 256);
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (blocks < 1) blocks = 1;
+    if (n > 0) tower_census_kernel<<<blocks, 256, 0, s>>>(u, v, w, n, g, range, vis_count, active, ntowers, err);
+    tower_floors_kernel<<<(ntowers + 127) / 128, 128, 0, s>>>(active, range, ntowers, floors);
 }
 
 __global__ void prepare_wproj_kernel(const double *__restrict__ u, const double *__restrict__ v,

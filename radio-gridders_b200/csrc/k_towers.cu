@@ -11,11 +11,8 @@ namespace rg {
 // contraction) and stored as its fraction of a turn in 32-bit fixed point:
 // phq[y*S + x] = round(frac(ph) 2^32) mod 2^32.  The row stage raises
 // exp(2 pi i ph) to the power -wp as the integer product -wp * phq mod 2^32,
-// exact to |wp| 2^-33 turns.  gtab (when given) holds exp(2 pi i ph) itself,
-// evaluated in FP64 (sincospi of the reduced fraction) and rounded to FP32:
-// the one-floor step of the row stage's Horner recurrence.
-__global__ void fresnel_table_kernel(uint32_t *__restrict__ phq, float2 *__restrict__ gtab, int S, double theta,
-                                     double winc)
+// exact to |wp| 2^-33 turns.
+__global__ void fresnel_table_kernel(uint32_t *__restrict__ phq, int S, double theta, double winc)
 {
     const int64_t total = (int64_t)S * S;
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total;
@@ -28,20 +25,15 @@ __global__ void fresnel_table_kernel(uint32_t *__restrict__ phq, float2 *__restr
         const double ph = __dmul_rn(winc, __dsub_rn(1.0, r));
         const double frac = __dsub_rn(ph, floor(ph));  // [0, 1), exact
         phq[k] = (uint32_t)__double2ull_rn(ldexp(frac, 32));  // 2^32 wraps to 0
-        if (gtab) {
-            double sn, cs;
-            sincospi(__dmul_rn(2.0, frac), &sn, &cs);
-            gtab[k] = make_float2((float)cs, (float)sn);
-        }
     }
 }
 
-void launch_fresnel_table(cudaStream_t s, uint32_t *phq, float2 *gtab, int subgrid, double theta, double winc)
+void launch_fresnel_table(cudaStream_t s, uint32_t *phq, int subgrid, double theta, double winc)
 {
     const int64_t total = (int64_t)subgrid * subgrid;
     int blocks = (int)((total + 255) / 256);
     if (blocks > 4096) blocks = 4096;
-    fresnel_table_kernel<<<blocks, 256, 0, s>>>(phq, gtab, subgrid, theta, winc);
+    fresnel_table_kernel<<<blocks, 256, 0, s>>>(phq, subgrid, theta, winc);
 }
 
 // a / d for 0 <= a < 2^24, d > 0: float reciprocal estimate, corrected to the

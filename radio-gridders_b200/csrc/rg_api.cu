@@ -1,5 +1,6 @@
 // C-ABI layer: argument checks, host/device staging, scratch management and
 // the launch sequences of each entry point (include/radio_gridders.h).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -84,15 +85,7 @@ rg_status stage_in(rg_context *ctx, const void *ptr, size_t bytes, const char *n
     return RG_OK;
 }
 
-// Output view: device pointer itself, or a scratch buffer copied back by finish_out.
-struct OutView {
-    void *user = nullptr;
-    void *dev = nullptr;
-    size_t bytes = 0;
-    bool host = false;
-};
-
-static rg_status out_view(rg_context *ctx, void *ptr, size_t bytes, const char *name, bool load,
+rg_status out_view(rg_context *ctx, void *ptr, size_t bytes, const char *name, bool load,
                           OutView *ov)
 {
     ov->user = ptr;
@@ -108,7 +101,7 @@ static rg_status out_view(rg_context *ctx, void *ptr, size_t bytes, const char *
     return RG_OK;
 }
 
-static rg_status finish_out(rg_context *ctx, const OutView &ov)
+rg_status finish_out(rg_context *ctx, const OutView &ov)
 {
     if (ov.host) RG_CUDA(cudaMemcpyAsync(ov.user, ov.dev, ov.bytes, cudaMemcpyDeviceToHost, ctx->stream));
     return RG_OK;
@@ -525,10 +518,9 @@ static rg_status wtowers_enqueue(rg_context *ctx, const DevVis &dv, const float2
         char key[160];
         std::snprintf(key, sizeof(key), "phq_%d_%.17g_%.17g", S, theta, winc);
         bool fresh = ctx->scratch.find(key) == ctx->scratch.end();
-        // the fixed-point phase table, then exp(2 pi i ph) in FP32
-        RG_CHECK(scratch(ctx, key, (sizeof(uint32_t) + sizeof(float2)) * (size_t)sub_cells, &ph));
+        RG_CHECK(scratch(ctx, key, sizeof(uint32_t) * (size_t)sub_cells, &ph));
         if (fresh) {
-            launch_fresnel_table(st, (uint32_t *)ph, (float2 *)((uint32_t *)ph + sub_cells), S, theta, winc);
+            launch_fresnel_table(st, (uint32_t *)ph, S, theta, winc);
             ctx->launches++;
         }
     }
@@ -552,6 +544,7 @@ static rg_status wtowers_enqueue(rg_context *ctx, const DevVis &dv, const float2
     g.winc = winc;
     g.wk_wmin = lt ? 0.0 : wkern->w_min;
     g.wk_wstep = lt ? 1.0 : wkern->w_step;
+    g.tower_sel = pl.tower_sel;
 
     begin_stage(ctx, "w_range");
     launch_minmax_w(st, dv.u, dv.v, dv.w, dv.n, (double *)mm, d.err);
@@ -599,7 +592,7 @@ static rg_status wtowers_enqueue(rg_context *ctx, const DevVis &dv, const float2
     begin_stage(ctx, "tower_rows");
     launch_tower_rows(st, (float2 *)slots, (const unsigned *)masks, (const int *)bin_of_slot, (const int *)gbegin,
                       (const int *)gend, range, counts, pl.slots_cap, pl.groups_cap, (const uint32_t *)ph,
-                      (const float2 *)((const uint32_t *)ph + sub_cells), (float2 *)partial, S, tw);
+                      (float2 *)partial, S, tw);
     end_stage(ctx);
     begin_stage(ctx, "tower_finish");
     launch_tower_finish(st, pl.groups_cap, (const int *)tgfirst, (const int *)tgcount, ntowers,
@@ -767,7 +760,7 @@ static void capture_pass(rg_context *ctx, const DevVis &dv, const float2 *taps, 
 // W-towers with table taps (lt == nullptr) or learned taps (wkern unused).
 rg_status grid_wtowers_impl(rg_context *ctx, double *uvgrid, int grid_size, double theta, const rg_vis *vis,
                             const rg_wkern *wkern, const LearnedTaps *lt, int subgrid_size, int subgrid_margin,
-                            double wincrement, int flags)
+                            double wincrement, int flags, const int32_t *part_of_tower, int part)
 {
     if (!ctx || !uvgrid) return fail(RG_ERR_INVALID_ARGUMENT, "ctx and uvgrid must be non-NULL");
     if (grid_size < 2 || grid_size > 16384) return fail(RG_ERR_UNSUPPORTED, "grid_size must be in [2, 16384]");
@@ -801,10 +794,36 @@ rg_status grid_wtowers_impl(rg_context *ctx, double *uvgrid, int grid_size, doub
                       !(flags & RG_GRID_OVERWRITE), &ov));
     end_stage(ctx);
 
-    char keybuf[200];
-    std::snprintf(keybuf, sizeof(keybuf), "%d_%d_%d_%.17g_%.17g_%lld_%c", N, S, M, theta, wincrement,
-                  (long long)dv.n, lt ? 'L' : 'T');
+    // a share of a tower-partitioned observation: the selected towers as one
+    // byte each in device memory, named by their fingerprint (a plan and its
+    // captured graph keep pointing at the same selection)
+    std::string selkey;
+    const unsigned char *sel_dev = nullptr;
+    if (part_of_tower) {
+        std::vector<unsigned char> sel((size_t)ntowers);
+        uint64_t h = 1469598103934665603ull;  // FNV-1a
+        for (int t = 0; t < ntowers; t++) {
+            sel[t] = part_of_tower[t] == part ? 1 : 0;
+            h = (h ^ sel[t]) * 1099511628211ull;
+        }
+        char hb[40];
+        std::snprintf(hb, sizeof(hb), "_sel%016llx", (unsigned long long)h);
+        selkey = hb;
+        const std::string name = "tower_sel" + selkey;
+        const bool fresh = ctx->scratch.find(name) == ctx->scratch.end();
+        void *p = nullptr;
+        RG_CHECK(scratch(ctx, name.c_str(), (size_t)ntowers, &p));
+        if (fresh) {
+            RG_CUDA(cudaMemcpyAsync(p, sel.data(), (size_t)ntowers, cudaMemcpyHostToDevice, ctx->stream));
+            RG_CUDA(cudaStreamSynchronize(ctx->stream));
+        }
+        sel_dev = (const unsigned char *)p;
+    }
+    char keybuf[240];
+    std::snprintf(keybuf, sizeof(keybuf), "%d_%d_%d_%.17g_%.17g_%lld_%c%s", N, S, M, theta, wincrement,
+                  (long long)dv.n, lt ? 'L' : 'T', selkey.c_str());
     TowerPlan &pl = ctx->tower_plans[keybuf];
+    pl.tower_sel = sel_dev;
     if (!pl.valid) {  // first call for this shape: generous capacities, learn the real sizes
         pl.floors_cap = 256;
         pl.slots_cap = ntowers * 16 + 64;
@@ -1054,6 +1073,122 @@ rg_status rg_grid_wtowers(rg_context *ctx, double *uvgrid, int grid_size, double
                                  wincrement, flags);
 }
 
+static rg_status check_towers_shape(int grid_size, double theta, int S, int M, double winc)
+{
+    if (grid_size < 2 || grid_size > 16384) return fail(RG_ERR_UNSUPPORTED, "grid_size must be in [2, 16384]");
+    if (!(theta > 0.0) || !std::isfinite(theta)) return fail(RG_ERR_INVALID_ARGUMENT, "theta must be > 0");
+    if (!(winc > 0.0) || !std::isfinite(winc)) return fail(RG_ERR_INVALID_ARGUMENT, "wincrement must be > 0");
+    if (S % 2 || M % 2 || M < 0 || M >= S || S < 2)
+        return fail(RG_ERR_INVALID_ARGUMENT, "subgrid size and margin must be even, 0 <= margin < subgrid");
+    return RG_OK;
+}
+
+int rg_wtowers_tower_count(int grid_size, int subgrid_size, int subgrid_margin)
+{
+    const int chunk = subgrid_size - subgrid_margin;
+    if (chunk <= 0 || grid_size < 1) return 0;
+    const int nc = grid_size / chunk + 1;
+    return nc * nc;
+}
+
+rg_status rg_wtowers_tower_loads(rg_context *ctx, int grid_size, double theta, const rg_vis *vis,
+                                 int subgrid_size, int subgrid_margin, double wincrement, int64_t *vis_per_tower,
+                                 int32_t *floors_per_tower, int ntowers)
+{
+    if (!ctx || !vis_per_tower || !floors_per_tower)
+        return fail(RG_ERR_INVALID_ARGUMENT, "ctx and the output arrays must be non-NULL");
+    RG_CHECK(check_towers_shape(grid_size, theta, subgrid_size, subgrid_margin, wincrement));
+    RG_CHECK(check_vis(vis));
+    const int S = subgrid_size, M = subgrid_margin, N = grid_size;
+    const int chunk = S - M, nchunk = N / chunk + 1, nt = nchunk * nchunk;
+    if (ntowers != nt)
+        return fail(RG_ERR_INVALID_ARGUMENT, "ntowers must be rg_wtowers_tower_count(grid, subgrid, margin)");
+    RG_CUDA(cudaSetDevice(ctx->device));
+    begin_call(ctx);
+    DevVis dv;
+    RG_CHECK(stage_vis(ctx, vis, &dv));
+    Diag d;
+    RG_CHECK(diag_begin(ctx, &d));
+    int *range = (int *)((char *)d.err + 48);
+    // the floor count is known only on the device: size the bins for the
+    // largest count the w range allows, read back once
+    void *mm, *vc, *fl, *act;
+    RG_CHECK(scratch(ctx, "wminmax", 16, &mm));
+    RG_CHECK(scratch(ctx, "census_vis", sizeof(unsigned long long) * (size_t)nt, &vc));
+    RG_CHECK(scratch(ctx, "census_floors", sizeof(int) * (size_t)nt, &fl));
+    launch_minmax_w(ctx->stream, dv.u, dv.v, dv.w, dv.n, (double *)mm, d.err);
+    double wr[2];
+    RG_CUDA(cudaMemcpyAsync(wr, mm, sizeof(wr), cudaMemcpyDeviceToHost, ctx->stream));
+    RG_CUDA(cudaStreamSynchronize(ctx->stream));
+    const double nf = std::floor(wr[1] / wincrement + 0.5) - std::floor(wr[0] / wincrement + 0.5) + 1;
+    if (!(nf >= 1) || nf * nt > (double)(1 << 28))
+        return fail(RG_ERR_UNSUPPORTED, "too many (tower, w-floor) bins; increase wincrement");
+    const int floors_cap = (int)nf;
+    RG_CHECK(scratch(ctx, "census_active", sizeof(int) * (size_t)nt * floors_cap, &act));
+    RG_CUDA(cudaMemsetAsync(act, 0, sizeof(int) * (size_t)nt * floors_cap, ctx->stream));
+    RG_CUDA(cudaMemsetAsync(vc, 0, sizeof(unsigned long long) * (size_t)nt, ctx->stream));
+    launch_w_floors(ctx->stream, (const double *)mm, wincrement, floors_cap, range, d.err);
+    TowerGeom g;
+    g.grid_size = N;
+    g.subgrid = S;
+    g.margin = M;
+    g.chunk = chunk;
+    g.nchunk = nchunk;
+    g.ksize = 0;
+    g.ov = 1;
+    g.planes = 1;
+    g.theta = theta;
+    g.winc = wincrement;
+    g.wk_wmin = 0.0;
+    g.wk_wstep = 1.0;
+    launch_tower_census(ctx->stream, dv.u, dv.v, dv.w, dv.n, g, range, (unsigned long long *)vc, (int *)act,
+                        (int *)fl, nt, floors_cap, d.err);
+    ctx->launches += 4;
+    RG_CHECK(check_launch("W-towers tower census"));
+    RG_CUDA(cudaMemcpyAsync(vis_per_tower, vc, sizeof(int64_t) * (size_t)nt, cudaMemcpyDeviceToHost, ctx->stream));
+    RG_CUDA(cudaMemcpyAsync(floors_per_tower, fl, sizeof(int32_t) * (size_t)nt, cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    RG_CHECK(diag_end(ctx, d, nullptr));
+    return RG_OK;
+}
+
+rg_status rg_wtowers_partition(const int64_t *vis_per_tower, const int32_t *floors_per_tower, int ntowers,
+                               int nparts, double vis_per_floor, int32_t *part_of_tower)
+{
+    if (!vis_per_tower || !floors_per_tower || !part_of_tower || ntowers < 0 || nparts < 1)
+        return fail(RG_ERR_INVALID_ARGUMENT, "bad partition arguments");
+    if (!(vis_per_floor >= 0.0) || !std::isfinite(vis_per_floor))
+        return fail(RG_ERR_INVALID_ARGUMENT, "vis_per_floor must be finite and >= 0");
+    const double wf = vis_per_floor > 0.0 ? vis_per_floor : 2400.0;
+    // longest-processing-time first: towers by cost, largest first (ties by
+    // index), each to the least loaded part (ties to the lowest part)
+    std::vector<int> order((size_t)ntowers);
+    std::vector<double> cost((size_t)ntowers);
+    for (int t = 0; t < ntowers; t++) {
+        order[t] = t;
+        cost[t] = (double)vis_per_tower[t] + wf * (double)floors_per_tower[t];
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    std::vector<double> load((size_t)nparts, 0.0);
+    for (int t : order) {
+        int best = 0;
+        for (int p = 1; p < nparts; p++)
+            if (load[p] < load[best]) best = p;
+        part_of_tower[t] = best;
+        load[best] += cost[t];
+    }
+    return RG_OK;
+}
+
+rg_status rg_grid_wtowers_part(rg_context *ctx, double *uvgrid, int grid_size, double theta, const rg_vis *vis,
+                               const rg_wkern *wkern, int subgrid_size, int subgrid_margin, double wincrement,
+                               int flags, const int32_t *part_of_tower, int part)
+{
+    if (!part_of_tower) return fail(RG_ERR_INVALID_ARGUMENT, "part_of_tower must be non-NULL");
+    return rg::grid_wtowers_impl(ctx, uvgrid, grid_size, theta, vis, wkern, nullptr, subgrid_size, subgrid_margin,
+                                 wincrement, flags, part_of_tower, part);
+}
+
 rg_status rg_grid_wtowers_batch(rg_context *ctx, int count, double *const *uvgrids, int grid_size, double theta,
                                 const rg_vis *vis, const rg_wkern *wkern, int subgrid_size, int subgrid_margin,
                                 double wincrement, int flags)
@@ -1118,8 +1253,8 @@ rg_status rg_image_from_grid(rg_context *ctx, double *uvgrid, int grid_size, dou
                              const double *taper_1d)
 {
     if (!ctx || !uvgrid || !image_out) return fail(RG_ERR_INVALID_ARGUMENT, "NULL argument");
-    if (!fft64_supported(grid_size) || grid_size < 2)
-        return fail(RG_ERR_UNSUPPORTED, "image formation needs a power-of-two grid_size in [2, 4096]");
+    if (!fft64_any_supported(grid_size) || grid_size % 2)
+        return fail(RG_ERR_UNSUPPORTED, "image formation needs an even grid_size in [2, 4096]");
     RG_CUDA(cudaSetDevice(ctx->device));
     const int N = grid_size;
     const int64_t cells = (int64_t)N * N;
@@ -1133,7 +1268,10 @@ rg_status rg_image_from_grid(rg_context *ctx, double *uvgrid, int grid_size, dou
     RG_CHECK(out_view(ctx, image_out, sizeof(double) * (size_t)cells, "img_out", false, &img));
     launch_make_hermitian(ctx->stream, (double2 *)g.dev, N);
     launch_fft_shift(ctx->stream, (double2 *)g.dev, N);
-    launch_fft64_2d(ctx->stream, (double2 *)g.dev, (double2 *)tmp, 1, N, N, -1);
+    void *work = nullptr;
+    if (fft64_any_work_elems(N) > 0)
+        RG_CHECK(scratch(ctx, "fft64_work", sizeof(double2) * (size_t)fft64_any_work_elems(N), &work));
+    launch_fft64_2d(ctx->stream, (double2 *)g.dev, (double2 *)tmp, 1, N, N, -1, (double2 *)work);
     launch_fft_shift(ctx->stream, (double2 *)g.dev, N);
     launch_real_part(ctx->stream, (const double2 *)g.dev, (double *)img.dev, N, (const double *)taper);
     RG_CHECK(check_launch("image formation"));
@@ -1161,13 +1299,16 @@ rg_status rg_fft2d(rg_context *ctx, void *data, int batch, int ny, int nx, int s
         RG_CHECK(check_launch("fft32"));
         RG_CHECK(finish_out(ctx, ov));
     } else if (complex_bytes == 16) {
-        if (!fft64_supported(nx) || !fft64_supported(ny))
-            return fail(RG_ERR_UNSUPPORTED, "FP64 transforms need power-of-two sizes <= 4096");
+        if (!fft64_any_supported(nx) || !fft64_any_supported(ny))
+            return fail(RG_ERR_UNSUPPORTED, "FP64 transforms need sizes in [2, 4096]");
         OutView ov;
         RG_CHECK(out_view(ctx, data, bytes, "fft_data", true, &ov));
         void *tmp;
         RG_CHECK(scratch(ctx, "fft_tmp", bytes, &tmp));
-        launch_fft64_2d(ctx->stream, (double2 *)ov.dev, (double2 *)tmp, batch, ny, nx, sign);
+        const int64_t wel = std::max(fft64_any_work_elems(nx), fft64_any_work_elems(ny));
+        void *work = nullptr;
+        if (wel > 0) RG_CHECK(scratch(ctx, "fft64_work", sizeof(double2) * (size_t)wel, &work));
+        launch_fft64_2d(ctx->stream, (double2 *)ov.dev, (double2 *)tmp, batch, ny, nx, sign, (double2 *)work);
         RG_CHECK(check_launch("fft64"));
         RG_CHECK(finish_out(ctx, ov));
     } else {

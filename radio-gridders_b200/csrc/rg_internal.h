@@ -59,9 +59,11 @@ struct LearnedTaps {
     float inv_wmax, scale;
     double wmax;
 };
+// part_of_tower (ntowers entries) with part: grid only the towers t with
+// part_of_tower[t] == part (one share of a tower-partitioned observation).
 rg_status grid_wtowers_impl(rg_context *ctx, double *uvgrid, int grid_size, double theta, const rg_vis *vis,
                             const rg_wkern *wkern, const LearnedTaps *lt, int subgrid_size, int subgrid_margin,
-                            double wincrement, int flags);
+                            double wincrement, int flags, const int32_t *part_of_tower = nullptr, int part = 0);
 
 }  // namespace rg
 
@@ -82,6 +84,7 @@ struct TowerPlan {
     std::string graph_key;
     int graph_launches = 0;
     uint64_t graph_scratch_gen = 0;  // scratch generation the graph's pointers belong to
+    const unsigned char *tower_sel = nullptr;  // device: the towers this plan grids (nullptr: all)
 };
 
 struct rg_stage_event {
@@ -140,6 +143,18 @@ rg_status stage_in(rg_context *ctx, const void *ptr, size_t bytes, const char *n
                    const void **dev);
 bool is_device_pointer(const void *p);
 
+// Output view of a caller buffer: the device pointer itself, or a scratch
+// buffer (loaded from the host buffer when `load`) that finish_out copies
+// back on the context stream.
+struct OutView {
+    void *user = nullptr;
+    void *dev = nullptr;
+    size_t bytes = 0;
+    bool host = false;
+};
+rg_status out_view(rg_context *ctx, void *ptr, size_t bytes, const char *name, bool load, OutView *ov);
+rg_status finish_out(rg_context *ctx, const OutView &ov);
+
 // ---------------------------------------------------------------------------
 // kernel launchers (defined in k_*.cu)
 // ---------------------------------------------------------------------------
@@ -171,16 +186,34 @@ void launch_fft32_rows(cudaStream_t s, float2 *data, int64_t rows, int n, int si
 // left as they are (live may be NULL: all)
 void launch_fft32_cols(cudaStream_t s, float2 *data, int batch, int n, int sign,
                        const float2 *tw, const int *live = nullptr);
-// FP64 transforms for image formation (n power of two, <= 4096)
+// FP64 transforms for image formation: power-of-two n <= 4096 directly,
+// any other n <= 4096 by Bluestein's algorithm (k_bluestein.cu), which needs
+// fft64_any_work_elems(n) double2 of work space (0 for powers of two).
 bool fft64_supported(int n);
+bool fft64_any_supported(int n);
+constexpr int kBluesteinRows = 512;  // rows per Bluestein chunk (work space)
+int64_t fft64_any_work_elems(int n);
+const double2 *fft64_twiddles(cudaStream_t s, int n);  // exp(-2 pi i k / n), k < n/2 (cached)
+void launch_fft64_pow2_rows(cudaStream_t s, double2 *data, int64_t rows, int n, int sign);
+void launch_fft64_any_rows(cudaStream_t s, double2 *data, int64_t rows, int n, int sign, double2 *work);
 void launch_fft64_2d(cudaStream_t s, double2 *data, double2 *tmp, int batch, int ny, int nx,
-                     int sign);
+                     int sign, double2 *work = nullptr);
 
 // k_prepare.cu
 struct TowerGeom {
     int grid_size, subgrid, margin, chunk, nchunk, ksize, ov, planes;
     double theta, winc, wk_wmin, wk_wstep;
+    // towers this call grids (one byte per tower, nonzero = grid it), or
+    // nullptr for all: the visibilities of the other towers are skipped (not
+    // counted as dropped) — one share of a tower-partitioned observation
+    const unsigned char *tower_sel = nullptr;
 };
+// Per-tower load of a W-towers observation: visibilities and active w-floors
+// of each tower (vis_count: ntowers int64, active: ntowers*nfloor ints zeroed
+// by the caller, floors: ntowers ints), with the binning cuts of the gridder.
+void launch_tower_census(cudaStream_t s, const double *u, const double *v, const double *w, int64_t n,
+                         TowerGeom g, const int *range, unsigned long long *vis_count, int *active,
+                         int *floors, int ntowers, int floors_cap, unsigned *err);
 void launch_minmax_w(cudaStream_t s, const double *u, const double *v, const double *w,
                      int64_t n, double *out4, unsigned *err);
 // range[0] = wp_min, range[1] = nfloor, range[2] = 1 if nfloor <= floors_cap
@@ -229,9 +262,7 @@ void launch_romein(cudaStream_t s, const int4 *rec, const float2 *visf, int64_t 
                    int points = 0, int strip_lg = 0);
 
 // k_towers.cu
-// phq: the Fresnel phase as a 32-bit fraction of a turn; gtab (optional):
-// exp(2 pi i ph) rounded from FP64 to FP32.
-void launch_fresnel_table(cudaStream_t s, uint32_t *phq, float2 *gtab, int subgrid, double theta, double winc);
+void launch_fresnel_table(cudaStream_t s, uint32_t *phq, int subgrid, double theta, double winc);
 // Sparse sub-grid transforms and the W-towers row stage.  Group g covers
 // active slots [group_begin[g], group_end[g]) of one tower; partial holds one
 // sub-grid per group; tower t's groups are [tower_group_first[t],
@@ -253,7 +284,7 @@ void launch_sparse_cols(cudaStream_t s, float2 *slots, const unsigned *masks, co
 void launch_tower_rows(cudaStream_t s, float2 *slots, const unsigned *masks, const int *bin_of_slot,
                        const int *group_begin, const int *group_end, const int *range,
                        const int *counts, int slot_cap, int group_cap, const uint32_t *phq,
-                       const float2 *gtab, float2 *partial, int subgrid, const float2 *tw);
+                       float2 *partial, int subgrid, const float2 *tw);
 // Per tower: the sum of its groups' partials (in group order) and the forward
 // row transform into subimg.  The forward column transform of subimg follows
 // (launch_fft32_cols).

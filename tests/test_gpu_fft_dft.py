@@ -33,6 +33,39 @@ def test_fft64_vs_numpy(ctx, n):
     assert rel_rms(y, np.fft.fft2(x)) < 1e-13
 
 
+@pytest.mark.parametrize("ny,nx", [(6, 10), (100, 250), (2500, 2500), (4094, 3)])
+@pytest.mark.parametrize("sign", [-1, 1])
+def test_fft64_any_length_vs_numpy(ctx, ny, nx, sign):
+    """Lengths that are not powers of two (Bluestein's chirp-z over
+    power-of-two transforms), both signs."""
+    rng = np.random.default_rng(ny * 7 + nx)
+    x = rng.normal(size=(1, ny, nx)) + 1j * rng.normal(size=(1, ny, nx))
+    y = x.copy()
+    ctx.fft2d(y, sign)
+    ref = np.fft.fft2(x) if sign < 0 else np.fft.ifft2(x) * (nx * ny)
+    assert rel_rms(y, ref) < 1e-12
+
+
+def test_image_at_a_grid_size_that_is_not_a_power_of_two(rg, ctx, sim, oracle):
+    """grid.out's grid size is floor(lambda * theta): theta 0.1, lambda 25000
+    gives 2500.  W-projection grid against the oracle, and the dirty image
+    (hermitian, shift, FFT sign -1, shift; src/reference/main.c:258-294)
+    against the oracle's hermitian and shift with numpy's FFT."""
+    obs = sim.wproj_plain(seed=3, lam=25000.0)
+    n, th = obs.meta["grid_size"], obs.meta["theta"]
+    assert n == 2500
+    u, v, w, vis = obs.flat()
+    wk = sim.wkernel_for(w, th, 10.0, size=16, oversampling=8)
+    g = np.zeros((n, n), np.complex128)
+    ctx.grid_wprojection(g, n, th, rg.Visibilities(u, v, w, vis), wk)
+    ref = oracle.grid_wprojection(n, th, u, v, w, vis, wk)
+    assert rel_rms(g, ref) < 1e-5
+    img = ctx.image_from_grid(g.copy())
+    h = oracle.fft_shift(oracle.make_hermitian(g.copy()))
+    img_ref = oracle.fft_shift(np.fft.fft2(h)).real
+    assert rel_rms(img, img_ref) < 1e-12
+
+
 @pytest.fixture(scope="module")
 def dft_case(sim):
     obs = sim.dft_study(n_vis=20_000)

@@ -185,3 +185,31 @@ def test_wtowers_full_benchmark_workload(rg, ctx, sim, oracle):
     assert rel_rms(g, ref) < TOL
     st = ctx.last_stats()
     assert st["gridded"] + st["dropped"] == len(u) and st["active_subgrids"] > 900
+
+
+def test_wtowers_tower_shares_sum_to_the_whole(rg, ctx, sim, oracle, wproj_data):
+    """One observation's towers split three ways (rg_wtowers_tower_loads +
+    rg_wtowers_partition): the device census equals the oracle's, and the
+    three shares gridded by rg_grid_wtowers_part sum to rg_grid_wtowers'
+    grid and to the oracle's."""
+    obs, u, v, w, vis = wproj_data
+    n, th = obs.meta["grid_size"], obs.meta["theta"]
+    S, M, winc = 128, 16, 10.0
+    wkt = sim.generate_wkernel(th, np.arange(-6, 7, 1.0))
+    Vs = V(rg, u, v, w, vis)
+    nv, nf = ctx.tower_loads(n, th, Vs, S, M, winc)
+    onv, onf = oracle.wtowers_census(n, th, u, v, w, S, M, winc)
+    assert np.array_equal(nv, onv) and np.array_equal(nf, onf)
+    parts = rg.partition_towers(nv, nf, 3)
+    total = np.zeros((n, n), np.complex128)
+    gridded = 0
+    for p in range(3):
+        g = np.zeros((n, n), np.complex128)
+        ctx.grid_wtowers_part(g, n, th, Vs, wkt, S, M, winc, parts, p)
+        gridded += ctx.last_stats()["gridded"]
+        total += g
+    whole = np.zeros((n, n), np.complex128)
+    ctx.grid_wtowers(whole, n, th, Vs, wkt, S, M, winc)
+    assert gridded == ctx.last_stats()["gridded"] == int(nv.sum())
+    assert rel_rms(total, whole) < 1e-6
+    assert rel_rms(total, oracle.grid_wtowers(n, th, u, v, w, vis, wkt, S, M, winc)) < TOL

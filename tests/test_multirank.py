@@ -1,10 +1,13 @@
 """The multi-GPU path of bench.py, run as world_size-2 gloo ranks on CPU.
 
-Each rank grids its own snapshot (the oracle stands in for the GPU gridder,
-which needs a B200) and bench.reduce_master sums the master grids onto rank 0.
-By linearity the result must equal gridding both snapshots together; a rank
-that raises is reported as a failure, not a hang (short process-group
-timeout)."""
+One observation's towers are split over the ranks by the library's own
+partition (rg_wtowers_partition, a host function: balanced by visibilities
+and active w-floors), each rank grids its share (the oracle's W-towers
+restricted to those towers stands in for rg_grid_wtowers_part, which needs a
+B200) and bench.reduce_master sums the FP64 master grids onto rank 0.  The
+towers are independent until the add-back, so the sum must equal gridding
+the whole observation on one rank to FP64 rounding; a rank that raises is
+reported as a failure, not a hang (short process-group timeout)."""
 import datetime
 import importlib
 import os
@@ -25,14 +28,14 @@ def _free_port():
     return port
 
 
-def _snapshot(sim, rank):
+S, M, WINC = 128, 16, 10.0
+
+
+def _observation(sim):
     obs = sim.wproj_plain(seed=0, n_dump=8)
-    # each rank observes a later stretch of hour angle (same array and sky)
     u, v, w, vis = obs.flat()
-    rot = 0.15 * rank
-    c, s = np.cos(rot), np.sin(rot)
-    uu, vv = c * u - s * v, s * u + c * v
-    return uu, vv, w, vis, obs.meta
+    wk = sim.generate_wkernel(obs.meta["theta"], np.arange(-6.0, 7.0, 1.0), 8, 4)
+    return u, v, w, vis, obs.meta, wk
 
 
 def _worker(rank, world, port, out_path, fail_rank):
@@ -47,15 +50,18 @@ def _worker(rank, world, port, out_path, fail_rank):
                             timeout=datetime.timedelta(seconds=30))
     try:
         sim = importlib.import_module("radio-gridders_b200.simulate")
-        u, v, w, vis, meta = _snapshot(sim, rank)
+        u, v, w, vis, meta, wk = _observation(sim)
         if rank == fail_rank:
             raise RuntimeError("injected failure on rank %d" % rank)
-        wk = sim.generate_wkernel(meta["theta"], np.arange(-1800, 1801, 10.0), 8, 4)
-        g = oracle.grid_wprojection(meta["grid_size"], meta["theta"], u, v, w, vis, wk)
+        n, th = meta["grid_size"], meta["theta"]
+        nv, nf = oracle.wtowers_census(n, th, u, v, w, S, M, WINC)
+        parts = bench.tower_parts(nv, nf, world)
+        g = oracle.grid_wtowers(n, th, u, v, w, vis, wk, S, M, WINC, towers=(parts == rank))
         t = torch.from_numpy(g)
         bench.reduce_master(t, world)
         if rank == 0:
             np.save(out_path, t.numpy())
+            np.save(out_path + ".parts.npy", parts)
     finally:
         dist.destroy_process_group()
 
@@ -77,20 +83,39 @@ def _run(world, fail_rank, tmp_path):
     return codes, out
 
 
-def test_two_ranks_reduce_equals_joint_gridding(sim, oracle, tmp_path):
+def test_two_ranks_tower_shares_sum_to_the_whole(sim, oracle, tmp_path):
     _free_port.port = _free_port()
     codes, out = _run(2, -1, tmp_path)
     assert codes == [0, 0]
     got = np.load(out)
-    wk = sim.generate_wkernel(0.1, np.arange(-1800, 1801, 10.0), 8, 4)
-    parts = [_snapshot(sim, r) for r in range(2)]
-    u = np.concatenate([p[0] for p in parts])
-    v = np.concatenate([p[1] for p in parts])
-    w = np.concatenate([p[2] for p in parts])
-    vis = np.concatenate([p[3] for p in parts])
-    meta = parts[0][4]
-    ref = oracle.grid_wprojection(meta["grid_size"], meta["theta"], u, v, w, vis, wk)
+    u, v, w, vis, meta, wk = _observation(sim)
+    n, th = meta["grid_size"], meta["theta"]
+    ref = oracle.grid_wtowers(n, th, u, v, w, vis, wk, S, M, WINC)
     assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-12
+    # both ranks had towers with data, and the loads are balanced
+    parts = np.load(out + ".parts.npy")
+    nv, nf = oracle.wtowers_census(n, th, u, v, w, S, M, WINC)
+    cost = nv + 2400.0 * nf
+    loads = [cost[parts == r].sum() for r in range(2)]
+    assert min(loads) > 0 and max(loads) <= 1.25 * np.mean(loads) + cost.max()
+
+
+def test_partition_is_deterministic_and_balanced(rg):
+    """Largest first to the least loaded part: every tower gets a part in
+    range, equal inputs give equal outputs, and no part exceeds the mean by
+    more than the largest tower."""
+    rng = np.random.default_rng(3)
+    nv = rng.integers(0, 200_000, 81)
+    nf = rng.integers(0, 60, 81)
+    for parts_n in (1, 2, 3, 8):
+        p1 = rg.partition_towers(nv, nf, parts_n)
+        p2 = rg.partition_towers(nv.copy(), nf.copy(), parts_n)
+        assert np.array_equal(p1, p2) and p1.min() >= 0 and p1.max() < parts_n
+        cost = nv + 2400.0 * nf
+        loads = np.array([cost[p1 == r].sum() for r in range(parts_n)])
+        assert loads.max() <= loads.mean() + cost.max()
+    with pytest.raises(rg.RGError):
+        rg.partition_towers(nv, nf, 0)
 
 
 def test_failing_rank_is_reported_not_hung(tmp_path):

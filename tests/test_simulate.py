@@ -1,4 +1,6 @@
 """The project's synthetic-data and w-kernel generator (CPU)."""
+import importlib
+
 import numpy as np
 import pytest
 
@@ -48,3 +50,17 @@ def test_generator_is_seeded(sim):
     b = sim.wproj_plain(seed=3, n_dump=4).flat()
     for x, y in zip(a, b):
         assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("c", [3.0 * np.pi, 7.0 * np.pi, 5.0, 40.0])
+def test_library_pswf_matches_generator(c):
+    """rg_pswf0 (the C ABI generator's taper: Sturm bisection and inverse
+    iteration for the Legendre coefficients) against the Python generator's
+    psi_0 (dense symmetric eigensolver), which is itself checked against
+    scipy.special.pro_ang1 above."""
+    rg = importlib.import_module("radio-gridders_b200")
+    sim = importlib.import_module("radio-gridders_b200.simulate")
+    x = np.linspace(-1.0, 1.0, 301)
+    assert np.abs(rg.pswf0(c, x) - sim.pswf0(c, x)).max() < 1e-13
+    with pytest.raises(rg.RGError):
+        rg.pswf0(c, np.array([1.5]))
