@@ -330,6 +330,35 @@ rg_status rg_hdf5_read_f64(const char *path, const char *dataset, double *out, i
                            int64_t *dims, int *ndims);
 rg_status rg_hdf5_attr_f64(const char *path, const char *object, const char *name, double *out);
 
+/* ---- W-stacking predict (degridding) ------------------------------------ */
+
+/* A separable kernel table: real values data[ov_index * size + tap] (the
+ * layout the reference's de-convolution indexes,
+ * src/wstack/wstack_common.h:460-478, from load_sep_kern /
+ * load_sep_kern_T, src/common/hdf5.c:372-497).  For a grid correction the
+ * size * oversampling entries sample one function on [-1/2, 1/2). */
+typedef struct rg_sepkern {
+    const double *data;
+    int size;
+    int oversampling;
+} rg_sepkern;
+
+/* Model visibilities of npoints unit point sources (points: l, m pairs) at
+ * (u, v, w) (wavelengths) by W-stacking: the quantised sky divided by the
+ * grid correction corr_lm(du l) corr_lm(du m) corr_n(dw n), padded to
+ * round(0.5 / x0) times floor(theta lambda) pixels, one FP64 FFT per w plane
+ * (planes every dw; ceil(sin(theta/2) sqrt(2) N / dw) + conv_w.size + 1 of
+ * them), then per visibility the separable conv_w x conv_uv^2 sum over the
+ * stack (du: the uv cell of the padded grid).  Replaces wstack_predict
+ * (src/wstack/predict.cpp:396-562) and wstack_predict_cu_3D
+ * (src/wstack/predict.cu:808-1081).  vis_out: 2*nvis doubles.  FP64.
+ * RG_ERR_INVALID_ARGUMENT for a source outside the image or a visibility
+ * whose taps leave the stack (the reference reads past its arrays). */
+rg_status rg_wstack_predict(rg_context *ctx, double theta, double lambda, const double *points, int npoints,
+                            const double *u, const double *v, const double *w, int64_t nvis, double du, double dw,
+                            double x0, const rg_sepkern *conv_uv, const rg_sepkern *conv_w,
+                            const rg_sepkern *corr_lm, const rg_sepkern *corr_n, double *vis_out);
+
 /* ---- w-kernel generator --------------------------------------------------- */
 
 /* An oversampled w-kernel table (rg_wkern layout: plane_count * ov * ov * size

@@ -79,6 +79,12 @@ def lib():
         L.rgo_image_from_grid.argtypes = [vp, i, vp]
         L.rgo_dft_image.argtypes = [vp, i, d, i64, vp, vp, vp, vp, d]
         L.rgo_dft_pixels.argtypes = [vp, i, vp, vp, i, d, i64, vp, vp, vp, vp, d]
+        L.rgo_wstack_planes.argtypes = [d, d, d, i]
+        L.rgo_wstack_planes.restype = i
+        L.rgo_wstack_predict.argtypes = [d, d, i, vp, i64, vp, vp, vp, d, d, d, vp, i, i, vp, i, i, vp, i, i,
+                                         vp, i, i, vp]
+        L.rgo_wstack_predict.restype = i
+        L.rgo_predict_dft_quantized.argtypes = [d, d, i, vp, i64, vp, vp, vp, vp]
         L.rgo_frac_coord.argtypes = [i, i, i, d, d, d, d, d, ct.POINTER(i), ct.POINTER(i)]
         _lib = L
     return _lib
@@ -172,6 +178,36 @@ def dft_pixels(grid_size, theta, u, v, w, vis, px, py, factor=2.0):
     out = np.zeros(len(px), np.float64)
     lib().rgo_dft_pixels(_ptr(out), len(px), _ptr(px), _ptr(py), grid_size, theta, len(u), _ptr(u), _ptr(v),
                          _ptr(w), _ptr(vis), factor)
+    return out
+
+
+def wstack_predict(theta, lam, points, u, v, w, du, dw, x0, conv_uv, conv_w, corr_lm, corr_n):
+    """src/wstack/predict.cpp:396-562.  points: [npts, 2] (l, m); each table
+    a 2-D float64 array [oversampling, size] (data[ov_index * size + tap])."""
+    u, v, w, _ = _flat(u, v, w, np.zeros(0))
+    pts = np.ascontiguousarray(points, np.float64).reshape(-1, 2)
+    tabs = [np.ascontiguousarray(t, np.float64) for t in (conv_uv, conv_w, corr_lm, corr_n)]
+    out = np.zeros(len(u), np.complex128)
+    args = []
+    for t in tabs:
+        args += [_ptr(t), t.shape[1], t.shape[0]]
+    st = lib().rgo_wstack_predict(theta, lam, len(pts), _ptr(pts), len(u), _ptr(u), _ptr(v), _ptr(w), du, dw, x0,
+                                  *args, _ptr(out))
+    if st != 0:
+        raise ValueError(f"wstack_predict oracle failed ({st})")
+    return out
+
+
+def wstack_planes(theta, lam, dw, support_w):
+    return lib().rgo_wstack_planes(theta, lam, dw, support_w)
+
+
+def predict_dft_quantized(theta, lam, points, u, v, w):
+    """src/wstack/predict.cpp:89-129."""
+    u, v, w, _ = _flat(u, v, w, np.zeros(0))
+    pts = np.ascontiguousarray(points, np.float64).reshape(-1, 2)
+    out = np.zeros(len(u), np.complex128)
+    lib().rgo_predict_dft_quantized(theta, lam, len(pts), _ptr(pts), len(u), _ptr(u), _ptr(v), _ptr(w), _ptr(out))
     return out
 
 

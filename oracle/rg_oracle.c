@@ -426,3 +426,152 @@ void rgo_dft_pixels(double *out, int npix, const int *px, const int *py, int gri
     for (int k = 0; k < npix; k++)
         out[k] = dft_pixel(px[k], py[k], grid_size, theta, nvis, u, v, w, vis, factor);
 }
+
+/* ------------------------------------------------------------------------
+ * W-stacking predict (degridding), src/wstack/predict.cpp:396-562 with the
+ * sky (:187-245), the Fresnel pattern (:152-183), the plane stepping
+ * (:248-273), the quadrant swap (:295-320) and the separable 3-D
+ * de-convolution of one visibility (src/wstack/wstack_common.h:423-484).
+ * Arrays are row-major [row][column]; the reference's (i, j) element access
+ * is column i of row j.  Separable tables: data[ov_index * size + tap].
+ * ------------------------------------------------------------------------ */
+
+/* fft_shift_2Darray, predict.cpp:295-320 (even sizes) */
+static void swap_quadrants(double complex *a, int n)
+{
+    for (int j = 0; j < n; j++)
+        for (int i = 0; i < n / 2; i++) {
+            int i1 = i + n / 2;
+            int j1 = j < n / 2 ? j + n / 2 : j - n / 2;
+            double complex t = a[(size_t)j * n + i];
+            a[(size_t)j * n + i] = a[(size_t)j1 * n + i1];
+            a[(size_t)j1 * n + i1] = t;
+        }
+}
+
+int rgo_wstack_planes(double theta, double lam, double dw, int support_w)
+{
+    int grid_size = (int)floor(theta * lam);
+    double max_w = sin(theta / 2) * sqrt(2 * (grid_size * grid_size));
+    return (int)ceil(max_w / dw) + support_w + 1;
+}
+
+int rgo_wstack_predict(double theta, double lam, int npts, const double *points, int64_t nvis,
+                       const double *u, const double *v, const double *w, double du, double dw, double x0,
+                       const double *conv_uv, int uv_size, int uv_ov, const double *conv_w, int w_size,
+                       int w_ov, const double *corr_lm, int lm_size, int lm_ov, const double *corr_n,
+                       int n_size, int n_ov, double complex *vis_out)
+{
+    const int N = (int)floor(theta * lam);
+    const double x0ih = round(0.5 / x0);
+    const int G = (int)(x0ih * N);
+    if (G <= N || G % 2) return 1;
+    const int gd = (G - N) / 2;
+    const int w_planes = rgo_wstack_planes(theta, lam, dw, w_size);
+    const size_t g2 = (size_t)G * G;
+
+    /* Fresnel pattern (predict.cpp:152-183) */
+    double complex *wtransfer = (double complex *)calloc(g2, sizeof(double complex));
+    for (int y = 0; y < N; y++)
+        for (int x = 0; x < N; x++) {
+            double l = theta * ((double)x - N / 2) / N;
+            double m = theta * ((double)y - N / 2) / N;
+            double ph = dw * (1.0 - sqrt(1.0 - l * l - m * m));
+            wtransfer[(size_t)(y + gd) * G + (x + gd)] = cexp(I * 2 * M_PI * ph);
+        }
+    /* the quantised sky over the grid correction (predict.cpp:187-245) */
+    double complex *sky = (double complex *)calloc(g2, sizeof(double complex));
+    const int lm_t = lm_size * lm_ov, n_t = n_size * n_ov;
+    const double lm_step = 1.0 / (double)lm_t, n_step = 1.0 / (double)n_t;
+    for (int i = 0; i < npts; i++) {
+        double l = points[2 * i], m = points[2 * i + 1];
+        int lc = (int)floor((l / theta + 0.5) * (double)N);
+        int mc = (int)floor((m / theta + 0.5) * (double)N);
+        double lq = (double)lc / lam - theta / 2;
+        double mq = (double)mc / lam - theta / 2;
+        double n = sqrt(1.0 - lq * lq - mq * mq) - 1.0;
+        int aau = (int)floor((du * lq) / lm_step) + lm_t / 2;
+        int aav = (int)floor((du * mq) / lm_step) + lm_t / 2;
+        int aaw = (int)floor((dw * n) / n_step) + n_t / 2;
+        if (aau < 0 || aau >= lm_t || aav < 0 || aav >= lm_t || aaw < 0 || aaw >= n_t) return 2;
+        if (gd + lc < 0 || gd + lc >= G || gd + mc < 0 || gd + mc >= G) return 2;
+        double a = 1.0;
+        a *= corr_lm[aau];
+        a *= corr_lm[aav];
+        a *= corr_n[aaw];
+        sky[(size_t)(gd + mc) * G + (gd + lc)] += 1.0 / a;
+    }
+    swap_quadrants(sky, G);
+    swap_quadrants(wtransfer, G);
+    /* to the first plane (predict.cpp:472: the pattern to the power
+     * floor(-w_planes / 2), skipping the zeros of the pattern) */
+    const int t0 = -w_planes / 2;
+    for (size_t k = 0; k < g2; k++) {
+        if (t0 == 1) sky[k] *= wtransfer[k];
+        else if (wtransfer[k] != 0) sky[k] *= cpow(wtransfer[k], (double)t0);
+    }
+    /* the planes (predict.cpp:480-491) */
+    double complex *stack = (double complex *)malloc(sizeof(double complex) * g2 * (size_t)w_planes);
+    for (int p = 0; p < w_planes; p++) {
+        double complex *plane = stack + g2 * (size_t)p;
+        rgo_fft2d(sky, plane, G, G, -1);
+        swap_quadrants(plane, G);
+        for (size_t k = 0; k < g2; k++) sky[k] *= wtransfer[k];
+    }
+    /* de-convolve each visibility (wstack_common.h:423-484) */
+    const int aa_h = uv_size / 2, aaw_h = w_size / 2;
+    int bad = 0;
+#pragma omp parallel for schedule(static, 1000) reduction(| : bad)
+    for (int64_t i = 0; i < nvis; i++) {
+        double complex acc = 0;
+        double flu = u[i] - ceil(u[i] / du) * du;
+        double flv = v[i] - ceil(v[i] / du) * du;
+        double flw = w[i] - ceil(w[i] / dw) * dw;
+        int ovu = (int)floor(fabs(flu) / du * uv_ov);
+        int ovv = (int)floor(fabs(flv) / du * uv_ov);
+        int ovw = (int)floor(fabs(flw) / dw * w_ov);
+        for (int dwi = -aaw_h; dwi < aaw_h; dwi++) {
+            int dws = (int)ceil(w[i] / dw) + w_planes / 2 + dwi;
+            double gw = conv_w[w_size * ovw + (dwi + aaw_h)];
+            for (int dvi = -aa_h; dvi < aa_h; dvi++) {
+                int dvs = (int)ceil(v[i] / du) + N + dvi;
+                double guv = gw * conv_uv[uv_size * ovv + (dvi + aa_h)];
+                for (int dui = -aa_h; dui < aa_h; dui++) {
+                    int dus = (int)ceil(u[i] / du) + N + dui;
+                    double g = guv * conv_uv[uv_size * ovu + (dui + aa_h)];
+                    if (dus < 0 || dus >= G || dvs < 0 || dvs >= G || dws < 0 || dws >= w_planes) {
+                        bad = 1;
+                        continue;
+                    }
+                    acc += stack[g2 * (size_t)dws + (size_t)dvs * G + dus] * g;
+                }
+            }
+        }
+        vis_out[i] = acc;
+    }
+    free(stack);
+    free(sky);
+    free(wtransfer);
+    return bad ? 3 : 0;
+}
+
+/* predict_visibility_quantized_vec, src/wstack/predict.cpp:89-129: the direct
+ * sum over the sources snapped to the image grid, unit amplitude. */
+void rgo_predict_dft_quantized(double theta, double lam, int npts, const double *points, int64_t nvis,
+                               const double *u, const double *v, const double *w, double complex *vis_out)
+{
+    const double grid_size = floor(theta * lam);
+#pragma omp parallel for schedule(static, 256)
+    for (int64_t k = 0; k < nvis; k++) {
+        double complex acc = 0;
+        for (int i = 0; i < npts; i++) {
+            double lc = floor((points[2 * i] / theta + 0.5) * grid_size);
+            double mc = floor((points[2 * i + 1] / theta + 0.5) * grid_size);
+            double lq = lc / lam - theta / 2;
+            double mq = mc / lam - theta / 2;
+            double n = sqrt(1.0 - lq * lq - mq * mq) - 1.0;
+            acc += cexp(-2 * M_PI * I * (u[k] * lq + v[k] * mq + w[k] * n));
+        }
+        vis_out[k] = acc;
+    }
+}

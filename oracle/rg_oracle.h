@@ -91,6 +91,23 @@ void rgo_dft_pixels(double *out, int npix, const int *px, const int *py, int gri
                     int64_t nvis, const double *u, const double *v, const double *w,
                     const double complex *vis, double factor);
 
+/* W-stacking predict, src/wstack/predict.cpp:396-562: visibilities of unit
+ * point sources at points[2k], points[2k+1] (l, m) from w-stacked planes of
+ * the quantised, grid-corrected sky and a separable 3-D de-convolution with
+ * the tables conv_uv / conv_w (data[ov_index * size + tap]) and the grid
+ * correction tables corr_lm / corr_n.  Returns 0, or 1 (x0 gives no padded
+ * grid), 2 (a source outside the grid or the correction tables), 3 (a
+ * visibility's taps outside the planes). */
+int rgo_wstack_planes(double theta, double lam, double dw, int support_w);
+int rgo_wstack_predict(double theta, double lam, int npts, const double *points, int64_t nvis,
+                       const double *u, const double *v, const double *w, double du, double dw, double x0,
+                       const double *conv_uv, int uv_size, int uv_ov, const double *conv_w, int w_size,
+                       int w_ov, const double *corr_lm, int lm_size, int lm_ov, const double *corr_n,
+                       int n_size, int n_ov, double complex *vis_out);
+/* predict_visibility_quantized_vec, src/wstack/predict.cpp:89-129. */
+void rgo_predict_dft_quantized(double theta, double lam, int npts, const double *points, int64_t nvis,
+                               const double *u, const double *v, const double *w, double complex *vis_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -46,8 +46,12 @@ EXPORTS = [
     "rg_free_wkern_data", "rg_write_vis_hdf5", "rg_write_vis_flat_hdf5", "rg_write_wkern_hdf5", "rg_hdf5_read_f64",
     "rg_hdf5_attr_f64", "rg_selftest_wait_timeout", "rg_wtowers_cuda_flat", "rg_wproj_cuda_flat",
     "rg_image_dft_host_flat", "rg_wtowers_tower_count", "rg_wtowers_tower_loads", "rg_wtowers_partition",
-    "rg_grid_wtowers_part", "rg_wkern_generate", "rg_pswf0",
+    "rg_grid_wtowers_part", "rg_wkern_generate", "rg_pswf0", "rg_wstack_predict",
 ]
+
+
+class _SepKern(ct.Structure):
+    _fields_ = [("data", ct.c_void_p), ("size", ct.c_int), ("oversampling", ct.c_int)]
 
 
 class RGError(RuntimeError):
@@ -112,6 +116,8 @@ def lib():
         L.rg_wtowers_partition.argtypes = [vp, vp, i, i, d, vp]
         L.rg_grid_wtowers_part.argtypes = [vp, vp, i, d, ct.POINTER(_Vis), ct.POINTER(_WKern), i, i, d, i, vp, i]
         L.rg_wkern_generate.argtypes = [vp, d, vp, i, i, i, d, i, vp]
+        L.rg_wstack_predict.argtypes = [vp, d, d, vp, i, vp, vp, vp, i64, d, d, d, ct.POINTER(_SepKern),
+                                        ct.POINTER(_SepKern), ct.POINTER(_SepKern), ct.POINTER(_SepKern), vp]
         L.rg_pswf0.argtypes = [d, vp, i64, vp]
         L.rg_grid_wtowers_batch.argtypes = [vp, i, ct.POINTER(vp), i, d, ct.POINTER(_Vis), ct.POINTER(_WKern),
                                             i, i, d, i]
@@ -286,6 +292,22 @@ class Context:
             out = np.empty((wp.size, oversampling, oversampling, size, size), np.complex128)
         _check(lib().rg_wkern_generate(self._h, float(theta), _ptr(wp), int(wp.size), int(size), int(oversampling),
                                        float(c), int(screen_pixels), _ptr(out)))
+        return out
+
+    def wstack_predict(self, theta, lam, points, u, v, w, du, dw, x0, conv_uv, conv_w, corr_lm, corr_n,
+                       out=None):
+        """rg_wstack_predict: complex128 visibilities of unit point sources
+        (points [npts, 2] l, m) at (u, v, w).  Each table is a 2-D float64
+        array [oversampling, size]."""
+        pts = np.ascontiguousarray(points, np.float64).reshape(-1, 2)
+        tabs = [np.ascontiguousarray(t, np.float64) for t in (conv_uv, conv_w, corr_lm, corr_n)]
+        ks = [_SepKern(_ptr(t), t.shape[1], t.shape[0]) for t in tabs]
+        n = int(u.shape[0]) if hasattr(u, "shape") else len(u)
+        if out is None:
+            out = np.zeros(n, np.complex128)
+        _check(lib().rg_wstack_predict(self._h, float(theta), float(lam), _ptr(pts), int(pts.shape[0]), _ptr(u),
+                                       _ptr(v), _ptr(w), n, float(du), float(dw), float(x0), ct.byref(ks[0]),
+                                       ct.byref(ks[1]), ct.byref(ks[2]), ct.byref(ks[3]), _ptr(out)))
         return out
 
     # ---- one observation's towers over several GPUs ----

@@ -114,13 +114,7 @@ static rg_status check_launch(const char *what)
     return RG_OK;
 }
 
-// Device error word + counters in one small scratch area.
-struct Diag {
-    unsigned *err;
-    unsigned long long *counters;  // [0] gridded, [1] dropped
-};
-
-static rg_status diag_begin(rg_context *ctx, Diag *d)
+rg_status diag_begin(rg_context *ctx, Diag *d)
 {
     void *p = nullptr;
     RG_CHECK(scratch(ctx, "diag", 64, &p));
@@ -130,7 +124,7 @@ static rg_status diag_begin(rg_context *ctx, Diag *d)
     return RG_OK;
 }
 
-static rg_status diag_end(rg_context *ctx, const Diag &d, unsigned long long *counters_out)
+rg_status diag_end(rg_context *ctx, const Diag &d, unsigned long long *counters_out)
 {
     unsigned char host[64];
     RG_CUDA(cudaMemcpyAsync(host, d.err, 64, cudaMemcpyDeviceToHost, ctx->stream));

@@ -153,6 +153,16 @@ struct OutView {
     bool host = false;
 };
 rg_status out_view(rg_context *ctx, void *ptr, size_t bytes, const char *name, bool load, OutView *ov);
+
+// Device error word + counters in one small scratch area: diag_begin zeroes
+// it on the context stream; diag_end reads it back (synchronising) and turns
+// the error bits into a status.
+struct Diag {
+    unsigned *err;
+    unsigned long long *counters;  // [0] gridded, [1] dropped
+};
+rg_status diag_begin(rg_context *ctx, Diag *d);
+rg_status diag_end(rg_context *ctx, const Diag &d, unsigned long long *counters_out);
 rg_status finish_out(rg_context *ctx, const OutView &ov);
 
 // ---------------------------------------------------------------------------

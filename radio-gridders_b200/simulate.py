@@ -461,3 +461,41 @@ def learned_training_set(n_triples: int, wmax: float, theta: float, size: int = 
     return (np.repeat(w, rep), np.repeat(du, rep), np.repeat(dv, rep),
             np.tile(tx.ravel(), n_triples).astype(np.float64),
             np.tile(ty.ravel(), n_triples).astype(np.float64), out.reshape(-1))
+
+
+# ----------------------------------------------------------------------------
+# Separable kernels for W-stacking predict
+# ----------------------------------------------------------------------------
+
+def sepkern_pswf(support: int, oversampling: int, x0: float = 0.25, c: float | None = None,
+                 corr_size: int = 64, corr_oversampling: int = 64):
+    """A separable gridding kernel and its grid correction in the table
+    layouts the W-stacking predict indexes (src/wstack/wstack_common.h:460-478
+    for the convolution, src/wstack/predict.cpp:219-234 for the correction):
+
+    * conv[j, t] = C(t - support/2 + (j + 1/2)/oversampling), C(x) =
+      psi_0(c, 2x/support) on |x| <= support/2: the predict maps a visibility
+      f of a cell before its first grid point (0 <= f < 1) to j = floor(f ov),
+      so row j holds the kernel at the middle of [j/ov, (j+1)/ov);
+    * corr[k] = C^(nu_k), nu_k = (k - T/2) / T, T = corr_size * corr_oversampling:
+      the kernel's continuous Fourier transform (what the gridded sky is
+      divided by), by Simpson quadrature.
+
+    The reference reads Sze-Tan kernels from HDF5 files instead
+    (load_sep_kern, src/common/hdf5.c:372-497); this is a PSWF stand-in with
+    the same meaning, c = 3 pi support x0 by default."""
+    if c is None:
+        c = 3.0 * math.pi * support * x0
+    ov = oversampling
+    t = np.arange(support)[None, :] - support // 2 + (np.arange(ov)[:, None] + 0.5) / ov
+    conv = np.where(np.abs(t) <= support / 2, pswf0(c, np.clip(2.0 * t / support, -1.0, 1.0)), 0.0)
+    T = corr_size * corr_oversampling
+    nu = (np.arange(T) - T // 2) / T
+    xq = np.linspace(0.0, support / 2, 4001)
+    cq = pswf0(c, 2.0 * xq / support)
+    wq = np.full(xq.size, 2.0)
+    wq[1::2] = 4.0
+    wq[0] = wq[-1] = 1.0
+    wq *= (xq[1] - xq[0]) / 3.0
+    corr = 2.0 * (np.cos(2 * np.pi * np.outer(nu, xq)) * (cq * wq)[None, :]).sum(axis=1)
+    return np.ascontiguousarray(conv), np.ascontiguousarray(corr.reshape(corr_oversampling, corr_size))
