@@ -330,6 +330,68 @@ rg_status rg_hdf5_read_f64(const char *path, const char *dataset, double *out, i
                            int64_t *dims, int *ndims);
 rg_status rg_hdf5_attr_f64(const char *path, const char *object, const char *name, double *out);
 
+/* ---- AW-projection ------------------------------------------------------ */
+
+/* Hierarchical visibilities (the reference's struct vis_data,
+ * src/reference/grid.h:7-30, with every baseline holding time_count times and
+ * freq_count channels): antenna1/antenna2 [bl], time [bl][time] (the file's
+ * time unit), freq [bl][freq] Hz, uvw [bl][time][3] metres, vis
+ * [bl][time][freq] complex interleaved. */
+typedef struct rg_vis_bl {
+    int bl_count, time_count, freq_count;
+    const int32_t *antenna1, *antenna2;
+    const double *time, *freq, *uvw, *vis;
+} rg_vis_bl;
+
+/* A-kernels per (antenna, time slot, channel) on evenly spaced axes
+ * t_min + i t_step, f_min + j f_step (struct a_kernel_data,
+ * src/reference/grid.h:69-85, as load_akern indexes it: kern_by_atf,
+ * src/common/hdf5.c:775-818): freq and time [ant][t][f] are each slot's own
+ * kernel frequency (Hz) and time, data [ant][t][f][size_y][size_x] complex. */
+typedef struct rg_akern {
+    int antenna_count, time_count, freq_count, size_x, size_y;
+    double t_min, t_step, f_min, f_step;
+    const double *freq, *time, *data;
+} rg_akern;
+
+/* AW-projection: grid_awprojection after convolve_aw_kernels
+ * (src/reference/grid.c:557-637) for baselines [bl_min, bl_max).  Each
+ * visibility is gridded like W-projection (rg_grid_wprojection) with the
+ * w-kernel plane nearest to uvw_w * f_A / c, f_A the frequency of antenna 1's
+ * A-kernel for the visibility's time slot and nearest channel; the A x W
+ * convolution is the reference's placeholder (it copies the w-kernel,
+ * grid.c:583-590), so the A-kernel values are not used.  Sizes of both
+ * kernel tables must agree (grid.c:562-563).  Every array of vis except
+ * vis->vis, and akern->freq, must be host memory; a time or channel outside
+ * the A-kernel axes or an antenna without kernels returns
+ * RG_ERR_INVALID_ARGUMENT (the reference indexes past its tables). */
+rg_status rg_grid_awprojection(rg_context *ctx, double *uvgrid, int grid_size, double theta, const rg_vis_bl *vis,
+                               const rg_wkern *wkern, const rg_akern *akern, int bl_min, int bl_max, int flags);
+
+/* Owned forms read from files (released with the matching free). */
+typedef struct rg_vis_bl_data {
+    int bl_count, time_count, freq_count;
+    int32_t *antenna1, *antenna2;
+    double *time, *freq, *uvw, *vis;
+} rg_vis_bl_data;
+typedef struct rg_akern_data {
+    int antenna_count, time_count, freq_count, size_x, size_y;
+    double t_min, t_step, f_min, f_step;
+    double *freq, *time, *data;
+} rg_akern_data;
+/* Hierarchical visibilities of a crocodile file (either layout), baselines
+ * whose first uvw sample has length in [bl_min, bl_max) metres; every
+ * baseline must have the same time and channel counts (else
+ * RG_ERR_UNSUPPORTED).  Replaces load_vis (src/reference/hdf5.c:173-318). */
+rg_status rg_read_vis_bl_hdf5(const char *path, double bl_min, double bl_max, rg_vis_bl_data *out);
+void rg_free_vis_bl_data(rg_vis_bl_data *d);
+/* Replaces load_akern (src/common/hdf5.c:652-820): group akern/<theta %g>,
+ * children <antenna>/<time>/<freq>/kern [size_y][size_x] complex; evenly
+ * spaced axes from the extremes, each slot the antenna's nearest kernel. */
+rg_status rg_read_akern_hdf5(const char *path, double theta, rg_akern_data *out);
+void rg_free_akern_data(rg_akern_data *d);
+rg_status rg_write_akern_hdf5(const char *path, double theta, const rg_akern *ak);
+
 /* ---- W-stacking predict (degridding) ------------------------------------ */
 
 /* A separable kernel table: real values data[ov_index * size + tap] (the

@@ -85,6 +85,9 @@ def lib():
                                          vp, i, i, vp]
         L.rgo_wstack_predict.restype = i
         L.rgo_predict_dft_quantized.argtypes = [d, d, i, vp, i64, vp, vp, vp, vp]
+        L.rgo_grid_awprojection.argtypes = [vp, i, d, i, i, i, i, vp, vp, vp, vp, vp, ct.POINTER(_Wk), i, i, i,
+                                            d, d, d, d, vp]
+        L.rgo_grid_awprojection.restype = i
         L.rgo_frac_coord.argtypes = [i, i, i, d, d, d, d, d, ct.POINTER(i), ct.POINTER(i)]
         _lib = L
     return _lib
@@ -211,6 +214,29 @@ def predict_dft_quantized(theta, lam, points, u, v, w):
     return out
 
 
+def grid_awprojection(grid_size, theta, hv, wk, ak, bl_min=0, bl_max=None):
+    """src/reference/grid.c:557-637 restated (convolve_aw_kernels +
+    grid_awprojection).  hv: HierVis-like (antenna1, time [bl, nt], freq
+    [bl, nf], uvw, vis); ak: AKernels-like (freq [ant, nt, nf], axes)."""
+    nbl, nt = hv.uvw.shape[:2]
+    nf = hv.freq.shape[1]
+    a1 = np.ascontiguousarray(hv.antenna1, np.int32)
+    tm = np.ascontiguousarray(np.broadcast_to(np.asarray(hv.time, np.float64), (nbl, nt)))
+    fr = np.ascontiguousarray(hv.freq, np.float64)
+    uvw = np.ascontiguousarray(hv.uvw, np.float64)
+    vis = np.ascontiguousarray(hv.vis, np.complex128)
+    akf = np.ascontiguousarray(ak.freq, np.float64)
+    grid = np.zeros((grid_size, grid_size), np.complex128)
+    s, keep = _wk_struct(wk)
+    st = lib().rgo_grid_awprojection(_ptr(grid), grid_size, theta, bl_min, nbl if bl_max is None else bl_max, nt, nf,
+                                     _ptr(a1), _ptr(tm), _ptr(fr), _ptr(uvw), _ptr(vis), ct.byref(s),
+                                     akf.shape[0], akf.shape[1], akf.shape[2], ak.t_min, ak.t_step, ak.f_min,
+                                     ak.f_step, _ptr(akf))
+    if st != 0:
+        raise ValueError("AW-projection oracle: an index leaves its table")
+    return grid
+
+
 def frac_coord(grid_size, ksize, ov, theta, u, v, du=0.0, dv=0.0):
     go, so = ct.c_int(), ct.c_int()
     lib().rgo_frac_coord(grid_size, ksize, ov, theta, u, v, du, dv, ct.byref(go), ct.byref(so))
@@ -248,6 +274,18 @@ class WKernData(ct.Structure):
                 ("kern_by_w", ct.POINTER(WKern)), ("w_min", ct.c_double),
                 ("w_max", ct.c_double), ("w_step", ct.c_double),
                 ("size_x", ct.c_int), ("size_y", ct.c_int), ("oversampling", ct.c_int)]
+
+
+class AKernelC(ct.Structure):  # struct a_kernel, src/reference/grid.h:70-76
+    _fields_ = [("data", ct.c_void_p), ("antenna", ct.c_int), ("time", ct.c_double), ("freq", ct.c_double)]
+
+
+class AKernelData(ct.Structure):  # struct a_kernel_data, src/reference/grid.h:77-85
+    _fields_ = [("antenna_count", ct.c_int), ("time_count", ct.c_int), ("freq_count", ct.c_int),
+                ("kern", ct.POINTER(AKernelC)), ("kern_by_atf", ct.POINTER(AKernelC)),
+                ("t_min", ct.c_double), ("t_max", ct.c_double), ("t_step", ct.c_double),
+                ("f_min", ct.c_double), ("f_max", ct.c_double), ("f_step", ct.c_double),
+                ("size_x", ct.c_int), ("size_y", ct.c_int)]
 
 
 _ref_libs = {}
@@ -293,6 +331,10 @@ def ref_lib(omp=False):
         L.grid_wtowers.restype = ct.c_uint64
         L.weight.argtypes = [vp, ct.c_int, ct.c_double, ct.POINTER(VisData)]
         L.make_hermitian.argtypes = [vp, ct.c_int]
+        L.convolve_aw_kernels.argtypes = [ct.POINTER(BlData), ct.POINTER(WKernData), ct.POINTER(AKernelData)]
+        L.grid_awprojection.argtypes = [vp, ct.c_int, ct.c_double, ct.POINTER(VisData), ct.POINTER(WKernData),
+                                        ct.POINTER(AKernelData), ct.c_int, ct.c_int]
+        L.grid_awprojection.restype = ct.c_uint64
         L.fft_shift.argtypes = [vp, ct.c_int]
         _ref_libs[name] = L
     return _ref_libs[name]
@@ -360,6 +402,36 @@ def ref_grid_wtowers(grid_size, theta, obs, wk, subgrid, margin, winc, omp=False
     with quiet_stdout():
         ref_lib(omp).grid_wtowers(_ptr(grid), grid_size, theta, ct.byref(r.vd), ct.byref(r.wkd),
                                   subgrid, margin, winc)
+    return grid
+
+
+def ref_grid_awprojection(grid_size, theta, obs, wk, ak):
+    """The reference's convolve_aw_kernels for every baseline, then its
+    grid_awprojection (src/reference/grid.c:557-637), on an Observation and
+    an AKernels-like table."""
+    r = RefInputs(obs, wk)
+    a, t, f = ak.freq.shape
+    slots = (AKernelC * (a * t * f))()
+    zeros = np.zeros(wk.size * wk.size, np.complex128)  # the reference never reads the A-kernel values
+    for ai in range(a):
+        for ti in range(t):
+            for fi in range(f):
+                k = slots[(ai * t + ti) * f + fi]
+                k.data = zeros.ctypes.data
+                k.antenna, k.time, k.freq = ai, float(ak.time[ai, ti, fi]), float(ak.freq[ai, ti, fi])
+    akd = AKernelData(a, t, f, slots, slots, ak.t_min, ak.t_min + (t - 1) * ak.t_step, ak.t_step,
+                      ak.f_min, ak.f_min + (f - 1) * ak.f_step, ak.f_step, wk.size, wk.size)
+    L = ref_lib()
+    for b in range(r.vd.bl_count):
+        L.convolve_aw_kernels(ct.byref(r.bl[b]), ct.byref(r.wkd), ct.byref(akd))
+    grid = np.zeros((grid_size, grid_size), np.complex128)
+    L.grid_awprojection(_ptr(grid), grid_size, theta, ct.byref(r.vd), ct.byref(r.wkd), ct.byref(akd), 0,
+                        r.vd.bl_count)
+    libc = ct.CDLL(None)
+    libc.free.argtypes = [ct.c_void_p]
+    for b in range(r.vd.bl_count):  # the kernels convolve_aw_kernels allocated
+        libc.free(r.bl[b].awkern)
+        r.bl[b].awkern = None
     return grid
 
 

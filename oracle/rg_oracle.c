@@ -575,3 +575,69 @@ void rgo_predict_dft_quantized(double theta, double lam, int npts, const double 
         vis_out[k] = acc;
     }
 }
+
+/* ------------------------------------------------------------------------
+ * AW-projection, src/reference/grid.c:557-637: convolve_aw_kernels picks, per
+ * baseline, time and A-kernel frequency channel, the w-plane nearest to
+ * w = uvw_w * f_A / c with f_A the frequency of antenna 1's A-kernel for that
+ * time and channel (and copies that w-kernel: the A-kernel convolution is a
+ * placeholder there, :583-590); grid_awprojection grids each visibility with
+ * the kernel of its nearest A-kernel channel.  Baselines [bl_min, bl_max) of
+ * arrays with uniform time and frequency counts: antenna1 [bl], time
+ * [bl][nt], freq [bl][nf], uvw [bl][nt][3] metres, vis [bl][nt][nf];
+ * akern_freq [ant][at][af].  Returns 0, or 1 when an index leaves its table.
+ * ------------------------------------------------------------------------ */
+int rgo_grid_awprojection(double complex *uvgrid, int grid_size, double theta, int bl_min, int bl_max,
+                          int nt, int nf, const int32_t *antenna1, const double *time, const double *freq,
+                          const double *uvw, const double complex *vis, const rgo_wkern *wk, int ak_ant,
+                          int ak_time, int ak_freq, double t_min, double t_step, double f_min, double f_step,
+                          const double *akern_freq)
+{
+    const double c = 299792458.0; /* grid.c:19 */
+    const int ks = wk->size, ov = wk->oversampling;
+    int *plane_of = (int *)malloc(sizeof(int) * (size_t)nt * ak_freq);
+    for (int bl = bl_min; bl < bl_max; bl++) {
+        const double *bt = time + (size_t)bl * nt, *bf = freq + (size_t)bl * nf;
+        const double *bu = uvw + (size_t)bl * nt * 3;
+        for (int t = 0; t < nt; t++)
+            for (int af = 0; af < ak_freq; af++) {
+                int atime = (int)floor((bt[t] - t_min) / t_step + .5);
+                if (antenna1[bl] < 0 || antenna1[bl] >= ak_ant || atime < 0 || atime >= ak_time) {
+                    free(plane_of);
+                    return 1;
+                }
+                int a1i = antenna1[bl] * ak_time * ak_freq + atime * ak_freq + af;
+                double w = bu[t * 3 + 2] * akern_freq[a1i] / c;
+                int w_plane = (int)floor((w - wk->w_min) / wk->w_step + .5);
+                if (w_plane < 0 || w_plane >= wk->plane_count) {
+                    free(plane_of);
+                    return 1;
+                }
+                plane_of[t * ak_freq + af] = w_plane;
+            }
+        for (int t = 0; t < nt; t++)
+            for (int f = 0; f < nf; f++) {
+                double u = bu[t * 3 + 0] * bf[f] / c; /* uvw_lambda, grid.c:21-24 */
+                double v = bu[t * 3 + 1] * bf[f] / c;
+                int goff, soff;
+                rgo_frac_coord(grid_size, ks, ov, theta, u, v, 0, 0, &goff, &soff);
+                int afreq = (int)floor((bf[f] - f_min) / f_step + .5);
+                if (afreq < 0 || afreq >= ak_freq) {
+                    free(plane_of);
+                    return 1;
+                }
+                const double complex *awk =
+                    wk->data + (size_t)plane_of[t * ak_freq + afreq] * ov * ov * ks * ks;
+                double complex vv = vis[((size_t)bl * nt + t) * nf + f];
+                const long long limit = (long long)grid_size * grid_size;
+                for (int y = 0; y < ks; y++)
+                    for (int x = 0; x < ks; x++) {
+                        long long idx = (long long)goff + (long long)y * grid_size + x;
+                        if (idx < 0 || idx >= limit) continue;
+                        uvgrid[idx] += vv * conj(awk[soff + y * ks + x]);
+                    }
+            }
+    }
+    free(plane_of);
+    return 0;
+}

@@ -108,6 +108,14 @@ int rgo_wstack_predict(double theta, double lam, int npts, const double *points,
 void rgo_predict_dft_quantized(double theta, double lam, int npts, const double *points, int64_t nvis,
                                const double *u, const double *v, const double *w, double complex *vis_out);
 
+/* AW-projection, src/reference/grid.c:557-637 (convolve_aw_kernels +
+ * grid_awprojection) on uniform hierarchical arrays; see rg_oracle.c. */
+int rgo_grid_awprojection(double complex *uvgrid, int grid_size, double theta, int bl_min, int bl_max,
+                          int nt, int nf, const int32_t *antenna1, const double *time, const double *freq,
+                          const double *uvw, const double complex *vis, const rgo_wkern *wk, int ak_ant,
+                          int ak_time, int ak_freq, double t_min, double t_step, double f_min, double f_step,
+                          const double *akern_freq);
+
 #ifdef __cplusplus
 }
 #endif

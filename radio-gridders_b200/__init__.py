@@ -46,7 +46,9 @@ EXPORTS = [
     "rg_free_wkern_data", "rg_write_vis_hdf5", "rg_write_vis_flat_hdf5", "rg_write_wkern_hdf5", "rg_hdf5_read_f64",
     "rg_hdf5_attr_f64", "rg_selftest_wait_timeout", "rg_wtowers_cuda_flat", "rg_wproj_cuda_flat",
     "rg_image_dft_host_flat", "rg_wtowers_tower_count", "rg_wtowers_tower_loads", "rg_wtowers_partition",
-    "rg_grid_wtowers_part", "rg_wkern_generate", "rg_pswf0", "rg_wstack_predict",
+    "rg_grid_wtowers_part", "rg_wkern_generate", "rg_pswf0", "rg_wstack_predict", "rg_grid_awprojection",
+    "rg_read_vis_bl_hdf5", "rg_free_vis_bl_data", "rg_read_akern_hdf5", "rg_free_akern_data",
+    "rg_write_akern_hdf5",
 ]
 
 
@@ -86,6 +88,63 @@ class _WKernData(ct.Structure):
                 ("oversampling", ct.c_int), ("w_min", ct.c_double), ("w_step", ct.c_double)]
 
 
+_dp = ct.POINTER(ct.c_double)
+
+
+class _VisBL(ct.Structure):
+    _fields_ = [("bl_count", ct.c_int), ("time_count", ct.c_int), ("freq_count", ct.c_int),
+                ("antenna1", ct.POINTER(ct.c_int32)), ("antenna2", ct.POINTER(ct.c_int32)),
+                ("time", _dp), ("freq", _dp), ("uvw", _dp), ("vis", _dp)]
+
+
+class _AKern(ct.Structure):
+    _fields_ = [("antenna_count", ct.c_int), ("time_count", ct.c_int), ("freq_count", ct.c_int),
+                ("size_x", ct.c_int), ("size_y", ct.c_int), ("t_min", ct.c_double), ("t_step", ct.c_double),
+                ("f_min", ct.c_double), ("f_step", ct.c_double), ("freq", _dp), ("time", _dp), ("data", _dp)]
+
+
+class HierVis:
+    """Hierarchical visibilities (rg_vis_bl): antenna1/antenna2 [bl], time
+    [bl, nt] (or [nt], shared), freq [bl, nf] Hz, uvw [bl, nt, 3] metres, vis
+    [bl, nt, nf] complex."""
+
+    def __init__(self, antenna1, antenna2, time, freq, uvw, vis):
+        self.uvw = np.ascontiguousarray(uvw, np.float64)
+        nbl, nt = self.uvw.shape[:2]
+        self.antenna1 = np.ascontiguousarray(antenna1, np.int32)
+        self.antenna2 = np.ascontiguousarray(antenna2, np.int32)
+        self.time = np.ascontiguousarray(np.broadcast_to(np.asarray(time, np.float64), (nbl, nt)))
+        self.freq = np.ascontiguousarray(freq, np.float64)
+        self.vis = np.ascontiguousarray(vis, np.complex128)
+
+    @classmethod
+    def of(cls, obs):
+        return cls(obs.antenna1, obs.antenna2, obs.time, obs.freq, obs.uvw, obs.vis)
+
+    def struct(self):
+        nbl, nt = self.uvw.shape[:2]
+        return _VisBL(nbl, nt, self.freq.shape[1], self.antenna1.ctypes.data_as(ct.POINTER(ct.c_int32)),
+                      self.antenna2.ctypes.data_as(ct.POINTER(ct.c_int32)), self.time.ctypes.data_as(_dp),
+                      self.freq.ctypes.data_as(_dp), self.uvw.ctypes.data_as(_dp), self.vis.ctypes.data_as(_dp))
+
+
+class AKernels:
+    """A-kernel table (rg_akern): freq, time [ant, nt, nf], data [ant, nt, nf,
+    size_y, size_x] complex, evenly spaced axes t_min + i t_step,
+    f_min + j f_step."""
+
+    def __init__(self, freq, time, data, t_min, t_step, f_min, f_step):
+        self.freq = np.ascontiguousarray(freq, np.float64)
+        self.time = np.ascontiguousarray(time, np.float64)
+        self.data = np.ascontiguousarray(data, np.complex128)
+        self.t_min, self.t_step, self.f_min, self.f_step = float(t_min), float(t_step), float(f_min), float(f_step)
+
+    def struct(self):
+        a, t, f, sy, sx = self.data.shape
+        return _AKern(a, t, f, sx, sy, self.t_min, self.t_step, self.f_min, self.f_step,
+                      self.freq.ctypes.data_as(_dp), self.time.ctypes.data_as(_dp), self.data.ctypes.data_as(_dp))
+
+
 _lib = None
 
 
@@ -116,6 +175,13 @@ def lib():
         L.rg_wtowers_partition.argtypes = [vp, vp, i, i, d, vp]
         L.rg_grid_wtowers_part.argtypes = [vp, vp, i, d, ct.POINTER(_Vis), ct.POINTER(_WKern), i, i, d, i, vp, i]
         L.rg_wkern_generate.argtypes = [vp, d, vp, i, i, i, d, i, vp]
+        L.rg_grid_awprojection.argtypes = [vp, vp, i, d, ct.POINTER(_VisBL), ct.POINTER(_WKern), ct.POINTER(_AKern),
+                                           i, i, i]
+        L.rg_read_vis_bl_hdf5.argtypes = [ct.c_char_p, d, d, ct.POINTER(_VisBL)]
+        L.rg_free_vis_bl_data.argtypes = [ct.POINTER(_VisBL)]
+        L.rg_read_akern_hdf5.argtypes = [ct.c_char_p, d, ct.POINTER(_AKern)]
+        L.rg_free_akern_data.argtypes = [ct.POINTER(_AKern)]
+        L.rg_write_akern_hdf5.argtypes = [ct.c_char_p, d, ct.POINTER(_AKern)]
         L.rg_wstack_predict.argtypes = [vp, d, d, vp, i, vp, vp, vp, i64, d, d, d, ct.POINTER(_SepKern),
                                         ct.POINTER(_SepKern), ct.POINTER(_SepKern), ct.POINTER(_SepKern), vp]
         L.rg_pswf0.argtypes = [d, vp, i64, vp]
@@ -309,6 +375,17 @@ class Context:
                                        _ptr(v), _ptr(w), n, float(du), float(dw), float(x0), ct.byref(ks[0]),
                                        ct.byref(ks[1]), ct.byref(ks[2]), ct.byref(ks[3]), _ptr(out)))
         return out
+
+    def grid_awprojection(self, uvgrid, grid_size, theta, hv: "HierVis", wkern, akern: "AKernels", bl_min=0,
+                          bl_max=None, flags=RG_GRID_ACCUMULATE):
+        """rg_grid_awprojection (grid_awprojection, src/reference/grid.c:595-637)."""
+        s, keep = _wkern_struct(wkern, None)
+        vb, ak = hv.struct(), akern.struct()
+        nbl = hv.uvw.shape[0]
+        _check(lib().rg_grid_awprojection(self._h, _ptr(uvgrid), int(grid_size), float(theta), ct.byref(vb),
+                                          ct.byref(s), ct.byref(ak), int(bl_min), int(nbl if bl_max is None else bl_max),
+                                          int(flags)))
+        return uvgrid
 
     # ---- one observation's towers over several GPUs ----
     def tower_loads(self, grid_size, theta, vis: Visibilities, subgrid_size, subgrid_margin, wincrement):
@@ -624,6 +701,44 @@ def write_wkern_hdf5(path, theta, wkern):
     st, keep = _wkern_struct(wkern)
     _check(lib().rg_write_wkern_hdf5(os.fsencode(path), float(theta), ct.byref(st)))
     del keep
+
+
+def read_vis_bl_hdf5(path, bl_min=0.0, bl_max=float("inf")):
+    """Hierarchical visibilities of a crocodile file (rg_read_vis_bl_hdf5)."""
+    L, d = lib(), _VisBL()
+    _check(L.rg_read_vis_bl_hdf5(os.fsencode(path), float(bl_min), float(min(bl_max, 1.7976931348623157e308)),
+                                 ct.byref(d)))
+    try:
+        nb, nt, nf = int(d.bl_count), int(d.time_count), int(d.freq_count)
+
+        def take(p, k, dt=np.float64):
+            return np.ctypeslib.as_array(p, shape=(k,)).copy() if k else np.zeros(0, dt)
+        return HierVis(take(d.antenna1, nb, np.int32), take(d.antenna2, nb, np.int32),
+                       take(d.time, nb * nt).reshape(nb, nt), take(d.freq, nb * nf).reshape(nb, nf),
+                       take(d.uvw, nb * nt * 3).reshape(nb, nt, 3),
+                       take(d.vis, 2 * nb * nt * nf).view(np.complex128).reshape(nb, nt, nf))
+    finally:
+        L.rg_free_vis_bl_data(ct.byref(d))
+
+
+def read_akern_hdf5(path, theta):
+    """The A-kernel table of a crocodile A-kernel file (rg_read_akern_hdf5)."""
+    L, d = lib(), _AKern()
+    _check(L.rg_read_akern_hdf5(os.fsencode(path), float(theta), ct.byref(d)))
+    try:
+        a, t, f, sy, sx = d.antenna_count, d.time_count, d.freq_count, d.size_y, d.size_x
+        k = a * t * f
+        data = np.ctypeslib.as_array(d.data, shape=(2 * k * sy * sx,)).copy().view(np.complex128)
+        return AKernels(np.ctypeslib.as_array(d.freq, shape=(k,)).copy().reshape(a, t, f),
+                        np.ctypeslib.as_array(d.time, shape=(k,)).copy().reshape(a, t, f),
+                        data.reshape(a, t, f, sy, sx), d.t_min, d.t_step, d.f_min, d.f_step)
+    finally:
+        L.rg_free_akern_data(ct.byref(d))
+
+
+def write_akern_hdf5(path, theta, akern: AKernels):
+    st = akern.struct()
+    _check(lib().rg_write_akern_hdf5(os.fsencode(path), float(theta), ct.byref(st)))
 
 
 def hdf5_read(path, dataset):

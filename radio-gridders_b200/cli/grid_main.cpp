@@ -37,6 +37,7 @@ static void help()
         "\t-device              GPU Device to use (Default: 0)\n"
         "\t-grid                uv grid output file (complex128, after make_hermitian)\n"
         "\t-weight              uniform weighting before gridding\n"
+        "\t-akern               A-kernel file: AW-projection with -wkernel (src/reference/main.c:32)\n"
         "\t-learned             learned w-kernel parameter file (float32, W-projection)\n"
         "\t-learned_ksize       learned kernel support (Default: 16)\n"
         "\t-learned_wmax        learned kernel w range it was trained on (Default: 2000)\n"
@@ -47,6 +48,33 @@ static int die(const char *what)
 {
     std::fprintf(stderr, "%s: %s\n", what, rg_last_error());
     return 1;
+}
+
+// Timing line, then the hermitian uv grid (-grid) and the dirty image (-image)
+// as raw float64 (src/reference/main.c:258-294).
+static int write_outputs(rg_context *ctx, std::vector<double> &grid, int N, const std::string &gridfile,
+                         const std::string &image)
+{
+    const char *names[64];
+    float ms[64];
+    const int nt = rg_last_timings(ctx, names, ms, 64);
+    float total = 0;
+    for (int i = 0; i < nt; i++) total += ms[i];
+    std::printf("Gridder Elapsed Time: %.6f seconds\n", total / 1000.0);
+    if (!gridfile.empty()) {
+        std::vector<double> h = grid;
+        if (rg_make_hermitian(ctx, h.data(), N) != RG_OK) return die("make_hermitian");
+        std::ofstream f(gridfile, std::ios::binary);
+        f.write((const char *)h.data(), (std::streamsize)(h.size() * sizeof(double)));
+    }
+    if (!image.empty()) {
+        std::vector<double> img((size_t)N * N);
+        if (rg_image_from_grid(ctx, grid.data(), N, img.data(), nullptr) != RG_OK) return die("image");
+        std::printf("Writing Image to File... \n");
+        std::ofstream f(image, std::ios::binary);
+        f.write((const char *)img.data(), (std::streamsize)(img.size() * sizeof(double)));
+    }
+    return 0;
 }
 
 int main(int argc, char **argv)
@@ -99,6 +127,52 @@ int main(int argc, char **argv)
 
     rg_context *ctx;
     if (rg_context_create(device, &ctx) != RG_OK) return die("context");
+    std::string akfile;
+    if (value(argc, argv, "akern", &akfile) && !wkfile.empty()) {
+        // AW-projection (src/reference/main.c:207-233): hierarchical
+        // visibilities, A-kernel channel frequencies pick the w-planes
+        rg_vis_bl_data hd;
+        if (rg_read_vis_bl_hdf5(visfile.c_str(), bl_min, bl_max, &hd) != RG_OK) return die("visibilities");
+        std::printf("Have %d baselines and %lld visibilities\n", hd.bl_count,
+                    (long long)hd.bl_count * hd.time_count * hd.freq_count);
+        rg_wkern_data wd;
+        if (rg_read_wkern_hdf5(wkfile.c_str(), theta, &wd) != RG_OK) return die("w-kernels");
+        rg_akern_data ad;
+        if (rg_read_akern_hdf5(akfile.c_str(), theta, &ad) != RG_OK) return die("A-kernels");
+        const int64_t nv = (int64_t)hd.bl_count * hd.time_count * hd.freq_count;
+        if (has(argc, argv, "weight") && nv > 0) {  // main.c:153, on the same visibility order
+            std::vector<double> u(nv), v(nv), w(nv);
+            int64_t k = 0;
+            for (int b = 0; b < hd.bl_count; b++)
+                for (int t = 0; t < hd.time_count; t++)
+                    for (int f = 0; f < hd.freq_count; f++, k++) {
+                        const double *uvw = hd.uvw + ((size_t)b * hd.time_count + t) * 3;
+                        const double fr = hd.freq[(size_t)b * hd.freq_count + f];
+                        u[k] = uvw[0] * fr / 299792458.0;
+                        v[k] = uvw[1] * fr / 299792458.0;
+                        w[k] = uvw[2] * fr / 299792458.0;
+                    }
+            rg_vis fv = {u.data(), v.data(), w.data(), hd.vis, nv};
+            if (rg_weight(ctx, N, theta, &fv, hd.vis) != RG_OK) return die("weighting");
+        }
+        rg_wkern wk = {wd.data, wd.plane_count, wd.size, wd.oversampling, wd.w_min, wd.w_step};
+        rg_akern ak = {ad.antenna_count, ad.time_count, ad.freq_count, ad.size_x, ad.size_y, ad.t_min, ad.t_step,
+                       ad.f_min, ad.f_step, ad.freq, ad.time, ad.data};
+        rg_vis_bl vb = {hd.bl_count, hd.time_count, hd.freq_count, hd.antenna1, hd.antenna2,
+                        hd.time, hd.freq, hd.uvw, hd.vis};
+        std::vector<double> grid((size_t)N * N * 2, 0.0);
+        std::printf("Gridder: AW-projection (ignoring convolution)\n");
+        rg_context_set_profiling(ctx, 1);
+        if (rg_grid_awprojection(ctx, grid.data(), N, theta, &vb, &wk, &ak, 0, hd.bl_count, RG_GRID_OVERWRITE) !=
+            RG_OK)
+            return die("gridding");
+        const int rc = write_outputs(ctx, grid, N, gridfile, image);
+        rg_free_akern_data(&ad);
+        rg_free_wkern_data(&wd);
+        rg_free_vis_bl_data(&hd);
+        rg_context_destroy(ctx);
+        return rc;
+    }
     rg_vis_data vd;
     if (rg_read_vis_hdf5(visfile.c_str(), bl_min, bl_max, &vd) != RG_OK) return die("visibilities");
     std::printf("Have %lld baselines and %lld visibilities\n", (long long)vd.bl_count, (long long)vd.n);
@@ -143,26 +217,8 @@ int main(int argc, char **argv)
         if (st != RG_OK) return die("gridding");
         rg_free_wkern_data(&wd);
     }
-    const char *names[64];
-    float ms[64];
-    const int nt = rg_last_timings(ctx, names, ms, 64);
-    float total = 0;
-    for (int i = 0; i < nt; i++) total += ms[i];
-    std::printf("Gridder Elapsed Time: %.6f seconds\n", total / 1000.0);
-    if (!gridfile.empty()) {
-        std::vector<double> h = grid;
-        if (rg_make_hermitian(ctx, h.data(), N) != RG_OK) return die("make_hermitian");
-        std::ofstream f(gridfile, std::ios::binary);
-        f.write((const char *)h.data(), (std::streamsize)(h.size() * sizeof(double)));
-    }
-    if (!image.empty()) {
-        std::vector<double> img((size_t)N * N);
-        if (rg_image_from_grid(ctx, grid.data(), N, img.data(), nullptr) != RG_OK) return die("image");
-        std::printf("Writing Image to File... \n");
-        std::ofstream f(image, std::ios::binary);
-        f.write((const char *)img.data(), (std::streamsize)(img.size() * sizeof(double)));
-    }
+    const int rc = write_outputs(ctx, grid, N, gridfile, image);
     rg_free_vis_data(&vd);
     rg_context_destroy(ctx);
-    return 0;
+    return rc;
 }

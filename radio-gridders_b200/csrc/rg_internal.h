@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <map>
 #include <vector>
 #include <string>
@@ -164,6 +165,18 @@ struct Diag {
 rg_status diag_begin(rg_context *ctx, Diag *d);
 rg_status diag_end(rg_context *ctx, const Diag &d, unsigned long long *counters_out);
 rg_status finish_out(rg_context *ctx, const OutView &ov);
+
+// One baseline of a crocodile visibility file (rg_io.cu): antenna ids (-1
+// when the file has none), times, frequencies (Hz), uvw [time][3] metres,
+// visibilities [time][freq] complex interleaved.
+struct BaselineRecord {
+    int a1 = -1, a2 = -1;
+    std::vector<double> time, freq, uvw, vis;
+};
+// Calls fn for every baseline of the file (hierarchical or legacy flat
+// layout) whose first uvw sample's length lies in [bl_min, bl_max) metres.
+rg_status visit_vis_hdf5(const char *path, double bl_min, double bl_max,
+                         const std::function<void(const BaselineRecord &)> &fn);
 
 // ---------------------------------------------------------------------------
 // kernel launchers (defined in k_*.cu)

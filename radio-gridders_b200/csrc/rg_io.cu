@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <string>
 #include <vector>
@@ -22,15 +23,11 @@ namespace {
 
 constexpr double kC = 299792458.0;  // src/reference/hdf5.c:12
 
-struct Flat {
-    std::vector<double> u, v, w, vis;
-};
-
-// One baseline group: flatten in time-major, frequency-minor order as
-// flatten_visibilities_CUDA does (src/common/hdf5.c:827-872), after the
-// baseline-length cut on the first uvw sample (src/reference/hdf5.c:104-106).
-bool add_baseline(h5::File &f, const h5::Object &g, double bl_min, double bl_max, Flat *out, bool *kept,
-                  std::string *err)
+// One baseline group (src/reference/hdf5.c:64-96, :305-349): its time, frequency,
+// uvw (metres) and visibility arrays, if the first uvw sample's (u, v) length
+// lies in [bl_min, bl_max) (src/reference/hdf5.c:104-106).
+bool read_baseline(h5::File &f, const h5::Object &g, double bl_min, double bl_max, BaselineRecord *rec, bool *kept,
+                   std::string *err)
 {
     std::vector<std::pair<std::string, uint64_t>> ent;
     if (!f.entries(g, &ent, err)) return false;
@@ -45,29 +42,18 @@ bool add_baseline(h5::File &f, const h5::Object &g, double bl_min, double bl_max
             return false;
         }
     }
-    std::vector<double> freq, uvw, vis;
-    if (!f.read_doubles(o[0].ds, &freq, err) || !f.read_doubles(o[2].ds, &uvw, err) ||
-        !f.read_doubles(o[3].ds, &vis, err))
+    if (!f.read_doubles(o[0].ds, &rec->freq, err) || !f.read_doubles(o[1].ds, &rec->time, err) ||
+        !f.read_doubles(o[2].ds, &rec->uvw, err) || !f.read_doubles(o[3].ds, &rec->vis, err))
         return false;
-    const size_t nt = o[1].ds.dims.empty() ? 0 : o[1].ds.dims[0];
-    const size_t nf = freq.size();
-    if (uvw.size() != nt * 3 || vis.size() != nt * nf * 2) {
+    const size_t nt = rec->time.size(), nf = rec->freq.size();
+    if (rec->uvw.size() != nt * 3 || rec->vis.size() != nt * nf * 2) {
         *err = "inconsistent baseline dataset shapes";
         return false;
     }
     *kept = false;
     if (nt == 0) return true;
-    const double len = std::sqrt(uvw[0] * uvw[0] + uvw[1] * uvw[1]);
-    if (len < bl_min || len >= bl_max) return true;
-    *kept = true;
-    for (size_t t = 0; t < nt; t++)
-        for (size_t k = 0; k < nf; k++) {
-            out->u.push_back(uvw[3 * t + 0] * freq[k] / kC);
-            out->v.push_back(uvw[3 * t + 1] * freq[k] / kC);
-            out->w.push_back(uvw[3 * t + 2] * freq[k] / kC);
-            out->vis.push_back(vis[2 * (t * nf + k)]);
-            out->vis.push_back(vis[2 * (t * nf + k) + 1]);
-        }
+    const double len = std::sqrt(rec->uvw[0] * rec->uvw[0] + rec->uvw[1] * rec->uvw[1]);
+    *kept = !(len < bl_min || len >= bl_max);
     return true;
 }
 
@@ -87,12 +73,11 @@ std::string fmt_g(double x)
 
 }  // namespace
 
-extern "C" {
+namespace rg {
 
-rg_status rg_read_vis_hdf5(const char *path, double bl_min, double bl_max, rg_vis_data *out)
+rg_status visit_vis_hdf5(const char *path, double bl_min, double bl_max,
+                         const std::function<void(const BaselineRecord &)> &fn)
 {
-    if (!path || !out) return fail(RG_ERR_INVALID_ARGUMENT, "path and out must be non-NULL");
-    std::memset(out, 0, sizeof(*out));
     h5::File f;
     std::string err;
     if (!f.open(path, &err)) return fail(RG_ERR_IO, err);
@@ -101,34 +86,37 @@ rg_status rg_read_vis_hdf5(const char *path, double bl_min, double bl_max, rg_vi
         return fail(RG_ERR_IO, std::string("no 'vis' group in ") + path + (err.empty() ? "" : ": " + err));
     std::vector<std::pair<std::string, uint64_t>> ent;
     if (!f.entries(vg, &ent, &err)) return fail(RG_ERR_IO, err);
-    Flat flat;
-    int64_t baselines = 0;
     bool legacy = false;
     for (auto &e : ent) legacy |= e.first == "uvw";
     if (legacy) {  // src/reference/hdf5.c:173-247: one baseline per row
         std::map<std::string, uint64_t> by;
         for (auto &e : ent) by[e.first] = e.second;
-        h5::Object ou, of, ov;
+        h5::Object ou, of, ov, ot, oa1, oa2;
         if (!by.count("frequency") || !by.count("vis") || !f.object_at(by["uvw"], &ou, &err) ||
             !f.object_at(by["frequency"], &of, &err) || !f.object_at(by["vis"], &ov, &err))
             return fail(RG_ERR_IO, "incomplete flat 'vis' group");
-        std::vector<double> uvw, freq, vis;
+        std::vector<double> uvw, freq, vis, time;
+        std::vector<int64_t> a1, a2;
         if (!f.read_doubles(ou.ds, &uvw, &err) || !f.read_doubles(of.ds, &freq, &err) ||
             !f.read_doubles(ov.ds, &vis, &err))
             return fail(RG_ERR_IO, err);
         const size_t nt = uvw.size() / 3, nf = freq.size();
         if (vis.size() != nt * nf * 2) return fail(RG_ERR_IO, "inconsistent flat visibility shapes");
+        // antenna and time columns, when present (AW-projection needs them)
+        if (by.count("time") && f.object_at(by["time"], &ot, &err)) f.read_doubles(ot.ds, &time, &err);
+        if (by.count("antenna1") && f.object_at(by["antenna1"], &oa1, &err)) f.read_int64(oa1.ds, &a1, &err);
+        if (by.count("antenna2") && f.object_at(by["antenna2"], &oa2, &err)) f.read_int64(oa2.ds, &a2, &err);
         for (size_t t = 0; t < nt; t++) {
             const double len = std::sqrt(uvw[3 * t] * uvw[3 * t] + uvw[3 * t + 1] * uvw[3 * t + 1]);
             if (len < bl_min || len >= bl_max) continue;
-            baselines++;
-            for (size_t k = 0; k < nf; k++) {
-                flat.u.push_back(uvw[3 * t] * freq[k] / kC);
-                flat.v.push_back(uvw[3 * t + 1] * freq[k] / kC);
-                flat.w.push_back(uvw[3 * t + 2] * freq[k] / kC);
-                flat.vis.push_back(vis[2 * (t * nf + k)]);
-                flat.vis.push_back(vis[2 * (t * nf + k) + 1]);
-            }
+            BaselineRecord r;
+            r.a1 = t < a1.size() ? (int)a1[t] : -1;
+            r.a2 = t < a2.size() ? (int)a2[t] : -1;
+            r.time.assign(1, t < time.size() ? time[t] : 0.0);
+            r.freq = freq;
+            r.uvw.assign(uvw.begin() + 3 * t, uvw.begin() + 3 * t + 3);
+            r.vis.assign(vis.begin() + 2 * t * nf, vis.begin() + 2 * (t + 1) * nf);
+            fn(r);
         }
     } else {  // src/reference/hdf5.c:249-303: antenna_count = children + 1
         std::map<std::string, uint64_t> a1s;
@@ -147,19 +135,50 @@ rg_status rg_read_vis_hdf5(const char *path, double bl_min, double bl_max, rg_vi
                 auto it2 = a2s.find(std::to_string(a2));
                 if (it2 == a2s.end()) continue;
                 h5::Object g2;
+                BaselineRecord r;
                 bool kept = false;
-                if (!f.object_at(it2->second, &g2, &err) || !add_baseline(f, g2, bl_min, bl_max, &flat, &kept, &err))
+                if (!f.object_at(it2->second, &g2, &err) || !read_baseline(f, g2, bl_min, bl_max, &r, &kept, &err))
                     return fail(RG_ERR_IO, "baseline " + std::to_string(a1) + "/" + std::to_string(a2) + ": " + err);
-                baselines += kept;
+                if (!kept) continue;
+                r.a1 = a1;
+                r.a2 = a2;
+                fn(r);
             }
         }
     }
-    out->n = (int64_t)flat.u.size();
+    return RG_OK;
+}
+
+}  // namespace rg
+
+extern "C" {
+
+rg_status rg_read_vis_hdf5(const char *path, double bl_min, double bl_max, rg_vis_data *out)
+{
+    if (!path || !out) return fail(RG_ERR_INVALID_ARGUMENT, "path and out must be non-NULL");
+    std::memset(out, 0, sizeof(*out));
+    // flattened in baseline, time-major, frequency-minor order as
+    // flatten_visibilities_CUDA does (src/common/hdf5.c:827-872)
+    std::vector<double> u, v, w, vis;
+    int64_t baselines = 0;
+    RG_CHECK(rg::visit_vis_hdf5(path, bl_min, bl_max, [&](const BaselineRecord &r) {
+        const size_t nt = r.time.size(), nf = r.freq.size();
+        baselines++;
+        for (size_t t = 0; t < nt; t++)
+            for (size_t k = 0; k < nf; k++) {
+                u.push_back(r.uvw[3 * t + 0] * r.freq[k] / kC);
+                v.push_back(r.uvw[3 * t + 1] * r.freq[k] / kC);
+                w.push_back(r.uvw[3 * t + 2] * r.freq[k] / kC);
+                vis.push_back(r.vis[2 * (t * nf + k)]);
+                vis.push_back(r.vis[2 * (t * nf + k) + 1]);
+            }
+    }));
+    out->n = (int64_t)u.size();
     out->bl_count = baselines;
-    out->u = copy_out(flat.u);
-    out->v = copy_out(flat.v);
-    out->w = copy_out(flat.w);
-    out->vis = copy_out(flat.vis);
+    out->u = copy_out(u);
+    out->v = copy_out(v);
+    out->w = copy_out(w);
+    out->vis = copy_out(vis);
     if (!out->u || !out->v || !out->w || !out->vis) {
         rg_free_vis_data(out);
         return fail(RG_ERR_OUT_OF_MEMORY, "host allocation failed");

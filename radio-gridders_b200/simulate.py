@@ -499,3 +499,31 @@ def sepkern_pswf(support: int, oversampling: int, x0: float = 0.25, c: float | N
     wq *= (xq[1] - xq[0]) / 3.0
     corr = 2.0 * (np.cos(2 * np.pi * np.outer(nu, xq)) * (cq * wq)[None, :]).sum(axis=1)
     return np.ascontiguousarray(conv), np.ascontiguousarray(corr.reshape(corr_oversampling, corr_size))
+
+
+def akern_for(obs, n_time: int = 3, n_freq: int = 2, size: int = 16, seed: int = 0, jitter: float = 0.0):
+    """An A-kernel table (rg_akern layout) for an observation: per antenna,
+    n_time slots spanning its times and n_freq channels spanning its
+    frequencies (each kernel's own time and frequency, optionally jittered by
+    `jitter` of a step so the nearest-slot search has something to decide),
+    smooth seeded complex kernel values.  The reference's AW-projection reads
+    only the kernels' frequencies (src/reference/grid.c:571-590)."""
+    rng = np.random.default_rng(seed)
+    n_ant = int(max(obs.antenna1.max(), obs.antenna2.max())) + 1
+    t = np.asarray(obs.time, np.float64)
+    f = np.asarray(obs.freq, np.float64)
+    t_min, t_max = float(t.min()), float(t.max())
+    f_min, f_max = float(f.min()), float(f.max())
+    t_step = (t_max - t_min) / (n_time - 1) if n_time > 1 else 1.0
+    f_step = (f_max - f_min) / (n_freq - 1) if n_freq > 1 else 1.0
+    ta = t_min + np.arange(n_time) * t_step
+    fa = f_min + np.arange(n_freq) * f_step
+    time = np.broadcast_to(ta[None, :, None], (n_ant, n_time, n_freq)).copy()
+    freq = np.broadcast_to(fa[None, None, :], (n_ant, n_time, n_freq)).copy()
+    if jitter:
+        freq = freq + jitter * f_step * rng.uniform(-1, 1, freq.shape)
+    y, x = np.mgrid[:size, :size] - size / 2
+    base = np.exp(-(x * x + y * y) / (size * size / 8.0))
+    data = base[None, None, None] * np.exp(1j * rng.uniform(0, 2 * np.pi, (n_ant, n_time, n_freq, 1, 1)))
+    from types import SimpleNamespace
+    return SimpleNamespace(freq=freq, time=time, data=data, t_min=t_min, t_step=t_step, f_min=f_min, f_step=f_step)

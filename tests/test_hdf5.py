@@ -145,3 +145,39 @@ def test_legacy_flat_layout_round_trip(rg, obs, tmp_path):
     lo = np.quantile(length, 0.5)
     _, kept = rg.read_vis_hdf5(str(p), lo)
     assert kept == int((length >= lo).sum())
+
+
+def test_akern_round_trip(rg, sim, tmp_path):
+    """A-kernel files (load_akern's layout, src/common/hdf5.c:652-820:
+    akern/<theta>/<antenna>/<time>/<freq>/kern): written and read back with
+    the same axes, frequencies and kernel values."""
+    obs = sim.wtowers_plain(seed=3, n_st=6, n_dump=4, n_chan=3, lam=5120.0)
+    ak = sim.akern_for(obs, 3, 3, 8)
+    A = rg.AKernels(ak.freq, ak.time, ak.data, ak.t_min, ak.t_step, ak.f_min, ak.f_step)
+    p = str(tmp_path / "ak.h5")
+    rg.write_akern_hdf5(p, 0.1, A)
+    back = rg.read_akern_hdf5(p, 0.1)
+    np.testing.assert_array_equal(back.data, A.data)
+    np.testing.assert_array_equal(back.freq, A.freq)
+    np.testing.assert_array_equal(back.time, A.time)
+    assert back.t_min == A.t_min and back.f_min == A.f_min
+    assert abs(back.t_step - A.t_step) < 1e-12 * abs(A.t_step)
+    with pytest.raises(rg.RGError):
+        rg.read_akern_hdf5(p, 0.2)  # no akern/0.2 group
+
+
+def test_hierarchical_read_keeps_baselines(rg, sim, tmp_path):
+    """rg_read_vis_bl_hdf5: the same baselines, antennas, times, channels,
+    uvw and visibilities as written, in the flat reader's order."""
+    obs = sim.wtowers_plain(seed=3, n_st=6, n_dump=4, n_chan=3, lam=5120.0)
+    p = tmp_path / "vis.h5"
+    _write(rg, p, obs)
+    hv = rg.read_vis_bl_hdf5(str(p))
+    np.testing.assert_array_equal(hv.antenna1, obs.antenna1)
+    np.testing.assert_array_equal(hv.antenna2, obs.antenna2)
+    np.testing.assert_array_equal(hv.uvw, obs.uvw)
+    np.testing.assert_array_equal(hv.freq, obs.freq)
+    np.testing.assert_array_equal(hv.vis, obs.vis)
+    np.testing.assert_array_equal(hv.time, np.broadcast_to(obs.time, hv.time.shape))
+    flat, _ = rg.read_vis_hdf5(str(p))
+    np.testing.assert_array_equal(flat.vis, hv.vis.ravel())

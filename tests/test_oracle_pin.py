@@ -148,3 +148,22 @@ def test_gridded_image_matches_dft_for_point_source(oracle, sim):
     # the source appears at (-l0, -m0) in this convention
     y, x = np.unravel_index(np.argmax(ref), ref.shape)
     assert abs((x - n // 2) * th / n + l0) < th / n and abs((y - n // 2) * th / n + m0) < th / n
+
+
+def test_awprojection_restatement_matches_reference(sim, oracle, rg):
+    """grid_awprojection after convolve_aw_kernels (src/reference/grid.c:
+    557-637), the reference's own build against the restatement: bit-identical
+    grids, and different from plain W-projection (the A-kernel channels'
+    frequencies pick the planes)."""
+    if not oracle.reference_available():
+        pytest.skip("reference build absent")
+    obs = sim.wtowers_plain(seed=3, n_st=30, n_dump=8, n_chan=4, lam=5120.0)
+    n, th = obs.meta["grid_size"], obs.meta["theta"]
+    u, v, w, vis = obs.flat()
+    wk = sim.wkernel_for(w * 1.01, th, 2.0, size=8, oversampling=4)
+    ak = sim.akern_for(obs, 3, 2, 8, jitter=0.1)
+    got = oracle.grid_awprojection(n, th, rg.HierVis.of(obs), wk, ak)
+    ref = oracle.ref_grid_awprojection(n, th, obs, wk, ak)
+    assert np.array_equal(got, ref)
+    wp = oracle.grid_wprojection(n, th, u, v, w, vis, wk)
+    assert np.linalg.norm(got - wp) / np.linalg.norm(wp) > 1e-6
