@@ -812,8 +812,81 @@ def learned_small(ctx, stations=64, steps=2000):
 
 
 
+def winc_sweep(ctx, wincs=(10.0, 20.0, 40.0, 80.0), steps=120000):
+    """The learned kernel's algorithmic route: the same C1 observation
+    (2048^2, S 512, margin 16, 2.09M vis) gridded by the table and the learned
+    W-towers paths at several w increments.  A larger winc means fewer
+    w-floors, hence fewer sub-grid transforms, but taps over a wider
+    |w - w_mid| <= winc/2: the table needs one plane per lambda of w (32x
+    oversampled 16-tap slices, 4.2 MB each stored twice), the network is
+    retrained on the wider range.  Each path: CUDA events around the whole
+    call (graph replay, L2 flushed between calls), image RMS / peak against the
+    FP64-reduced DFT."""
+    import torch
+    obs = _SIM().wtowers_plain()
+    u, v, w, vis = obs.flat()
+    n, th, S, M = 2048, 0.1, 512, 16
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    ctx.set_stream(stream.cuda_stream)
+    V = _RG().Visibilities(*(torch.from_numpy(a).to(dev) for a in (u, v, w)), torch.from_numpy(vis).to(dev))
+    g = torch.zeros((n, n), dtype=torch.complex128, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    ref = ctx.dft_image(n, th, _RG().Visibilities(u, v, w, vis), _RG().RG_DFT_FP64_REDUCED, 2.0)
+
+    def timed(fn, reps=5):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        out = []
+        for _ in range(reps):
+            flush.fill_(1)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            out.append(a.elapsed_time(b))
+        return sorted(out)[len(out) // 2]
+
+    rows = []
+    for winc in wincs:
+        half = winc / 2
+        wk = _SIM().generate_wkernel(th, np.arange(-half - 1.0, half + 1.5, 1.0), 16, 32)
+        dwk = torch.from_numpy(np.ascontiguousarray(wk.data)).to(dev)
+        t_ms = timed(lambda: ctx.grid_wtowers(g, n, th, V, wk, S, M, winc, flags=1, wkern_data=dwk))
+        st = ctx.last_stats()
+        img_t = ctx.image_from_grid(g.cpu().numpy(), taper_1d=_SIM().taper_1d(th, n, wk.c))
+        t_rms, t_pk = _LEARNED().image_errors(img_t, ref)
+        del dwk
+        t0 = time.time()
+        mlp, losses = _LEARNED().train(ctx, wmax=half + 1.0, theta=th, ksize=16, n_triples=16384, steps=steps,
+                                       batch=32768, lr_max=2e-3)
+        train_s = time.time() - t0
+        tap_err, _ = _LEARNED().tap_error(mlp, wmax=half + 1.0, theta=th)
+        l_ms = timed(lambda: _RG().grid_wtowers_learned(ctx, mlp, g, n, th, V, S, M, winc, flags=1), reps=3)
+        img_l = ctx.image_from_grid(g.cpu().numpy(), taper_1d=_SIM().taper_1d(th, n, wk.c))
+        l_rms, l_pk = _LEARNED().image_errors(img_l, ref)
+        mlp.close()
+        rows.append({"winc": winc, "floors": st["floors"], "active_subgrids": st["active_subgrids"],
+                     "table_planes": wk.plane_count, "table_mb_dup": 2 * wk.data.size * 8 / 1e6,
+                     "table_ms": t_ms, "table_vis_per_s": len(u) / (t_ms * 1e-3),
+                     "table_image_rms": t_rms, "table_image_peak": t_pk,
+                     "learned_ms": l_ms, "learned_vis_per_s": len(u) / (l_ms * 1e-3),
+                     "learned_image_rms": l_rms, "learned_image_peak": l_pk, "learned_tap_err": tap_err,
+                     "train_s": train_s})
+        print(json.dumps({"study": "winc_sweep_row", **rows[-1]}), flush=True)
+    ok_t = [r for r in rows if r["table_image_rms"] <= 1e-4]
+    ok_l = [r for r in rows if r["learned_image_rms"] <= 1e-4]
+    best_t = min(ok_t, key=lambda r: r["table_ms"]) if ok_t else None
+    best_l = min(ok_l, key=lambda r: r["learned_ms"]) if ok_l else None
+    ctx.set_stream(None)
+    return {"rows": rows, "best_table_winc": best_t and best_t["winc"], "best_learned_winc": best_l and best_l["winc"],
+            "learned_over_table_at_best": (best_t["table_ms"] / best_l["learned_ms"]) if best_t and best_l else None}
+
+
 STUDIES = ("dft", "towers", "towers_ov", "learned", "learned_small", "baselines", "learned_towers",
-           "learned_towers_c4")
+           "learned_towers_c4", "winc_sweep")
 
 
 def run_study(which):
@@ -837,6 +910,8 @@ def run_study(which):
         print(json.dumps({"study": "learned_small", **learned_small(ctx)}), flush=True)
     elif which == "baselines":
         print(json.dumps({"study": "baselines", **baselines(ctx)}), flush=True)
+    elif which == "winc_sweep":
+        print(json.dumps({"study": "winc_sweep", **winc_sweep(ctx)}), flush=True)
     elif which in ("learned_towers", "learned_towers_c4"):
         cfg = "C4" if which.endswith("c4") else "C1"
         print(json.dumps({"study": "learned_towers", **learned_towers(ctx, cfg)}), flush=True)

@@ -110,7 +110,8 @@ int main(int argc, char **argv)
     const double theta = number(argc, argv, "theta", 0), lambda = number(argc, argv, "lambda", 0);
     const int device = (int)number(argc, argv, "device", 0);
     const double bl_min = number(argc, argv, "bl_min", 0), bl_max = number(argc, argv, "bl_max", DBL_MAX);
-    if (!wproj && (!has(argc, argv, "subgrid") || !has(argc, argv, "margin") || !has(argc, argv, "winc"))) {
+    const bool awproj = has(argc, argv, "akern");
+    if (!wproj && !awproj && (!has(argc, argv, "subgrid") || !has(argc, argv, "margin") || !has(argc, argv, "winc"))) {
         std::printf("Missing W-Towers Parameters. Check subgrid/margin/winc\n");
         help();
         return 0;

@@ -60,7 +60,7 @@ def test_grid_out_akern(rg, oracle, aw_case, tmp_path):
                         f"-theta={th}", f"-lambda={obs.meta['lam']}", f"-grid={tmp_path}/aw.grid",
                         f"-image={tmp_path}/aw.img"], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert "AW-projection" in r.stdout
+    assert "Gridder: AW-projection" in r.stdout
     wkr = rg.read_wkern_hdf5(str(tmp_path / "wk.h5"), th)
     akr = rg.read_akern_hdf5(str(tmp_path / "ak.h5"), th)
     ref = oracle.grid_awprojection(n, th, rg.HierVis.of(obs), wkr, akr)
