@@ -491,6 +491,21 @@ def run_b200(args, rank, world, local_rank):
     # and complex64) and the FP64 master grid out
     compulsory = 20 * nvis + 16 * GRID * GRID
     dense_bytes = dense_dataflow_bytes(stats, nvis)
+    # The row stage is bound by instruction issue, not HBM: its FP32 work
+    # against the FP32 pipe (the 5 N log2 N convention per transform, as the
+    # reference's complexity analysis counts FFTs, plus 8 flops per Fresnel
+    # multiply-add), for context beside the HBM roofline.
+    rows_ms = kernel_stages.get("tower_rows")
+    compute_roofline = None
+    if rows_ms:
+        s2 = SUBGRID * SUBGRID
+        flops = stats["active_subgrids"] * (SUBGRID * 5 * SUBGRID * math.log2(SUBGRID) + 8 * s2)
+        fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12
+        compute_roofline = {"kernel": "tower_rows", "flops_per_launch": flops,
+                            "achieved": flops / (rows_ms * 1e-3) / 1e12, "peak": fp32_peak, "unit": "TFLOP/s",
+                            "frac": flops / (rows_ms * 1e-3) / 1e12 / fp32_peak,
+                            "peak_source": "nominal FP32 (148 SMs x 128 lanes x 2 x 1.965 GHz); "
+                                           "no measured FP32 peak on this pool"}
     line = {
         "impl": "b200", "metric": METRIC, "value": value, "unit": "vis/s", "n_gpus": world,
         "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step,
@@ -523,6 +538,7 @@ def run_b200(args, rank, world, local_rank):
                           "dense_dataflow_bytes_per_step": dense_bytes,
                           "dense_equivalent_gbs": dense_bytes / (ms_per_step * 1e-3) / 1e9,
                           "dense_equivalent_frac": dense_bytes / (ms_per_step * 1e-3) / 1e9 / peak},
+        "compute_roofline": compute_roofline,
         "step_ms_min_median_max": [round(min(step_ms), 4), round(statistics.median(step_ms), 4),
                                    round(max(step_ms), 4)],
         "stage_ms": {k: round(statistics.mean(v), 4) for k, v in stage_ms.items()},

@@ -668,6 +668,9 @@ static rg_status wtowers_autotune(rg_context *ctx, const DevVis &dv, const float
     RG_CUDA(cudaEventCreate(&e1));
     const bool prof = ctx->profiling;
     ctx->profiling = false;
+    // A candidate whose floor groups outgrow the plan's capacity (more work
+    // items per SM make more, smaller groups) is skipped: its pass wrote
+    // nothing, and the plan keeps the capacities the caller's pass sized.
     auto time_pass = [&](float *ms) -> rg_status {
         bool overflow = false;
         for (int rep = 0; rep < 2; rep++) {
@@ -676,7 +679,10 @@ static rg_status wtowers_autotune(rg_context *ctx, const DevVis &dv, const float
                                   pl, &overflow));
             RG_CUDA(cudaEventRecord(e1, ctx->stream));
             RG_CUDA(cudaEventSynchronize(e1));
-            if (overflow) return fail(RG_ERR_UNSUPPORTED, "capacity overflow while tuning");
+            if (overflow) {
+                *ms = 1e30f;
+                return RG_OK;
+            }
         }
         RG_CUDA(cudaEventElapsedTime(ms, e0, e1));
         return RG_OK;
