@@ -60,6 +60,10 @@ def parse():
     p.add_argument("--no-image-check", action="store_true")
     p.add_argument("--no-learned", action="store_true",
                    help="skip the learned-kernel W-towers measurement (training takes ~40 s)")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="keep the default schedule (Romein 8 points per thread, 8 row-stage items per SM: the "
+                        "tuner's usual choice here) instead of timing candidates; for profiled runs, whose "
+                        "serialised launches would skew the tuner")
     p.add_argument("--study", choices=STUDIES, default=None,
                    help="run one of the studies beside the headline line instead (one JSON object each)")
     p.add_argument("--stations", type=int, default=256,
@@ -319,6 +323,8 @@ def run_b200(args, rank, world, local_rank):
     ctx = rg.Context(local_rank)
     stream = torch.cuda.current_stream(dev)
     ctx.set_stream(stream.cuda_stream)
+    if args.no_autotune:
+        ctx.set_autotune(False)
 
     # inputs resident in HBM
     du = torch.from_numpy(u).to(dev)
@@ -523,7 +529,7 @@ def run_b200(args, rank, world, local_rank):
                    "precision": "FP32 sub-grids and transforms; FP64 coordinates, Fresnel phase and master grid",
                    "schedule": {"romein_points_per_thread": stats["romein_points"],
                                 "row_stage_items_per_sm": stats["group_items_per_sm"],
-                                "graph_replay": bool(stats["graph"]), "autotuned": True},
+                                "graph_replay": bool(stats["graph"]), "autotuned": not args.no_autotune},
                    "marked_strips": stats["marked_strips"], "floor_groups": stats["floor_groups"]},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,

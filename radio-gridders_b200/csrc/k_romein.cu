@@ -57,18 +57,19 @@ __global__ void __launch_bounds__(K *K / P, (RomeinBounds<K, P>::min_ctas)) rome
     __shared__ int4 srec[BATCH];
     __shared__ float2 svis[BATCH];
     const int myU = threadIdx.x % K, myV0 = threadIdx.x / K;
-    const int limit = side * side;
-    auto addr = [strip_lg](int L) { return STRIP ? strip_addr(L, strip_lg) : L; };
+    // Each point is tracked by its key: its element offset in the grid (the
+    // strip-major address for sub-grids), or -1 when it lies off the grid.
+    // Keys are equal exactly when the points are.
 
     for (int64_t c0 = (int64_t)blockIdx.x * chunk; c0 < n; c0 += (int64_t)gridDim.x * chunk) {
         const int64_t c1 = c0 + chunk < n ? c0 + chunk : n;
         int cur_bin = -1, cur_goff = 0, cur_res = 0;
         float2 *cur_grid = nullptr;  // the current bin's sub-grid (null: past the slot capacity)
-        int cur_idx[P];
+        int cur_key[P];
         float2 sum[P];
 #pragma unroll
         for (int p = 0; p < P; p++) {
-            cur_idx[p] = 0;
+            cur_key[p] = -1;
             sum[p] = make_float2(0.f, 0.f);
         }
         for (int64_t b0 = c0; b0 < c1; b0 += BATCH) {
@@ -108,10 +109,20 @@ __global__ void __launch_bounds__(K *K / P, (RomeinBounds<K, P>::min_ctas)) rome
                 }
                 cur_goff = r.y;
                 cur_res = r.w;
-                int idx[P];
+                int key[P];
                 if (STRIP) {
+                    // the thread's points share one linear column: L = base + cv*S has
+                    // column base mod S and row floor(base / S) + cv, so the strip-major
+                    // address is a column part plus 8 per row (strip_addr, unrolled)
+                    const int base = r.y + cu;
+                    const int col = base & (side - 1);
+                    const int colpart = ((col >> 3) << (strip_lg + 3)) + (col & 7);
+                    const int rowb = base >> strip_lg;
 #pragma unroll
-                    for (int p = 0; p < P; p++) idx[p] = r.y + ((cv0 + p * RS) & (K - 1)) * side + cu;
+                    for (int p = 0; p < P; p++) {
+                        const int row = rowb + ((cv0 + p * RS) & (K - 1));
+                        key[p] = (unsigned)row < (unsigned)side ? colpart + (row << 3) : -1;
+                    }
                 } else {
                     // per-axis check; -1 (never flushed) for a tap off the grid
                     const int col = (r.w & 0xffff) - 64 + cu;
@@ -119,15 +130,15 @@ __global__ void __launch_bounds__(K *K / P, (RomeinBounds<K, P>::min_ctas)) rome
 #pragma unroll
                     for (int p = 0; p < P; p++) {
                         const int row = row0 + ((cv0 + p * RS) & (K - 1));
-                        idx[p] = ((unsigned)col < (unsigned)side && (unsigned)row < (unsigned)side) ? row * side + col
+                        key[p] = ((unsigned)col < (unsigned)side && (unsigned)row < (unsigned)side) ? row * side + col
                                                                                                   : -1;
                     }
                 }
                 if (r.x != cur_bin) {
 #pragma unroll
                     for (int p = 0; p < P; p++) {
-                        if (cur_grid && (unsigned)cur_idx[p] < (unsigned)limit) atomicAdd(cur_grid + addr(cur_idx[p]), sum[p]);
-                        cur_idx[p] = idx[p];
+                        if (cur_grid && cur_key[p] >= 0) atomicAdd(cur_grid + cur_key[p], sum[p]);
+                        cur_key[p] = key[p];
                         sum[p] = make_float2(0.f, 0.f);
                     }
                     cur_bin = r.x;
@@ -136,9 +147,9 @@ __global__ void __launch_bounds__(K *K / P, (RomeinBounds<K, P>::min_ctas)) rome
                 }
 #pragma unroll
                 for (int p = 0; p < P; p++) {
-                    if (idx[p] != cur_idx[p]) {
-                        if (cur_grid && (unsigned)cur_idx[p] < (unsigned)limit) atomicAdd(cur_grid + addr(cur_idx[p]), sum[p]);
-                        cur_idx[p] = idx[p];
+                    if (key[p] != cur_key[p]) {
+                        if (cur_grid && cur_key[p] >= 0) atomicAdd(cur_grid + cur_key[p], sum[p]);
+                        cur_key[p] = key[p];
                         sum[p] = make_float2(0.f, 0.f);
                     }
                     sum[p].x = fmaf(vz.x, t[p].x, fmaf(vz.y, t[p].y, sum[p].x));
@@ -149,7 +160,7 @@ __global__ void __launch_bounds__(K *K / P, (RomeinBounds<K, P>::min_ctas)) rome
         if (cur_grid) {
 #pragma unroll
             for (int p = 0; p < P; p++)
-                if ((unsigned)cur_idx[p] < (unsigned)limit) atomicAdd(cur_grid + addr(cur_idx[p]), sum[p]);
+                if (cur_key[p] >= 0) atomicAdd(cur_grid + cur_key[p], sum[p]);
         }
     }
 }
@@ -162,8 +173,11 @@ static void romein_launch(cudaStream_t s, const int4 *rec, const float2 *visf, i
     // Every CTA resident at once, each with an equal contiguous run of
     // visibilities: occupancy, not the chunk size, decides the grid.
     constexpr int NT = K * K / P;
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, romein_kernel<K, P, false>, NT, 0);
+    int per_sm = 0;  // of the instantiation that runs (the two register counts can differ)
+    if (strip_lg)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, romein_kernel<K, P, true>, NT, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, romein_kernel<K, P, false>, NT, 0);
     if (per_sm < 1) per_sm = 1;
     int64_t blocks = (int64_t)sm_count * per_sm;
     int64_t chunk = (n + blocks - 1) / blocks;

@@ -70,7 +70,7 @@ rg_status grid_wtowers_impl(rg_context *ctx, double *uvgrid, int grid_size, doub
 
 // Schedule knobs of a W-towers pass (picked by the autotuner).
 struct TowerTuning {
-    int romein_points = 4;  // grid points per Romein thread (threads per CTA = K^2 / points)
+    int romein_points = 8;  // grid points per Romein thread (threads per CTA = K^2 / points)
     int group_items = 8;    // row-stage work items per SM (sets the floor-group size)
 };
 
