@@ -132,6 +132,16 @@ rg_status rg_context_set_graphs(rg_context *ctx, int enabled);
 rg_status rg_grid_wprojection(rg_context *ctx, double *uvgrid, int grid_size, double theta,
                               const rg_vis *vis, const rg_wkern *wkern, int flags);
 
+/* Nearest-cell gridding without a kernel: each visibility added to the grid
+ * cell nearest its (u, v).  Replaces grid_simple (src/reference/grid.h:115-116,
+ * grid.c:83-99), grid_CPU.out's gridder when no w-kernel file is given
+ * (src/reference/main.c:200-206).  FP64 atomics (the order of additions to a
+ * cell varies from call to call: grids agree to FP64 rounding).  A
+ * visibility whose cell lies off the grid returns RG_ERR_INVALID_ARGUMENT
+ * (the reference writes out of bounds) and leaves uvgrid unchanged. */
+rg_status rg_grid_simple(rg_context *ctx, double *uvgrid, int grid_size, double theta, const rg_vis *vis,
+                         int flags);
+
 /* W-projection that allocates nothing.  No counterpart in the reference.
  * For callers that cannot allocate device memory or let a library do it:
  * code running while another framework owns the device memory pool and its

@@ -74,6 +74,8 @@ def lib():
         L.rgo_wtowers_census.argtypes = [i, d, i64, vp, vp, vp, i, i, d, vp, vp]
         L.rgo_grid_wtowers.restype = ct.c_uint64
         L.rgo_weight.argtypes = [i, d, i64, vp, vp, vp]
+        L.rgo_grid_simple.argtypes = [vp, i, d, i64, vp, vp, vp]
+        L.rgo_grid_simple.restype = i
         L.rgo_make_hermitian.argtypes = [vp, i]
         L.rgo_fft_shift.argtypes = [vp, i]
         L.rgo_image_from_grid.argtypes = [vp, i, vp]
@@ -137,6 +139,15 @@ def wtowers_census(grid_size, theta, u, v, w, subgrid, margin, winc):
     lib().rgo_wtowers_census(grid_size, theta, len(u), _ptr(u), _ptr(v), _ptr(w), subgrid, margin, winc,
                              _ptr(nv), _ptr(nf))
     return nv, nf
+
+
+def grid_simple(grid_size, theta, u, v, vis):
+    """grid.c:83-99 restated (nearest-cell gridding)."""
+    u, v, _, vis = _flat(u, v, u, vis)
+    grid = np.zeros((grid_size, grid_size), np.complex128)
+    if lib().rgo_grid_simple(_ptr(grid), grid_size, theta, len(u), _ptr(u), _ptr(v), _ptr(vis)):
+        raise ValueError("a visibility's cell lies off the grid")
+    return grid
 
 
 def weight(grid_size, theta, u, v, vis):
@@ -330,6 +341,8 @@ def ref_lib(omp=False):
                                    ct.POINTER(WKernData), ct.c_int, ct.c_int, ct.c_double]
         L.grid_wtowers.restype = ct.c_uint64
         L.weight.argtypes = [vp, ct.c_int, ct.c_double, ct.POINTER(VisData)]
+        L.grid_simple.argtypes = [vp, ct.c_int, ct.c_double, ct.POINTER(VisData)]
+        L.grid_simple.restype = ct.c_uint64
         L.make_hermitian.argtypes = [vp, ct.c_int]
         L.convolve_aw_kernels.argtypes = [ct.POINTER(BlData), ct.POINTER(WKernData), ct.POINTER(AKernelData)]
         L.grid_awprojection.argtypes = [vp, ct.c_int, ct.c_double, ct.POINTER(VisData), ct.POINTER(WKernData),
@@ -432,6 +445,13 @@ def ref_grid_awprojection(grid_size, theta, obs, wk, ak):
     for b in range(r.vd.bl_count):  # the kernels convolve_aw_kernels allocated
         libc.free(r.bl[b].awkern)
         r.bl[b].awkern = None
+    return grid
+
+
+def ref_grid_simple(grid_size, theta, obs):
+    r = RefInputs(obs)
+    grid = np.zeros((grid_size, grid_size), np.complex128)
+    ref_lib().grid_simple(_ptr(grid), grid_size, theta, ct.byref(r.vd))
     return grid
 
 

@@ -332,6 +332,24 @@ static int nearest_cell(int grid_size, double theta, double u, double v)
     return (y + grid_size / 2) * grid_size + (x + grid_size / 2);
 }
 
+/* grid.c:83-99: each visibility added to its nearest cell (grid.c:27-35).
+ * Returns 1 (nothing written past the grid) when a cell lies off the grid. */
+int rgo_grid_simple(double complex *uvgrid, int grid_size, double theta, int64_t nvis, const double *u,
+                    const double *v, const double complex *vis)
+{
+    int bad = 0;
+    for (int64_t i = 0; i < nvis; i++) {
+        int x = (int)floor(theta * u[i] + .5), y = (int)floor(theta * v[i] + .5);
+        if (x + grid_size / 2 < 0 || x + grid_size / 2 >= grid_size || y + grid_size / 2 < 0 ||
+            y + grid_size / 2 >= grid_size) {
+            bad = 1;
+            continue;
+        }
+        uvgrid[nearest_cell(grid_size, theta, u[i], v[i])] += vis[i];
+    }
+    return bad;
+}
+
 /* grid.c:59-81 */
 void rgo_weight(int grid_size, double theta, int64_t nvis, const double *u,
                 const double *v, double complex *vis)

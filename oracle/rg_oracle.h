@@ -65,6 +65,10 @@ void rgo_wtowers_census(int grid_size, double theta, int64_t nvis, const double 
                         const double *w, int subgrid_size, int subgrid_margin, double wincrement,
                         int64_t *vis_per_tower, int32_t *floors_per_tower);
 
+/* grid.c:83-99: nearest-cell gridding; 1 when a cell lies off the grid. */
+int rgo_grid_simple(double complex *uvgrid, int grid_size, double theta, int64_t nvis, const double *u,
+                    const double *v, const double complex *vis);
+
 /* grid.c:59-81: uniform weighting, vis[i] /= count of visibilities in its cell. */
 void rgo_weight(int grid_size, double theta, int64_t nvis, const double *u,
                 const double *v, double complex *vis);

@@ -48,7 +48,7 @@ EXPORTS = [
     "rg_image_dft_host_flat", "rg_wtowers_tower_count", "rg_wtowers_tower_loads", "rg_wtowers_partition",
     "rg_grid_wtowers_part", "rg_wkern_generate", "rg_pswf0", "rg_wstack_predict", "rg_grid_awprojection",
     "rg_read_vis_bl_hdf5", "rg_free_vis_bl_data", "rg_read_akern_hdf5", "rg_free_akern_data",
-    "rg_write_akern_hdf5",
+    "rg_write_akern_hdf5", "rg_grid_simple",
 ]
 
 
@@ -175,6 +175,7 @@ def lib():
         L.rg_wtowers_partition.argtypes = [vp, vp, i, i, d, vp]
         L.rg_grid_wtowers_part.argtypes = [vp, vp, i, d, ct.POINTER(_Vis), ct.POINTER(_WKern), i, i, d, i, vp, i]
         L.rg_wkern_generate.argtypes = [vp, d, vp, i, i, i, d, i, vp]
+        L.rg_grid_simple.argtypes = [vp, vp, i, d, ct.POINTER(_Vis), i]
         L.rg_grid_awprojection.argtypes = [vp, vp, i, d, ct.POINTER(_VisBL), ct.POINTER(_WKern), ct.POINTER(_AKern),
                                            i, i, i]
         L.rg_read_vis_bl_hdf5.argtypes = [ct.c_char_p, d, d, ct.POINTER(_VisBL)]
@@ -422,6 +423,12 @@ class Context:
         _check(lib().rg_grid_wtowers_batch(self._h, count, gp, int(grid_size), float(theta), vs, ct.byref(s),
                                            int(subgrid_size), int(subgrid_margin), float(wincrement), int(flags)))
         return uvgrids
+
+    def grid_simple(self, uvgrid, grid_size, theta, vis: Visibilities, flags=RG_GRID_ACCUMULATE):
+        """rg_grid_simple (grid_simple, src/reference/grid.c:83-99)."""
+        vs = vis.struct()
+        _check(lib().rg_grid_simple(self._h, _ptr(uvgrid), int(grid_size), float(theta), ct.byref(vs), int(flags)))
+        return uvgrid
 
     def weight(self, grid_size, theta, vis: Visibilities, out=None):
         if out is None:

@@ -38,6 +38,7 @@ static void help()
         "\t-grid                uv grid output file (complex128, after make_hermitian)\n"
         "\t-weight              uniform weighting before gridding\n"
         "\t-akern               A-kernel file: AW-projection with -wkernel (src/reference/main.c:32)\n"
+        "\t-simple              nearest-cell gridding, no w-kernel (grid_CPU.out without --wkern)\n"
         "\t-learned             learned w-kernel parameter file (float32, W-projection)\n"
         "\t-learned_ksize       learned kernel support (Default: 16)\n"
         "\t-learned_wmax        learned kernel w range it was trained on (Default: 2000)\n"
@@ -92,7 +93,8 @@ int main(int argc, char **argv)
     }
     const bool wproj = has(argc, argv, "wproj");
     value(argc, argv, "learned", &learned);
-    if (!value(argc, argv, "wkernel", &wkfile) && learned.empty()) {
+    const bool simple = has(argc, argv, "simple");
+    if (!value(argc, argv, "wkernel", &wkfile) && learned.empty() && !simple) {
         std::printf("No W-Kernel File Specified!! \n");
         help();
         return 0;
@@ -111,7 +113,8 @@ int main(int argc, char **argv)
     const int device = (int)number(argc, argv, "device", 0);
     const double bl_min = number(argc, argv, "bl_min", 0), bl_max = number(argc, argv, "bl_max", DBL_MAX);
     const bool awproj = has(argc, argv, "akern");
-    if (!wproj && !awproj && (!has(argc, argv, "subgrid") || !has(argc, argv, "margin") || !has(argc, argv, "winc"))) {
+    if (!wproj && !awproj && !simple &&
+        (!has(argc, argv, "subgrid") || !has(argc, argv, "margin") || !has(argc, argv, "winc"))) {
         std::printf("Missing W-Towers Parameters. Check subgrid/margin/winc\n");
         help();
         return 0;
@@ -184,7 +187,10 @@ int main(int argc, char **argv)
     rg_vis vis = {vd.u, vd.v, vd.w, vd.vis, vd.n};
     std::vector<double> grid((size_t)N * N * 2, 0.0);
     rg_context_set_profiling(ctx, 1);
-    if (!learned.empty()) {
+    if (simple) {  // grid_CPU.out without a w-kernel file (src/reference/main.c:200-206)
+        std::printf("Gridder: Simple imaging\n");
+        if (rg_grid_simple(ctx, grid.data(), N, theta, &vis, RG_GRID_OVERWRITE) != RG_OK) return die("gridding");
+    } else if (!learned.empty()) {
         rg_mlp *mlp;
         const int lk = (int)number(argc, argv, "learned_ksize", 16);
         const double lw = number(argc, argv, "learned_wmax", 2000.0);

@@ -186,6 +186,53 @@ void launch_weight_apply(cudaStream_t s, const double *u, const double *v, const
     weight_apply_kernel<<<blocks_for(nvis), 256, 0, s>>>(u, v, vis, out, nvis, n, theta, count);
 }
 
+// grid_simple (src/reference/grid.c:83-99): each visibility added to its
+// nearest cell, FP64 atomics on the master grid; a cell off the grid sets
+// DERR_GRID_RANGE (the reference writes out of bounds).
+__global__ void simple_grid_kernel(const double *__restrict__ u, const double *__restrict__ v,
+                                   const double2 *__restrict__ vis, int64_t nvis, int n, double theta,
+                                   double2 *__restrict__ grid, unsigned *err)
+{
+    bool bad = false;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nvis;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double uu = u[i], vv = v[i];
+        if (!isfinite(uu) || !isfinite(vv) || fabs(theta * uu) > 1e9 || fabs(theta * vv) > 1e9) {
+            bad = true;
+            continue;
+        }
+        const int64_t c = nearest_cell(uu, vv, n, theta);
+        if (c < 0) {
+            bad = true;
+            continue;
+        }
+        const double2 z = vis[i];
+        atomicAdd(&grid[c].x, z.x);
+        atomicAdd(&grid[c].y, z.y);
+    }
+    if (bad) atomicOr(err, DERR_GRID_RANGE);
+}
+
+__global__ void add_f64_kernel(const double2 *__restrict__ src, double2 *__restrict__ dst, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 a = src[i], b = dst[i];
+        dst[i] = make_double2(b.x + a.x, b.y + a.y);
+    }
+}
+
+void launch_add_f64(cudaStream_t s, const double2 *src, double2 *dst, int64_t n)
+{
+    add_f64_kernel<<<blocks_for(n), 256, 0, s>>>(src, dst, n);
+}
+
+void launch_simple_grid(cudaStream_t s, const double *u, const double *v, const double2 *vis, int64_t nvis, int n,
+                        double theta, double2 *grid, unsigned *err)
+{
+    simple_grid_kernel<<<blocks_for(nvis), 256, 0, s>>>(u, v, vis, nvis, n, theta, grid, err);
+}
+
 __global__ void add_f32_to_f64_kernel(const float2 *__restrict__ src, double2 *__restrict__ dst,
                                       int64_t n, int overwrite)
 {

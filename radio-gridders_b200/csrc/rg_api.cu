@@ -1222,6 +1222,44 @@ rg_status rg_weight(rg_context *ctx, int grid_size, double theta, const rg_vis *
     return RG_OK;
 }
 
+rg_status rg_grid_simple(rg_context *ctx, double *uvgrid, int grid_size, double theta, const rg_vis *vis, int flags)
+{
+    if (!ctx || !uvgrid) return fail(RG_ERR_INVALID_ARGUMENT, "ctx and uvgrid must be non-NULL");
+    if (grid_size < 2 || grid_size > 16384) return fail(RG_ERR_UNSUPPORTED, "grid_size must be in [2, 16384]");
+    if (!(theta > 0.0) || !std::isfinite(theta)) return fail(RG_ERR_INVALID_ARGUMENT, "theta must be > 0");
+    RG_CHECK(check_vis(vis));
+    RG_CUDA(cudaSetDevice(ctx->device));
+    begin_call(ctx);
+    DevVis dv;
+    RG_CHECK(stage_vis(ctx, vis, &dv));
+    const int64_t cells = (int64_t)grid_size * grid_size;
+    Diag d;
+    RG_CHECK(diag_begin(ctx, &d));
+    // accumulate into a scratch copy, so a call rejected for its data leaves
+    // the caller's grid as it was
+    void *acc;
+    RG_CHECK(scratch(ctx, "simple_grid", sizeof(double2) * (size_t)cells, &acc));
+    RG_CUDA(cudaMemsetAsync(acc, 0, sizeof(double2) * (size_t)cells, ctx->stream));
+    if (dv.n > 0) {
+        launch_simple_grid(ctx->stream, dv.u, dv.v, dv.vis, dv.n, grid_size, theta, (double2 *)acc, d.err);
+        ctx->launches++;
+        RG_CHECK(check_launch("simple gridding"));
+    }
+    RG_CHECK(diag_end(ctx, d, nullptr));
+    OutView ov;
+    RG_CHECK(out_view(ctx, uvgrid, sizeof(double2) * (size_t)cells, "out_grid", !(flags & RG_GRID_OVERWRITE), &ov));
+    if (flags & RG_GRID_OVERWRITE)
+        RG_CUDA(cudaMemcpyAsync(ov.dev, acc, sizeof(double2) * (size_t)cells, cudaMemcpyDeviceToDevice, ctx->stream));
+    else
+        launch_add_f64(ctx->stream, (const double2 *)acc, (double2 *)ov.dev, cells);
+    RG_CHECK(check_launch("grid accumulation"));
+    RG_CHECK(finish_out(ctx, ov));
+    RG_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->stats[0] = dv.n;
+    ctx->stats[5] = ctx->launches;
+    return RG_OK;
+}
+
 static rg_status grid_inplace(rg_context *ctx, double *uvgrid, int grid_size, int op)
 {
     if (!ctx || !uvgrid) return fail(RG_ERR_INVALID_ARGUMENT, "ctx and uvgrid must be non-NULL");

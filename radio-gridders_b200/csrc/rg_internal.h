@@ -198,6 +198,9 @@ void launch_weight_apply(cudaStream_t s, const double *u, const double *v,
                          const unsigned *count);
 void launch_add_f32_to_f64(cudaStream_t s, const float2 *src, double2 *dst, int64_t n,
                            int overwrite);
+void launch_add_f64(cudaStream_t s, const double2 *src, double2 *dst, int64_t n);
+void launch_simple_grid(cudaStream_t s, const double *u, const double *v, const double2 *vis, int64_t nvis, int n,
+                        double theta, double2 *grid, unsigned *err);
 
 // k_fft.cu — FP32 four-step FFTs for power-of-two n in [64, 1024]
 bool fft32_supported(int n);

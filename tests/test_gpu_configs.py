@@ -181,3 +181,25 @@ def test_grid_out_weight(rg, sim, oracle, tmp_path):
     assert rel_rms(grid, oracle.make_hermitian(ref.copy())) < TOL
     img = np.fromfile(f"{d}/w.img", np.float64).reshape(n, n)
     assert rel_rms(img, oracle.image_from_grid(ref.copy())) < TOL
+
+
+def test_grid_out_simple(rg, sim, oracle, tmp_path):
+    """grid.out -simple: grid_CPU.out's nearest-cell gridder (no w-kernel file,
+    src/reference/main.c:200-206) from a visibility file, image as main.c
+    forms it."""
+    obs = sim.wproj_plain(seed=9, n_dump=16)
+    n_bl, n_time = obs.uvw.shape[:2]
+    rg.write_vis_hdf5(str(tmp_path / "vis.h5"), obs.antenna1, obs.antenna2, np.broadcast_to(obs.time, (n_bl, n_time)),
+                      obs.freq, obs.uvw, obs.vis)
+    th, n = obs.meta["theta"], obs.meta["grid_size"]
+    u, v, w, vis = obs.flat()
+    binary = os.path.join(os.path.dirname(__file__), "..", "radio-gridders_b200", "bin", "grid.out")
+    r = subprocess.run([binary, f"-vis={tmp_path}/vis.h5", f"-theta={th}", f"-lambda={obs.meta['lam']}", "-simple",
+                        f"-image={tmp_path}/s.img", f"-grid={tmp_path}/s.grid"], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0 and "Simple imaging" in r.stdout, r.stdout + r.stderr
+    ref = oracle.grid_simple(n, th, u, v, vis)
+    grid = np.fromfile(f"{tmp_path}/s.grid", np.float64).view(np.complex128).reshape(n, n)
+    assert rel_rms(grid, oracle.make_hermitian(ref.copy())) < 1e-14
+    img = np.fromfile(f"{tmp_path}/s.img", np.float64).reshape(n, n)
+    assert rel_rms(img, oracle.image_from_grid(ref.copy())) < 1e-12

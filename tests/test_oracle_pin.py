@@ -167,3 +167,14 @@ def test_awprojection_restatement_matches_reference(sim, oracle, rg):
     assert np.array_equal(got, ref)
     wp = oracle.grid_wprojection(n, th, u, v, w, vis, wk)
     assert np.linalg.norm(got - wp) / np.linalg.norm(wp) > 1e-6
+
+
+def test_grid_simple_restatement_matches_reference(sim, oracle):
+    """grid_simple (src/reference/grid.c:83-99): the restatement and the
+    reference's build give bit-identical grids."""
+    if not oracle.reference_available():
+        pytest.skip("reference build absent")
+    obs = sim.wproj_plain(seed=4, n_dump=8)
+    u, v, w, vis = obs.flat()
+    n, th = obs.meta["grid_size"], obs.meta["theta"]
+    assert np.array_equal(oracle.grid_simple(n, th, u, v, vis), oracle.ref_grid_simple(n, th, obs))
