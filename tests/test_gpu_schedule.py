@@ -93,7 +93,7 @@ def test_autotune_choices_and_results(rg, sim, case):
         out[tune] = g.copy()
         assert st["romein_points"] in (2, 4, 8) and st["group_items_per_sm"] in (4, 8, 16)
         if not tune:
-            assert (st["romein_points"], st["group_items_per_sm"]) == (4, 8)
+            assert (st["romein_points"], st["group_items_per_sm"]) == (8, 8)
     assert rel_rms(out[True], out[False]) < 1e-6
 
 
