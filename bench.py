@@ -673,7 +673,7 @@ def towers_image_error(ctx, oversampling=8, w_step=1.0):
             "region": "central half of each axis", "dft_s": time.time() - t0}
 
 
-def learned_towers(ctx, config="C1", steps=120000, n_triples=16384):
+def study_learned_towers(ctx, config="C1", steps=120000, n_triples=16384):
     """Learned-kernel W-towers against the table W-towers on the same
     workload: a network trained on the GPU (own forward/backward kernels) on
     generator kernels over the residual w range |w - w_mid| <= winc/2, then
@@ -936,7 +936,7 @@ def run_study(which):
         print(json.dumps({"study": "winc_sweep", **winc_sweep(ctx)}), flush=True)
     elif which in ("learned_towers", "learned_towers_c4"):
         cfg = "C4" if which.endswith("c4") else "C1"
-        print(json.dumps({"study": "learned_towers", **learned_towers(ctx, cfg)}), flush=True)
+        print(json.dumps({"study": "learned_towers", **study_learned_towers(ctx, cfg)}), flush=True)
     ctx.close()
     return 0
 

@@ -233,3 +233,18 @@ def test_grid_simple_matches_oracle(rg, ctx, oracle, wproj_data):
     with pytest.raises(rg.RGError):
         ctx.grid_simple(g, n, th, V(rg, far, v, w, vis))
     assert np.array_equal(g, keep)
+
+
+def test_wtowers_grid_size_not_a_power_of_two(rg, ctx, sim, oracle):
+    """grid.out's grid size floor(lambda * theta) is rarely a power of two:
+    W-towers at N = 2500 (6 x 6 towers of 496 cells, the last ones clipped at
+    the grid edge) against the oracle."""
+    obs = sim.wtowers_plain(seed=7, n_st=48, n_dump=8, n_chan=2, lam=25000.0)
+    n, th = obs.meta["grid_size"], obs.meta["theta"]
+    assert n == 2500
+    u, v, w, vis = obs.flat()
+    wkt = sim.generate_wkernel(th, np.arange(-6, 7, 1.0), 16, 16)
+    g = np.zeros((n, n), np.complex128)
+    ctx.grid_wtowers(g, n, th, V(rg, u, v, w, vis), wkt, 512, 16, 10.0)
+    ref = oracle.grid_wtowers(n, th, u, v, w, vis, wkt, 512, 16, 10.0)
+    assert rel_rms(g, ref) < TOL
