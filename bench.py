@@ -504,9 +504,10 @@ def run_b200(args, rank, world, local_rank):
         with open(tpath) as f:
             tdoc = json.load(f)
         entry = tdoc.get(dom)
-        traffic = entry["dram_bytes"] if isinstance(entry, dict) else entry
+        traffic = entry["dram_bytes"] if isinstance(entry, dict) else entry  # None for a kernel not captured
         traffic_src = ("profiles/wtowers_traffic.json: ncu dram__bytes_read.sum + dram__bytes_write.sum per launch "
-                       "of the same workload, captured separately (not this run)")
+                       "on the 128-station case, scaled to this workload by the kernel's algorithmic bytes; "
+                       "captured separately (not this run)") if entry else None
     path_bytes = algorithmic_bytes(stats, nvis)
     # the bytes no implementation avoids: 20 B per visibility in (f32 u, v, w
     # and complex64) and the FP64 master grid out
