@@ -64,9 +64,6 @@ def parse():
                    help="keep the default schedule (Romein 8 points per thread, 8 row-stage items per SM: the "
                         "tuner's usual choice here) instead of timing candidates; for profiled runs, whose "
                         "serialised launches would skew the tuner")
-    p.add_argument("--gridder", choices=["auto", "romein", "strip"], default="auto",
-                   help="W-towers gridder: the tuner's choice (auto), Romein's scatter gridder, or the strip "
-                        "gridder (per-strip lists, shared-memory gridding fused with the column transform)")
     p.add_argument("--study", choices=STUDIES, default=None,
                    help="run one of the studies beside the headline line instead (one JSON object each)")
     p.add_argument("--stations", type=int, default=256,
@@ -166,13 +163,6 @@ class Clocks:
 
 STAGES = ("prepare", "romein", "fft_cols_backward", "tower_rows", "tower_finish", "fft_cols_forward",
           "add_back")
-# with the strip gridder, gridding and the backward column transform are its
-# two stages instead
-STAGES_STRIP = ("prepare", "strip_lists", "strip_grid", "tower_rows", "tower_finish", "fft_cols_forward",
-                "add_back")
-# list entries per visibility for 16-tap footprints over 8-column strips: a
-# footprint starting at column offset a (mod 8) spans (a + 15) // 8 + 1 strips
-STRIP_ENTRIES_PER_VIS = 23 / 8
 
 
 def stage_bytes(stage, stats, nvis):
@@ -187,9 +177,6 @@ def stage_bytes(stage, stats, nvis):
     return {
         "prepare": 40 * nvis + 24 * nvis,                   # f64 uvw + c128 in, record + c64 out
         "romein": 24 * nvis + strip,                        # records + vis in, marked strips out
-        # records in twice (count, fill), 16 B list entries out
-        "strip_lists": int(40 * nvis + 16 * STRIP_ENTRIES_PER_VIS * nvis),
-        "strip_grid": int(16 * STRIP_ENTRIES_PER_VIS * nvis) + strip,  # entries in, marked strips out
         "fft_cols_backward": 2 * strip,                     # marked strips in place
         "tower_rows": 2 * strip + 8 * s2 * ng,              # strips in + cleared, partials out
         "tower_finish": 8 * s2 * ng + 8 * s2 * nt,          # partials in, sub-images out
@@ -200,7 +187,7 @@ def stage_bytes(stage, stats, nvis):
 
 def algorithmic_bytes(stats, nvis):
     """Bytes per step of the sparse dataflow: the sum over its stages."""
-    return sum(stage_bytes(k, stats, nvis) for k in (STAGES_STRIP if stats.get("strip_gridder") else STAGES))
+    return sum(stage_bytes(k, stats, nvis) for k in STAGES)
 
 
 def dense_dataflow_bytes(stats, nvis):
@@ -338,8 +325,6 @@ def run_b200(args, rank, world, local_rank):
     ctx.set_stream(stream.cuda_stream)
     if args.no_autotune:
         ctx.set_autotune(False)
-    ctx.set_wtowers_gridder({"auto": rg.RG_WTOWERS_GRIDDER_AUTO, "romein": rg.RG_WTOWERS_GRIDDER_ROMEIN,
-                             "strip": rg.RG_WTOWERS_GRIDDER_STRIP}[args.gridder])
 
     # inputs resident in HBM
     du = torch.from_numpy(u).to(dev)
@@ -543,9 +528,7 @@ def run_b200(args, rank, world, local_rank):
                                    "reduced over NCCL") if world > 1 else "1 GPU",
                    "l2": "256 MiB buffer written between steps, outside each step's event pair",
                    "precision": "FP32 sub-grids and transforms; FP64 coordinates, Fresnel phase and master grid",
-                   "schedule": {"gridder": "strip" if stats["strip_gridder"] else "romein",
-                                "gridder_choice": args.gridder,
-                                "romein_points_per_thread": stats["romein_points"],
+                   "schedule": {"romein_points_per_thread": stats["romein_points"],
                                 "row_stage_items_per_sm": stats["group_items_per_sm"],
                                 "graph_replay": bool(stats["graph"]), "autotuned": not args.no_autotune},
                    "marked_strips": stats["marked_strips"], "floor_groups": stats["floor_groups"]},

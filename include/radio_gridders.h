@@ -97,8 +97,7 @@ const char *rg_last_error(void);
  * columns holding data (the strips the transforms touch), 7 floor groups of
  * the row stage, 8 Romein grid points per thread and 9 row-stage work items
  * per SM in use (the tuned schedule), 10 one when the pass ran as a captured
- * graph, 11 one when the strip gridder ran in place of Romein's (see
- * rg_context_set_wtowers_gridder).
+ * graph.
  * Returns the count written (<= n). */
 int rg_last_stats(rg_context *ctx, int64_t *out, int n);
 
@@ -123,20 +122,6 @@ int rg_last_timings(rg_context *ctx, const char **names, float *ms, int n);
  * fall back to ordinary launches and capture again. */
 rg_status rg_context_set_autotune(rg_context *ctx, int enabled);
 rg_status rg_context_set_graphs(rg_context *ctx, int enabled);
-
-/* W-towers gridding of table taps comes in two forms.  Romein's scatter
- * gridder fills each (tower, w-floor) sub-grid in HBM with 8-byte atomics and
- * a separate kernel then applies the backward column transform to the marked
- * column strips.  The strip gridder lists each strip's visibilities first and
- * grids one strip at a time in shared memory, applying the column transform in
- * the same kernel (sub-grids of 256 or 512, 8 or 16 taps; other shapes use
- * Romein's).  AUTO (default): the autotuner times both and keeps the faster
- * per shape; untuned passes use Romein's.  Changing the choice drops the
- * context's tuned schedules and captured passes. */
-#define RG_WTOWERS_GRIDDER_AUTO 0
-#define RG_WTOWERS_GRIDDER_ROMEIN 1
-#define RG_WTOWERS_GRIDDER_STRIP 2
-rg_status rg_context_set_wtowers_gridder(rg_context *ctx, int gridder);
 
 /* ---- gridders ---------------------------------------------------------- */
 

@@ -27,7 +27,6 @@ LIB_PATH = os.path.join(HERE, "librg_b200.so")
 
 RG_GRID_ACCUMULATE = 0
 RG_GRID_OVERWRITE = 1
-RG_WTOWERS_GRIDDER_AUTO, RG_WTOWERS_GRIDDER_ROMEIN, RG_WTOWERS_GRIDDER_STRIP = 0, 1, 2
 RG_DFT_FP32_NAIVE = 0
 RG_DFT_FP64_REDUCED = 1
 RG_DFT_FP64 = 2
@@ -39,7 +38,6 @@ STATUS = {0: "RG_OK", 1: "RG_ERR_INVALID_ARGUMENT", 2: "RG_ERR_CUDA", 3: "RG_ERR
 EXPORTS = [
     "rg_context_create", "rg_context_destroy", "rg_context_set_stream", "rg_last_error",
     "rg_last_stats", "rg_context_set_profiling", "rg_context_set_autotune", "rg_context_set_graphs",
-    "rg_context_set_wtowers_gridder",
     "rg_last_timings", "rg_grid_wprojection", "rg_grid_wtowers", "rg_weight",
     "rg_make_hermitian", "rg_fft_shift", "rg_image_from_grid", "rg_fft2d", "rg_dft_image",
     "rg_grid_wprojection_noalloc", "rg_mlp_param_count", "rg_mlp_create", "rg_mlp_destroy",
@@ -167,7 +165,6 @@ def lib():
         L.rg_context_set_profiling.argtypes = [vp, i]
         L.rg_context_set_autotune.argtypes = [vp, i]
         L.rg_context_set_graphs.argtypes = [vp, i]
-        L.rg_context_set_wtowers_gridder.argtypes = [vp, i]
         L.rg_last_timings.argtypes = [vp, ct.POINTER(ct.c_char_p), ct.POINTER(ct.c_float), i]
         L.rg_last_timings.restype = i
         L.rg_grid_wprojection.argtypes = [vp, vp, i, d, ct.POINTER(_Vis), ct.POINTER(_WKern), i]
@@ -313,10 +310,6 @@ class Context:
     def set_graphs(self, enabled=True):
         _check(lib().rg_context_set_graphs(self._h, int(bool(enabled))))
 
-    def set_wtowers_gridder(self, gridder=RG_WTOWERS_GRIDDER_AUTO):
-        """RG_WTOWERS_GRIDDER_AUTO (the tuner's choice), _ROMEIN or _STRIP."""
-        _check(lib().rg_context_set_wtowers_gridder(self._h, int(gridder)))
-
     def set_profiling(self, enabled=True):
         _check(lib().rg_context_set_profiling(self._h, 1 if enabled else 0))
 
@@ -334,11 +327,10 @@ class Context:
         return [(names[k].decode(), float(ms[k])) for k in range(n)]
 
     def last_stats(self):
-        out = (ct.c_int64 * 12)()
-        n = lib().rg_last_stats(self._h, out, 12)
+        out = (ct.c_int64 * 11)()
+        n = lib().rg_last_stats(self._h, out, 11)
         keys = ["gridded", "active_subgrids", "towers_with_data", "floors", "dropped", "launches",
-                "marked_strips", "floor_groups", "romein_points", "group_items_per_sm", "graph",
-                "strip_gridder"]
+                "marked_strips", "floor_groups", "romein_points", "group_items_per_sm", "graph"]
         return {k: int(out[j]) for j, k in enumerate(keys[:n])}
 
     # ---- gridders (src/reference/grid.h:121-126) -------------------------

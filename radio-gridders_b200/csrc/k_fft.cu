@@ -322,197 +322,6 @@ __global__ void __launch_bounds__(kSparseColThreads) sparse_cols_kernel(
 }
 
 // ---------------------------------------------------------------------------
-// Strip gridder: gridding and the backward column transform of one marked
-// (sub-grid, strip) pair in one CTA, the strip held in shared memory, so the
-// gridded values never travel through HBM and need no global atomics.
-//
-// The visibilities whose footprints reach the strip are listed per (slot,
-// strip) beforehand (launch_strip_lists), as entries {goff, slice offset,
-// visibility}.  Gridding follows Romein's ownership scheme inside the strip:
-// lane (c, q) of a warp owns strip column c and the rows congruent to q + 4j
-// modulo K (j < K/4), so for each visibility it meets exactly one tap per
-// owned row class — footprint column tx with (goff + tx) mod S = the column,
-// footprint row ty = (q + 4j - rb) mod K with rb the footprint's first row in
-// that column — and keeps the sum for its current point in registers, adding
-// it to the strip (a shared-memory atomic: the four warps take quarters of the
-// list) only when the point changes.  Per tap grid += vis * conj(tap) at the
-// reference's linear index goff + ty * S + tx (src/reference/grid.c:177-182),
-// rows outside the sub-grid dropped.  The strip (S rows x 8 columns, rows
-// padded to 9 entries) then goes through the column transform, its exchange
-// buffer reusing the strip's shared memory, and is written to the slot's
-// strip block.  Every marked strip is written, so the sub-grids need no
-// zeroing beforehand.
-// ---------------------------------------------------------------------------
-constexpr int kStripGridThreads = 128;
-constexpr int kStripRowPad = kStripCols + 1;
-
-template <int N1, int K>
-__global__ void __launch_bounds__(kStripGridThreads) strip_grid_kernel(
-    const int4 *__restrict__ entries, const int *__restrict__ off, const int *__restrict__ items,
-    int *__restrict__ ctl, const float2 *__restrict__ taps, float2 *__restrict__ slots, const float2 *__restrict__ tw)
-{
-    using G = StripGeom<N1>;
-    constexpr int N = G::N, C = G::C, STRIPS = N / C, LG = ilog2c(N);
-    constexpr int NW = kStripGridThreads / 32;
-    constexpr int Q = 32 / C;  // row classes per warp
-    constexpr int P = K / Q;   // points per lane
-    static_assert(C == 8 && K % Q == 0 && P >= 1, "8-column strips, K a multiple of 4");
-    static_assert(C * N1 <= kStripGridThreads, "one step-1 item per thread");
-    static_assert(G::T_ELEMS <= N * kStripRowPad, "the exchange buffer fits in the strip's memory");
-    extern __shared__ float2 smem[];
-    float2 *A = smem;  // [N][kStripRowPad]; the column transform's exchange buffer T reuses it
-    float2 *T = smem;
-    float2 *W = smem + N * kStripRowPad;
-    __shared__ int4 stage[kStripGridThreads];
-    __shared__ int s_item;
-    load_twiddles<N1>(W, tw);
-    const int nitems = ctl[0];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int c = lane % C, q = lane / C;
-    for (;;) {
-        __syncthreads();  // the previous item's transform is done with T
-        if (threadIdx.x == 0) s_item = atomicAdd(ctl + 1, 1);
-        for (int e = threadIdx.x; e < N * kStripRowPad; e += kStripGridThreads) A[e] = make_float2(0.f, 0.f);
-        __syncthreads();
-        const int k = s_item;
-        if (k >= nitems) break;
-        const int pair = items[k];
-        const int st = pair % STRIPS;
-        const int q0 = off[pair], len = off[pair + 1] - q0;
-        const int per = (len + NW - 1) / NW;
-        const int w0 = q0 + min(len, warp * per), w1 = q0 + min(len, (warp + 1) * per);
-        const int colabs = st * C + c;
-        int goff_cur = 0, toff = 0, key[P];
-        bool have = false, in = false;
-        float2 sum[P];
-#pragma unroll
-        for (int j = 0; j < P; j++) {
-            key[j] = -1;
-            sum[j] = make_float2(0.f, 0.f);
-        }
-        int4 *stg = stage + warp * 32;
-        for (int b = w0; b < w1; b += 32) {
-            const int m = min(32, w1 - b);
-            __syncwarp();
-            if (lane < m) stg[lane] = entries[b + lane];
-            __syncwarp();
-            for (int i = 0; i < m; i++) {
-                const int4 e = stg[i];
-                if (!have || e.x != goff_cur) {
-                    have = true;
-                    goff_cur = e.x;
-                    const int tx = (colabs - e.x) & (N - 1);
-                    in = tx < K;
-                    const int rb = (e.x + tx) >> LG;  // floor: the footprint's first row in this column
-                    const int ty0 = (q - rb) & (K - 1);
-                    toff = ty0 * K + tx;
-#pragma unroll
-                    for (int j = 0; j < P; j++) {
-                        const int row = rb + ((ty0 + j * Q) & (K - 1));
-                        const int nk = (in && (unsigned)row < (unsigned)N) ? row : -1;
-                        if (nk != key[j]) {
-                            if (key[j] >= 0) {
-                                atomicAdd(&A[key[j] * kStripRowPad + c].x, sum[j].x);
-                                atomicAdd(&A[key[j] * kStripRowPad + c].y, sum[j].y);
-                            }
-                            key[j] = nk;
-                            sum[j] = make_float2(0.f, 0.f);
-                        }
-                    }
-                }
-                if (in) {
-                    const float2 vz = make_float2(__int_as_float(e.z), __int_as_float(e.w));
-                    // duplicated slices (2K rows): rows ty0 + jQ need no wrap
-                    const float2 *tp = taps + 2 * (int64_t)e.y + toff;
-#pragma unroll
-                    for (int j = 0; j < P; j++) {
-                        const float2 t = __ldg(tp + j * Q * K);
-                        sum[j].x = fmaf(vz.x, t.x, fmaf(vz.y, t.y, sum[j].x));
-                        sum[j].y = fmaf(vz.y, t.x, fmaf(-vz.x, t.y, sum[j].y));
-                    }
-                }
-            }
-        }
-#pragma unroll
-        for (int j = 0; j < P; j++)
-            if (key[j] >= 0) {
-                atomicAdd(&A[key[j] * kStripRowPad + c].x, sum[j].x);
-                atomicAdd(&A[key[j] * kStripRowPad + c].y, sum[j].y);
-            }
-        __syncthreads();
-        // backward column transform: step 1 from the strip into registers, then
-        // (after every thread has read) through T, step 2 into the slot's strip
-        {
-            const bool act = threadIdx.x < C * N1;
-            const int cc = threadIdx.x % C, n1 = threadIdx.x / C;
-            float2 a[32];
-            if (act) {
-#pragma unroll
-                for (int n2 = 0; n2 < 32; n2++) a[n2] = A[(n1 + n2 * N1) * kStripRowPad + cc];
-                reg_fft<32, +1>(a);
-            }
-            __syncthreads();
-            if (act) {
-#pragma unroll
-                for (int j = 0; j < 32; j++) {
-                    const int k2 = bitrevc(j, 5);
-                    T[cc * G::CS + n1 * kPad + k2] = cmulf(a[j], twiddle<+1>(W, k2 * N1 + n1));
-                }
-            }
-        }
-        __syncthreads();
-        float2 *col = slots + (int64_t)(pair / STRIPS) * N * N + (int64_t)st * (C * N);
-        for (int it = threadIdx.x; it < C * 32; it += kStripGridThreads) {
-            const int cc = it % C, k2 = it / C;
-            float2 v[N1];
-#pragma unroll
-            for (int n1 = 0; n1 < N1; n1++) v[n1] = T[cc * G::CS + n1 * kPad + k2];
-            reg_fft<N1, +1>(v);
-#pragma unroll
-            for (int j = 0; j < N1; j++) col[(k2 + 32 * bitrevc(j, G::LB)) * C + cc] = v[j];
-        }
-    }
-}
-
-template <int N1>
-static size_t strip_grid_smem()
-{
-    return sizeof(float2) * ((size_t)N1 * 32 * kStripRowPad + N1 * 32);
-}
-
-template <int N1, int K>
-static void strip_grid_impl(cudaStream_t s, const int4 *entries, const int *off, const int *items, int *ctl,
-                            const float2 *taps, float2 *slots, const float2 *tw, int sm_count)
-{
-    const size_t sm = strip_grid_smem<N1>();
-    cudaFuncSetAttribute(strip_grid_kernel<N1, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, strip_grid_kernel<N1, K>, kStripGridThreads, sm);
-    if (per_sm < 1) per_sm = 1;
-    strip_grid_kernel<N1, K><<<(unsigned)(per_sm * sm_count), kStripGridThreads, sm, s>>>(entries, off, items, ctl,
-                                                                                        taps, slots, tw);
-}
-
-bool strip_grid_supported(int subgrid, int ksize)
-{
-    return (subgrid == 256 || subgrid == 512) && (ksize == 8 || ksize == 16);
-}
-
-void launch_strip_grid(cudaStream_t s, const int4 *entries, const int *off, const int *items, int *ctl,
-                       const float2 *taps, float2 *slots, int subgrid, int ksize, const float2 *tw, int sm_count)
-{
-#define RG_SG(N1, K) strip_grid_impl<N1, K>(s, entries, off, items, ctl, taps, slots, tw, sm_count)
-    if (subgrid == 512) {
-        if (ksize == 16) RG_SG(16, 16);
-        else if (ksize == 8) RG_SG(16, 8);
-    } else if (subgrid == 256) {
-        if (ksize == 16) RG_SG(8, 16);
-        else if (ksize == 8) RG_SG(8, 8);
-    }
-#undef RG_SG
-}
-
-// ---------------------------------------------------------------------------
 // Row stage, in two kernels so uneven towers balance.
 //
 // tower_rows_kernel: CTA = (floor group, strip of R rows).  For each floor of

@@ -578,147 +578,4 @@ void launch_compact_bins(cudaStream_t s, const int *active, const int *range, in
                                            tower_group_count);
 }
 
-// ---------------------------------------------------------------------------
-// Per-(sub-grid, strip) visibility lists for the strip gridder.
-//
-// A record's footprint covers the sub-grid columns (goff + tx) mod S, tx < K:
-// ((goff mod S) mod 8 + K - 1) / 8 + 1 consecutive strips, cyclically — the
-// strips prepare_towers marks.  strip_count_kernel counts the records of each
-// (slot, strip), strip_scan_kernel turns the counts into list offsets and
-// lists the marked (slot, strip) pairs, strip_fill_kernel writes each record's
-// entry {goff, slice offset, visibility} into the lists of its strips.  Lanes
-// of a warp bound for the same list share one atomic.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ int strip_span(const int4 &r, const int *__restrict__ slot_of_bin, int slot_cap, int S,
-                                          int K, int *s0, int *ns)
-{
-    if (r.x < 0) return -1;
-    const int slot = slot_of_bin[r.x];
-    if (slot < 0 || slot >= slot_cap) return -1;
-    const int col0 = r.y & (S - 1);
-    *s0 = col0 / kStripCols;
-    *ns = ((col0 & (kStripCols - 1)) + K - 1) / kStripCols + 1;
-    return slot;
-}
-
-__device__ __forceinline__ int strip_max_span(int K) { return (K + kStripCols - 2) / kStripCols + 1; }
-
-__global__ void strip_count_kernel(const int4 *__restrict__ rec, int64_t n, const int *__restrict__ slot_of_bin,
-                                   int slot_cap, int S, int K, int *__restrict__ cnt)
-{
-    const int strips = S / kStripCols, maxs = strip_max_span(K);
-    const int lane = threadIdx.x & 31;
-    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = base + threadIdx.x;
-        int slot = -1, s0 = 0, ns = 0;
-        if (i < n) slot = strip_span(rec[i], slot_of_bin, slot_cap, S, K, &s0, &ns);
-        for (int t = 0; t < maxs; t++) {
-            const int key = (slot >= 0 && t < ns) ? slot * strips + ((s0 + t) & (strips - 1)) : -1;
-            const unsigned peers = __match_any_sync(0xffffffffu, key);
-            if (key >= 0 && lane == __ffs(peers) - 1) atomicAdd(cnt + key, __popc(peers));
-        }
-    }
-}
-
-// One CTA of 512 threads, kStripScanE consecutive pairs per thread and round.
-constexpr int kStripScanE = 16;
-__global__ void __launch_bounds__(512) strip_scan_kernel(const int *__restrict__ cnt,
-                                                          const unsigned *__restrict__ masks,
-                                                          const int *__restrict__ counts, int slot_cap, int strips,
-                                                          int *__restrict__ off, int *__restrict__ cur,
-                                                          int *__restrict__ items, int *__restrict__ ctl)
-{
-    __shared__ int warp_sums[32];
-    const int words = (strips + 31) / 32;
-    const int live = counts[0] < slot_cap ? counts[0] : slot_cap;
-    const int n = live * strips;
-    int carry_e = 0, carry_i = 0;
-    for (int base = 0; base < n; base += (int)blockDim.x * kStripScanE) {
-        const int i0 = base + (int)threadIdx.x * kStripScanE;
-        int c[kStripScanE];
-        unsigned marked = 0;
-        int se = 0, si = 0;
-#pragma unroll
-        for (int e = 0; e < kStripScanE; e++) {
-            const int i = i0 + e;
-            c[e] = 0;
-            if (i < n) {
-                const int slot = i / strips, st = i % strips;
-                c[e] = cnt[i];
-                if ((masks[(int64_t)slot * words + st / 32] >> (st & 31)) & 1u) marked |= 1u << e;
-            }
-            se += c[e];
-        }
-        si = __popc(marked);
-        int te, ti;
-        const int xe = block_exclusive_scan(se, warp_sums, &te);
-        const int xi = block_exclusive_scan(si, warp_sums, &ti);
-        int pe = carry_e + xe, pi = carry_i + xi;
-#pragma unroll
-        for (int e = 0; e < kStripScanE; e++) {
-            const int i = i0 + e;
-            if (i < n) {
-                off[i] = pe;
-                cur[i] = pe;
-                if ((marked >> e) & 1u) items[pi++] = i;
-                pe += c[e];
-            }
-        }
-        carry_e += te;
-        carry_i += ti;
-    }
-    if (threadIdx.x == 0) {
-        off[n] = carry_e;
-        ctl[0] = carry_i;  // marked pairs
-        ctl[1] = 0;        // the gridder's work counter
-    }
-}
-
-__global__ void strip_fill_kernel(const int4 *__restrict__ rec, const float2 *__restrict__ visf, int64_t n,
-                                  const int *__restrict__ slot_of_bin, int slot_cap, int S, int K,
-                                  int *__restrict__ cur, int4 *__restrict__ entries, int64_t entry_cap)
-{
-    const int strips = S / kStripCols, maxs = strip_max_span(K);
-    const int lane = threadIdx.x & 31;
-    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = base + threadIdx.x;
-        int slot = -1, s0 = 0, ns = 0;
-        int4 r = make_int4(-1, 0, 0, 0);
-        float2 vz = make_float2(0.f, 0.f);
-        if (i < n) {
-            r = rec[i];
-            slot = strip_span(r, slot_of_bin, slot_cap, S, K, &s0, &ns);
-            if (slot >= 0) vz = visf[i];
-        }
-        for (int t = 0; t < maxs; t++) {
-            const int key = (slot >= 0 && t < ns) ? slot * strips + ((s0 + t) & (strips - 1)) : -1;
-            const unsigned peers = __match_any_sync(0xffffffffu, key);
-            const int leader = __ffs(peers) - 1;
-            int b = 0;
-            if (key >= 0 && lane == leader) b = atomicAdd(cur + key, __popc(peers));
-            b = __shfl_sync(0xffffffffu, b, leader);
-            const int64_t pos = (int64_t)b + __popc(peers & ((1u << lane) - 1u));
-            if (key >= 0 && pos < entry_cap)
-                entries[pos] = make_int4(r.y, r.z, __float_as_int(vz.x), __float_as_int(vz.y));
-        }
-    }
-}
-
-int strip_max_entries_per_record(int ksize) { return (ksize + kStripCols - 2) / kStripCols + 1; }
-
-void launch_strip_lists(cudaStream_t s, const int4 *rec, const float2 *visf, int64_t n, const int *slot_of_bin,
-                        const unsigned *masks, const int *counts, int slot_cap, int subgrid, int ksize, int *cnt,
-                        int *off, int *cur, int *items, int *ctl, int4 *entries, int64_t entry_cap, int sm_count)
-{
-    const int strips = subgrid / kStripCols;
-    cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)slot_cap * strips, s);
-    int64_t blocks = (n + 255) / 256;
-    if (blocks > (int64_t)sm_count * 8) blocks = (int64_t)sm_count * 8;
-    if (blocks < 1) blocks = 1;
-    strip_count_kernel<<<(unsigned)blocks, 256, 0, s>>>(rec, n, slot_of_bin, slot_cap, subgrid, ksize, cnt);
-    strip_scan_kernel<<<1, 512, 0, s>>>(cnt, masks, counts, slot_cap, strips, off, cur, items, ctl);
-    strip_fill_kernel<<<(unsigned)blocks, 256, 0, s>>>(rec, visf, n, slot_of_bin, slot_cap, subgrid, ksize, cur,
-                                                       entries, entry_cap);
-}
-
 }  // namespace rg

@@ -354,24 +354,6 @@ rg_status rg_context_set_autotune(rg_context *ctx, int enabled)
     return RG_OK;
 }
 
-rg_status rg_context_set_wtowers_gridder(rg_context *ctx, int gridder)
-{
-    if (!ctx) return fail(RG_ERR_INVALID_ARGUMENT, "ctx is NULL");
-    if (gridder < RG_WTOWERS_GRIDDER_AUTO || gridder > RG_WTOWERS_GRIDDER_STRIP)
-        return fail(RG_ERR_INVALID_ARGUMENT, "gridder must be RG_WTOWERS_GRIDDER_AUTO, _ROMEIN or _STRIP");
-    if (gridder == ctx->wt_gridder) return RG_OK;
-    ctx->wt_gridder = gridder;
-    for (auto &kv : ctx->tower_plans) {  // schedules and captured passes were made under the old choice
-        TowerPlan &pl = kv.second;
-        if (pl.graph_exec) cudaGraphExecDestroy(pl.graph_exec);
-        pl.graph_exec = nullptr;
-        pl.graph_key.clear();
-        pl.tuned = false;
-        pl.tune = TowerTuning();
-    }
-    return RG_OK;
-}
-
 rg_status rg_context_set_graphs(rg_context *ctx, int enabled)
 {
     if (!ctx) return fail(RG_ERR_INVALID_ARGUMENT, "ctx is NULL");
@@ -402,7 +384,7 @@ int rg_last_timings(rg_context *ctx, const char **names, float *ms, int n)
 int rg_last_stats(rg_context *ctx, int64_t *out, int n)
 {
     if (!ctx || !out) return 0;
-    int k = n < 12 ? n : 12;
+    int k = n < 11 ? n : 11;
     for (int i = 0; i < k; i++) out[i] = ctx->stats[i];
     return k;
 }
@@ -484,15 +466,6 @@ namespace rg {
 // diagnostics block (error word, counters, counts, floor range) into the
 // context's pinned host buffer; wtowers_check reads it after a sync.  Nothing
 // here synchronises, so the sequence can also be captured into a CUDA graph.
-// The strip gridder runs for table taps where it covers the shape, when the
-// caller chose it or the plan's tuned schedule did.
-static bool use_strip_gridder(const rg_context *ctx, const TowerPlan &pl, bool learned, int S, int K)
-{
-    return !learned && strip_grid_supported(S, K) &&
-           (ctx->wt_gridder == RG_WTOWERS_GRIDDER_STRIP ||
-            (ctx->wt_gridder == RG_WTOWERS_GRIDDER_AUTO && pl.tune.strip_gridder));
-}
-
 static rg_status wtowers_enqueue(rg_context *ctx, const DevVis &dv, const float2 *taps, const rg_wkern *wkern,
                                  const LearnedTaps *lt, double *out_dev, int N, double theta, int S, int M,
                                  double winc, int flags, TowerPlan &pl, void *diag_host = nullptr,
@@ -533,19 +506,6 @@ static rg_status wtowers_enqueue(rg_context *ctx, const DevVis &dv, const float2
     RG_CHECK(scratch(ctx, "slots", sizeof(float2) * (size_t)(sub_cells * pl.slots_cap), &slots));
     RG_CHECK(scratch(ctx, "partial", sizeof(float2) * (size_t)(sub_cells * pl.groups_cap), &partial));
     RG_CHECK(scratch(ctx, "subimg", sizeof(float2) * (size_t)(sub_cells * ntowers), &subimg));
-    const bool strip = use_strip_gridder(ctx, pl, lt != nullptr, S, K);
-    void *scnt = nullptr, *soff = nullptr, *scur = nullptr, *sitems = nullptr, *sctl = nullptr, *sent = nullptr;
-    int64_t entry_cap = 0;
-    if (strip) {
-        const size_t pairs = (size_t)pl.slots_cap * strips;
-        RG_CHECK(scratch(ctx, "strip_count", sizeof(int) * pairs, &scnt));
-        RG_CHECK(scratch(ctx, "strip_offset", sizeof(int) * (pairs + 1), &soff));
-        RG_CHECK(scratch(ctx, "strip_cursor", sizeof(int) * pairs, &scur));
-        RG_CHECK(scratch(ctx, "strip_items", sizeof(int) * pairs, &sitems));
-        RG_CHECK(scratch(ctx, "strip_ctl", sizeof(int) * 2, &sctl));
-        entry_cap = (int64_t)strip_max_entries_per_record(K) * dv.n;
-        RG_CHECK(scratch(ctx, "strip_entries", sizeof(int4) * (size_t)(entry_cap > 0 ? entry_cap : 1), &sent));
-    }
     float2 *tw;
     RG_CHECK(get_twiddles32(ctx, S, &tw));
     {
@@ -610,18 +570,6 @@ static rg_status wtowers_enqueue(rg_context *ctx, const DevVis &dv, const float2
                                   (const int *)slot_of_bin, pl.slots_cap, (float2 *)slots, S, lt->P, lt->PB,
                                   lt->ksize, lt->inv_wmax, lt->scale, ctx->sm_count, d.err);
         end_stage(ctx);
-    } else if (strip) {
-        begin_stage(ctx, "strip_lists");
-        launch_slot_masks(st, (const unsigned char *)marks, (const int *)bin_of_slot, counts, pl.slots_cap, S,
-                          (unsigned *)masks);
-        launch_strip_lists(st, (const int4 *)rec, (const float2 *)visf, dv.n, (const int *)slot_of_bin,
-                           (const unsigned *)masks, counts, pl.slots_cap, S, K, (int *)scnt, (int *)soff,
-                           (int *)scur, (int *)sitems, (int *)sctl, (int4 *)sent, entry_cap, ctx->sm_count);
-        end_stage(ctx);
-        begin_stage(ctx, "strip_grid");
-        launch_strip_grid(st, (const int4 *)sent, (const int *)soff, (const int *)sitems, (int *)sctl, taps,
-                          (float2 *)slots, S, K, tw, ctx->sm_count);
-        end_stage(ctx);
     } else {
         begin_stage(ctx, "romein");
         if (dv.n > 0)
@@ -630,14 +578,11 @@ static rg_status wtowers_enqueue(rg_context *ctx, const DevVis &dv, const float2
                           pl.tune.romein_points, ilog2_int(S));
         end_stage(ctx);
     }
-    if (!strip) {
-        begin_stage(ctx, "fft_cols_backward");
-        launch_slot_masks(st, (const unsigned char *)marks, (const int *)bin_of_slot, counts, pl.slots_cap, S,
-                          (unsigned *)masks);
-        launch_sparse_cols(st, (float2 *)slots, (const unsigned *)masks, counts, pl.slots_cap, S, tw,
-                           ctx->sm_count);
-        end_stage(ctx);
-    }
+    begin_stage(ctx, "fft_cols_backward");
+    launch_slot_masks(st, (const unsigned char *)marks, (const int *)bin_of_slot, counts, pl.slots_cap, S,
+                      (unsigned *)masks);
+    launch_sparse_cols(st, (float2 *)slots, (const unsigned *)masks, counts, pl.slots_cap, S, tw, ctx->sm_count);
+    end_stage(ctx);
     begin_stage(ctx, "tower_rows");
     launch_tower_rows(st, (float2 *)slots, (const unsigned *)masks, (const int *)bin_of_slot, (const int *)gbegin,
                       (const int *)gend, range, counts, pl.slots_cap, pl.groups_cap, (const uint32_t *)ph,
@@ -654,10 +599,7 @@ static rg_status wtowers_enqueue(rg_context *ctx, const DevVis &dv, const float2
     launch_add_back(st, (const float2 *)subimg, (const int *)tcount, (double2 *)out_dev, N, S, M, chunk, nchunk,
                     (flags & RG_GRID_OVERWRITE) ? 1 : 0, range, counts, pl.slots_cap, pl.groups_cap, poison);
     end_stage(ctx);
-    // minmax, floors, prepare, compact, (romein, masks, cols | masks, count, scan, fill, strip grid), rows,
-    // finish, cols, add-back
-    ctx->launches += strip ? 13 : 11;
-    ctx->stats[11] = strip ? 1 : 0;
+    ctx->launches += 11;  // minmax, floors, prepare, compact, romein, masks, cols, rows, finish, cols, add-back
     RG_CHECK(check_launch("W-towers pass"));
 
     RG_CUDA(cudaMemcpyAsync(diag_host ? diag_host : ctx->pinned, d.err, 64, cudaMemcpyDeviceToHost, st));
@@ -753,17 +695,8 @@ static rg_status wtowers_autotune(rg_context *ctx, const DevVis &dv, const float
         if (K == 16) { cand[0] = 2; cand[1] = 4; cand[2] = 8; nc = 3; }
         else if (K == 8) { cand[0] = 1; cand[1] = 2; cand[2] = 4; nc = 3; }
         else if (K == 32) { cand[0] = 4; cand[1] = 8; nc = 2; }
-        const bool romein = ctx->wt_gridder != RG_WTOWERS_GRIDDER_STRIP || !strip_grid_supported(S, K);
-        for (int c = 0; c < nc && st == RG_OK && romein; c++) {
+        for (int c = 0; c < nc && st == RG_OK; c++) {
             pl.tune.romein_points = cand[c];
-            pl.tune.strip_gridder = 0;
-            float ms = 0;
-            st = time_pass(&ms);
-            if (st == RG_OK && ms < best_ms) { best_ms = ms; best = pl.tune; }
-        }
-        if (st == RG_OK && ctx->wt_gridder != RG_WTOWERS_GRIDDER_ROMEIN && strip_grid_supported(S, K)) {
-            pl.tune = best;
-            pl.tune.strip_gridder = 1;
             float ms = 0;
             st = time_pass(&ms);
             if (st == RG_OK && ms < best_ms) { best_ms = ms; best = pl.tune; }
@@ -912,7 +845,6 @@ rg_status grid_wtowers_impl(rg_context *ctx, double *uvgrid, int grid_size, doub
         RG_CHECK(wtowers_check(ctx, pl, &overflow));
         ctx->launches += pl.graph_launches;
         ctx->stats[10] = 1;
-        ctx->stats[11] = use_strip_gridder(ctx, pl, lt != nullptr, S, lt ? lt->ksize : wkern->size) ? 1 : 0;
         if (overflow) {
             drop_graph(pl);  // the data outgrew the plan: size it again eagerly
             begin_call(ctx);
@@ -943,14 +875,13 @@ rg_status grid_wtowers_impl(rg_context *ctx, double *uvgrid, int grid_size, doub
         drop_graph(pl);
     }
     if (!done && ctx->autotune && !pl.tuned && !ctx->profiling) {
-        int64_t keep[12];
+        int64_t keep[11];
         std::memcpy(keep, ctx->stats, sizeof(keep));
         const int launches = ctx->launches;
         RG_CHECK(wtowers_autotune(ctx, dv, taps, wkern, lt, N, theta, S, M, wincrement, pl));
         std::memcpy(ctx->stats, keep, sizeof(keep));
         ctx->stats[8] = pl.tune.romein_points;
         ctx->stats[9] = pl.tune.group_items;
-        ctx->stats[11] = use_strip_gridder(ctx, pl, lt != nullptr, S, lt ? lt->ksize : wkern->size) ? 1 : 0;
         ctx->launches = launches;
         drop_graph(pl);
     }

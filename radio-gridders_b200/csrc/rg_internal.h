@@ -71,7 +71,6 @@ rg_status grid_wtowers_impl(rg_context *ctx, double *uvgrid, int grid_size, doub
 // Schedule knobs of a W-towers pass (picked by the autotuner).
 struct TowerTuning {
     int romein_points = 8;  // grid points per Romein thread (threads per CTA = K^2 / points)
-    int strip_gridder = 0;  // 1: strip gridder (gridding fused with the column transform) instead of Romein
     int group_items = 8;    // row-stage work items per SM (sets the floor-group size)
 };
 
@@ -117,8 +116,7 @@ struct rg_context {
     void *pinned = nullptr;  // small pinned host buffer (diagnostics read-back)
     bool autotune = true;    // tune W-towers schedules once per shape
     bool use_graphs = true;  // replay W-towers passes as CUDA graphs
-    int wt_gridder = 0;      // RG_WTOWERS_GRIDDER_*: W-towers gridder (0: the tuner's choice)
-    int64_t stats[12] = {0};
+    int64_t stats[11] = {0};
     int launches = 0;
 };
 
@@ -305,21 +303,6 @@ void launch_slot_masks(cudaStream_t s, const unsigned char *marks, const int *bi
 // Backward column transform, in place, of the marked strips of the live slots.
 void launch_sparse_cols(cudaStream_t s, float2 *slots, const unsigned *masks, const int *counts,
                         int slot_cap, int subgrid, const float2 *tw, int sm_count);
-// Strip gridder, the alternative to Romein + launch_sparse_cols for table taps
-// (subgrid 256 or 512, ksize 8 or 16): launch_strip_lists builds, per live
-// (slot, strip), the list of entries {goff, slice offset, visibility} of the
-// records whose footprints reach the strip (cnt, off, cur: slot_cap * S/8 (+1
-// for off) ints; items: slot_cap * S/8 ints; ctl: 2 ints; entries: at most
-// strip_max_entries_per_record(ksize) per record), and launch_strip_grid grids
-// each marked strip in shared memory and applies the backward column
-// transform, writing every marked strip of the live slots.
-bool strip_grid_supported(int subgrid, int ksize);
-int strip_max_entries_per_record(int ksize);
-void launch_strip_lists(cudaStream_t s, const int4 *rec, const float2 *visf, int64_t n, const int *slot_of_bin,
-                        const unsigned *masks, const int *counts, int slot_cap, int subgrid, int ksize, int *cnt,
-                        int *off, int *cur, int *items, int *ctl, int4 *entries, int64_t entry_cap, int sm_count);
-void launch_strip_grid(cudaStream_t s, const int4 *entries, const int *off, const int *items, int *ctl,
-                       const float2 *taps, float2 *slots, int subgrid, int ksize, const float2 *tw, int sm_count);
 // Row stage: per group and strip of rows, for each floor the backward row
 // transform (reading only marked strips and leaving them zeroed: the reference
 // clears its sub-grid after each floor, grid.c:473-481), times the floor's
