@@ -331,8 +331,8 @@ __global__ void __launch_bounds__(kSparseColThreads) sparse_cols_kernel(
 // wtransfer^(-wp), grid.c:304-319 and :473-496, which also covers the w = 0
 // transfer — accumulated in registers; the strip sum goes to the group's
 // partial buffer.  The phase -wp * ph is formed modulo one turn as an integer
-// product with the 32-bit fixed-point table (fresnel_table_kernel); sin/cos of
-// its top 24 bits in FP32.
+// product with the 32-bit fixed-point table (fresnel_table_kernel), converted
+// to FP32 (24 significant bits) for sin/cos.
 //
 // tower_rows_finish_kernel: CTA = (tower, strip of R rows).  Sums the tower's
 // group partials in group order (deterministic) and applies the forward row
@@ -484,13 +484,12 @@ __global__ void __launch_bounds__(kRowThreads) tower_rows_kernel(
 #pragma unroll
                 for (int j = 0; j < N1; j++) {
                     const int col = k2 + 32 * bitrevc(j, G::LB);
-                    // -wp ph modulo one turn as a signed 32-bit fraction, rounded to
-                    // its top 24 bits (k, |k| <= 2^22), converted exactly by the
-                    // 1.5 * 2^23 magic number
-                    const int k = (int)(mwp * P[r * N + col] + 256u) >> 9;
-                    const float turns = __int_as_float(0x4B400000 + k) - 12582912.f;
+                    // -wp ph modulo one turn as a signed 32-bit fraction of a turn,
+                    // rounded to 24 significant bits by the conversion (at most
+                    // 2^-25 turns off)
+                    const int k = (int)(mwp * P[r * N + col]);
                     float sn, cs;
-                    __sincosf(turns * (6.28318530717958647f / 8388608.f), &sn, &cs);
+                    __sincosf(__int2float_rn(k) * (6.28318530717958647f / 4294967296.f), &sn, &cs);
                     // acc += b * (cs + i sn), two fused multiply-adds per component
                     acc[q][j].x = fmaf(b[j].x, cs, fmaf(-b[j].y, sn, acc[q][j].x));
                     acc[q][j].y = fmaf(b[j].x, sn, fmaf(b[j].y, cs, acc[q][j].y));
