@@ -53,45 +53,54 @@ __device__ __forceinline__ int div_nonneg(int a, int d, float inv)
 // capacity) nothing is written, so the caller can rerun on the same grid.  In
 // a batch (poison != nullptr) an overflow also stops the later passes' writes
 // until the batch reruns them.
+constexpr int kAddBackRows = 4;
+
 __global__ void add_back_kernel(const float2 *__restrict__ subimg, const int *__restrict__ tower_count,
                                 double2 *__restrict__ master, int N, int S, int M, int chunk,
                                 int nchunk, int overwrite, const int *__restrict__ range,
                                 const int *__restrict__ counts, int slot_cap, int group_cap, int *poison)
 {
     const int gx = blockIdx.x * blockDim.x + threadIdx.x;
-    const int gy = blockIdx.y * blockDim.y + threadIdx.y;
-    if (gx >= N || gy >= N) return;
+    if (gx >= N) return;
     if (range && (!range[2] || counts[0] > slot_cap || counts[1] > group_cap)) {
         if (poison) *poison = 1;  // later passes of a batch may see unconsumed sub-grids
         return;
     }
     if (poison && *poison) return;
-    const int ax = gx + M / 2, ay = gy + M / 2;  // x + N/2 + M/2 with x = gx - N/2
+    const int ax = gx + M / 2;  // x + N/2 + M/2 with x = gx - N/2
     const float inv = 1.0f / (float)chunk;
-    int cx_hi = div_nonneg(ax, chunk, inv), cy_hi = div_nonneg(ay, chunk, inv);
-    int cx_lo = (ax - S) >= 0 ? div_nonneg(ax - S, chunk, inv) + 1 : 0;
-    int cy_lo = (ay - S) >= 0 ? div_nonneg(ay - S, chunk, inv) + 1 : 0;
+    int cx_hi = div_nonneg(ax, chunk, inv);
+    const int cx_lo = (ax - S) >= 0 ? div_nonneg(ax - S, chunk, inv) + 1 : 0;
     if (cx_hi >= nchunk) cx_hi = nchunk - 1;
-    if (cy_hi >= nchunk) cy_hi = nchunk - 1;
-    const int64_t at = (int64_t)gy * N + gx;
-    double2 acc = overwrite ? make_double2(0.0, 0.0) : master[at];
     // S is a power of two, so 1 / S^2 is exact and multiplying by it gives
     // the quotient the division would, bit for bit
     const double inv_norm = 1.0 / (double)(S * S);
-    for (int cy = cy_lo; cy <= cy_hi; cy++) {
-        const int sy = ay - chunk * cy;
-        if (sy < 0 || sy >= S) continue;
-        for (int cx = cx_lo; cx <= cx_hi; cx++) {
-            const int sx = ax - chunk * cx;
-            if (sx < 0 || sx >= S) continue;
-            const int t = cy * nchunk + cx;
-            if (tower_count[t] == 0) continue;
-            const float2 z = subimg[(int64_t)t * S * S + (int64_t)sy * S + sx];
-            acc.x += (double)z.x * inv_norm;
-            acc.y += (double)z.y * inv_norm;
+    // kAddBackRows rows per thread, blockDim.y apart (the column's tower range
+    // is found once)
+    const int gy_end = min(N, (int)(blockIdx.y + 1) * (int)blockDim.y * kAddBackRows);
+#pragma unroll 1
+    for (int gy = blockIdx.y * blockDim.y * kAddBackRows + threadIdx.y; gy < gy_end; gy += blockDim.y) {
+        const int ay = gy + M / 2;
+        int cy_hi = div_nonneg(ay, chunk, inv);
+        const int cy_lo = (ay - S) >= 0 ? div_nonneg(ay - S, chunk, inv) + 1 : 0;
+        if (cy_hi >= nchunk) cy_hi = nchunk - 1;
+        const int64_t at = (int64_t)gy * N + gx;
+        double2 acc = overwrite ? make_double2(0.0, 0.0) : master[at];
+        for (int cy = cy_lo; cy <= cy_hi; cy++) {
+            const int sy = ay - chunk * cy;
+            if (sy < 0 || sy >= S) continue;
+            for (int cx = cx_lo; cx <= cx_hi; cx++) {
+                const int sx = ax - chunk * cx;
+                if (sx < 0 || sx >= S) continue;
+                const int t = cy * nchunk + cx;
+                if (tower_count[t] == 0) continue;
+                const float2 z = subimg[(int64_t)t * S * S + (int64_t)sy * S + sx];
+                acc.x += (double)z.x * inv_norm;
+                acc.y += (double)z.y * inv_norm;
+            }
         }
+        master[at] = acc;
     }
-    master[at] = acc;
 }
 
 void launch_add_back(cudaStream_t s, const float2 *subimg, const int *tower_count, double2 *master,
@@ -99,7 +108,7 @@ void launch_add_back(cudaStream_t s, const float2 *subimg, const int *tower_coun
                      const int *range, const int *counts, int slot_cap, int group_cap, int *poison)
 {
     dim3 blk(32, 8);
-    dim3 grd((grid_size + 31) / 32, (grid_size + 7) / 8);
+    dim3 grd((grid_size + 31) / 32, (grid_size + 8 * kAddBackRows - 1) / (8 * kAddBackRows));
     add_back_kernel<<<grd, blk, 0, s>>>(subimg, tower_count, master, grid_size, subgrid, margin,
                                         chunk, nchunk, overwrite, range, counts, slot_cap, group_cap, poison);
 }
