@@ -230,6 +230,15 @@ def cpu_baseline(obs, wk, reps=1):
             "seconds": dt}
 
 
+def workload_config(nvis, stations):
+    """The workload both arms time (identical in their lines)."""
+    return {"workload": "wtowers_plain: 2048x2048 grid (theta 0.1, lambda 20480), subgrid 512, "
+                        f"margin 16, winc 10, {nvis:,} vis ({stations} stations, 16 dumps x 4 ch), "
+                        "16x16 taps x32 oversampled, 11 w-planes",
+            "grid_size": GRID, "theta": THETA, "subgrid": SUBGRID, "margin": MARGIN, "winc": WINC,
+            "vis_per_step": nvis}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
@@ -254,8 +263,9 @@ def run_reference(args, rank, world):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": {"workload": "wtowers_plain", "grid_size": GRID, "theta": THETA,
-                       "subgrid": SUBGRID, "margin": MARGIN, "winc": WINC},
+            "config": workload_config(len(obs.flat()[0]), 256),
+            "run": {"parallelism": f"{cores} host threads (OpenMP over towers)" if kind == "reference"
+                    else "1 host thread"},
             "cpu_baseline": {"value": value, "unit": "vis/s", "cores": res["cores"] if kind == "reference" else 1,
                              "kind": kind, "sample": res["sample"]},
             "e2e": {"value": value, "unit": "vis/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -518,20 +528,17 @@ def run_b200(args, rank, world, local_rank):
         "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded Earth-rotation synthesis, power-law point sources)",
-        "config": {"workload": "wtowers_plain: 2048x2048 grid (theta 0.1, lambda 20480), subgrid 512, "
-                               f"margin 16, winc 10, {nvis:,} vis ({args.stations} stations, 16 dumps x 4 ch), "
-                               "16x16 taps x32 oversampled, 11 w-planes",
-                   "grid_size": GRID, "subgrid": SUBGRID, "margin": MARGIN, "winc": WINC,
-                   "vis_per_gpu": nvis, "active_subgrids": stats["active_subgrids"],
-                   "towers_with_data": stats["towers_with_data"], "floors": stats["floors"],
-                   "parallelism": (f"{world} ranks, the observation's towers split by load, FP64 master grids "
-                                   "reduced over NCCL") if world > 1 else "1 GPU",
-                   "l2": "256 MiB buffer written between steps, outside each step's event pair",
-                   "precision": "FP32 sub-grids and transforms; FP64 coordinates, Fresnel phase and master grid",
-                   "schedule": {"romein_points_per_thread": stats["romein_points"],
-                                "row_stage_items_per_sm": stats["group_items_per_sm"],
-                                "graph_replay": bool(stats["graph"]), "autotuned": not args.no_autotune},
-                   "marked_strips": stats["marked_strips"], "floor_groups": stats["floor_groups"]},
+        "config": workload_config(nvis, args.stations),
+        "run": {"parallelism": (f"{world} ranks, the observation's towers split by load, FP64 master grids "
+                                "reduced over NCCL") if world > 1 else "1 GPU",
+                "vis_per_gpu": nvis, "active_subgrids": stats["active_subgrids"],
+                "towers_with_data": stats["towers_with_data"], "floors": stats["floors"],
+                "l2": "256 MiB buffer written between steps, outside each step's event pair",
+                "precision": "FP32 sub-grids and transforms; FP64 coordinates, Fresnel phase and master grid",
+                "schedule": {"romein_points_per_thread": stats["romein_points"],
+                             "row_stage_items_per_sm": stats["group_items_per_sm"],
+                             "graph_replay": bool(stats["graph"]), "autotuned": not args.no_autotune},
+                "marked_strips": stats["marked_strips"], "floor_groups": stats["floor_groups"]},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": dom_bytes, "launch_ms": dom_ms,
