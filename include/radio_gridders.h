@@ -153,10 +153,9 @@ rg_status rg_grid_simple(rg_context *ctx, double *uvgrid, int grid_size, double 
  * every GPU that loads the library until exit), which limits grid_size to
  * 1024 and the w-kernel table to 524288 taps; larger requests fail with
  * RG_ERR_UNSUPPORTED.  Any number of visibilities.  The first call on each
- * device resolves the array's address (cudaGetSymbolAddress); make that first
- * call before any stream capture.  Calls share the array: calls that overlap
- * on the GPU (other streams, other host threads) race.  Runs on the calling
- * thread's current device.  The call synchronises with `cuda_stream` twice:
+ * device resolves the array's address (cudaGetSymbolAddress).  Calls share
+ * the array: calls that overlap on the GPU (other streams, other host
+ * threads) race.  Runs on the calling thread's current device.  The call synchronises with `cuda_stream` twice:
  * it reads the error word back before it touches uvgrid (a call rejected for
  * its data, e.g. w outside the table, leaves uvgrid as it was), and it returns
  * after the grid is written.  A CUDA error already pending when the call
