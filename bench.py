@@ -79,22 +79,6 @@ def workload(stations: int = 256):
     return obs, wk
 
 
-def tower_parts(vis_per_tower, floors_per_tower, world):
-    """Part (rank) of each tower: the library's deterministic balance of
-    visibilities and active w-floors, the same on every rank."""
-    rg = importlib.import_module("radio-gridders_b200")
-    return rg.partition_towers(vis_per_tower, floors_per_tower, world)
-
-
-def reduce_master(grid, world):
-    """Sum the ranks' FP64 master grids onto rank 0 (one collective).  The grid
-    is a complex128 torch tensor; it travels as its real view."""
-    if world > 1:
-        import torch
-        import torch.distributed as dist
-        dist.reduce(torch.view_as_real(grid), dst=0)
-
-
 def peaks():
     path = os.path.join(REPO, "MEASURED_PEAKS.json")
     try:
@@ -324,6 +308,7 @@ def run_b200(args, rank, world, local_rank):
     import torch.distributed as dist
 
     rg = importlib.import_module("radio-gridders_b200")
+    sharding = importlib.import_module("radio-gridders_b200.sharding")
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     obs, wk = workload(args.stations)
@@ -349,7 +334,7 @@ def run_b200(args, rank, world, local_rank):
     parts = None
     if world > 1:  # this rank's towers (planning, outside the timed steps)
         nv, nf = ctx.tower_loads(GRID, THETA, V, SUBGRID, MARGIN, WINC)
-        parts = tower_parts(nv, nf, world)
+        parts = sharding.tower_parts(nv, nf, world)
 
     def step():
         if parts is None:
@@ -358,7 +343,7 @@ def run_b200(args, rank, world, local_rank):
         else:
             ctx.grid_wtowers_part(grid, GRID, THETA, V, wk, SUBGRID, MARGIN, WINC, parts, rank,
                                   flags=rg.RG_GRID_OVERWRITE, wkern_data=dwk)
-        reduce_master(grid, world)
+        sharding.reduce_grid(grid, world)
 
     for _ in range(max(args.warmup, 3)):
         step()

@@ -253,6 +253,14 @@ rg_status rg_fft2d(rg_context *ctx, void *data, int batch, int ny, int nx, int s
  * factor 2 matches the hermitian gridder pipeline, 1 the reference dft.out. */
 rg_status rg_dft_image(rg_context *ctx, double *image_out, int grid_size, double theta,
                        const rg_vis *vis, int precision, double factor);
+/* Rows [row0, row0 + nrows) of the same image into image_out (nrows rows of
+ * grid_size), e.g. one GPU's share of an image whose rows are split over
+ * several GPUs (the shares are then gathered; no counterpart in the
+ * reference, whose DFT runs on one GPU).  A share starting on a row that is a
+ * multiple of 32 equals those rows of rg_dft_image bit for bit; other starts
+ * differ within the precision mode's rounding. */
+rg_status rg_dft_image_rows(rg_context *ctx, double *image_out, int grid_size, double theta,
+                            const rg_vis *vis, int precision, double factor, int row0, int nrows);
 
 /* ---- file-level drop-ins for the reference's host wrappers --------------- */
 

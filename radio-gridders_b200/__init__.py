@@ -39,7 +39,7 @@ EXPORTS = [
     "rg_context_create", "rg_context_destroy", "rg_context_set_stream", "rg_last_error",
     "rg_last_stats", "rg_context_set_profiling", "rg_context_set_autotune", "rg_context_set_graphs",
     "rg_last_timings", "rg_grid_wprojection", "rg_grid_wtowers", "rg_weight",
-    "rg_make_hermitian", "rg_fft_shift", "rg_image_from_grid", "rg_fft2d", "rg_dft_image",
+    "rg_make_hermitian", "rg_fft_shift", "rg_image_from_grid", "rg_fft2d", "rg_dft_image", "rg_dft_image_rows",
     "rg_grid_wprojection_noalloc", "rg_mlp_param_count", "rg_mlp_create", "rg_mlp_destroy",
     "rg_mlp_set_params", "rg_mlp_get_params", "rg_mlp_gradient", "rg_mlp_train", "rg_mlp_eval",
     "rg_grid_wprojection_learned", "rg_grid_wtowers_learned", "rg_grid_wtowers_batch", "rg_read_vis_hdf5", "rg_free_vis_data", "rg_read_wkern_hdf5",
@@ -194,6 +194,7 @@ def lib():
         L.rg_image_from_grid.argtypes = [vp, vp, i, vp, vp]
         L.rg_fft2d.argtypes = [vp, vp, i, i, i, i, i]
         L.rg_dft_image.argtypes = [vp, vp, i, d, ct.POINTER(_Vis), i, d]
+        L.rg_dft_image_rows.argtypes = [vp, vp, i, d, ct.POINTER(_Vis), i, d, i, i]
         L.rg_grid_wprojection_noalloc.argtypes = [vp, i, d, ct.POINTER(_Vis), ct.POINTER(_WKern), i, vp]
         L.rg_mlp_param_count.restype = i
         L.rg_mlp_create.argtypes = [vp, i, d, d, ct.c_uint64, ct.POINTER(vp)]
@@ -471,6 +472,16 @@ class Context:
         vs = vis.struct()
         _check(lib().rg_dft_image(self._h, _ptr(image), int(grid_size), float(theta),
                                   ct.byref(vs), int(precision), float(factor)))
+        return image
+
+    def dft_image_rows(self, grid_size, theta, vis: Visibilities, row0, nrows,
+                       precision=RG_DFT_FP64_REDUCED, factor=2.0, image=None):
+        """Rows [row0, row0 + nrows) of dft_image (one rank's share)."""
+        if image is None:
+            image = np.empty((nrows, grid_size), np.float64)
+        vs = vis.struct()
+        _check(lib().rg_dft_image_rows(self._h, _ptr(image), int(grid_size), float(theta),
+                                       ct.byref(vs), int(precision), float(factor), int(row0), int(nrows)))
         return image
 
 

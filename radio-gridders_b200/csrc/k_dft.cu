@@ -8,6 +8,9 @@
 // wavelengths (its defects, src/dft/dft_cuda.cu:55-57 and :98-112, removed).
 //
 // A CTA owns a 32 x 32 pixel tile; each thread four pixels of one column.
+// Rows [row0, row0 + nrows) only (a rank's share of a row-partitioned image):
+// tiles start at row0, so a share that starts on a multiple of 32 computes its
+// rows exactly as the whole image does.
 // Visibilities are staged through shared memory 256 at a time.  Precision
 // modes (the precision study):
 //   FP64_REDUCED: per (tile, visibility) the phase at the tile centre phi0 is
@@ -30,12 +33,12 @@ __global__ void __launch_bounds__(256) dft_kernel(const double *__restrict__ u,
                                                   const double *__restrict__ w,
                                                   const double2 *__restrict__ vis, int64_t nvis,
                                                   double *__restrict__ image, int N, double theta,
-                                                  double factor)
+                                                  double factor, int row0, int nrows)
 {
     __shared__ float su[DFT_BATCH], sv[DFT_BATCH], sw[DFT_BATCH], sr[DFT_BATCH], si[DFT_BATCH];
     __shared__ double du[DFT_BATCH], dv[DFT_BATCH], dw[DFT_BATCH], dr[DFT_BATCH], di[DFT_BATCH];
     const int tx = threadIdx.x % TILE, ty = threadIdx.x / TILE;  // ty in [0, 8)
-    const int x0 = blockIdx.x * TILE, y0 = blockIdx.y * TILE;
+    const int x0 = blockIdx.x * TILE, y0 = row0 + blockIdx.y * TILE;
     const int cx = x0 + TILE / 2, cy = y0 + TILE / 2;
     const double l0 = theta * (double)(cx - N / 2) / N;
     const double m0 = theta * (double)(cy - N / 2) / N;
@@ -139,25 +142,33 @@ __global__ void __launch_bounds__(256) dft_kernel(const double *__restrict__ u,
 #pragma unroll
     for (int p = 0; p < PIX; p++) {
         const int y = y0 + ty + 8 * p;
-        if (x < N && y < N) image[(int64_t)y * N + x] = factor * acc[p];
+        if (x < N && y < row0 + nrows) image[(int64_t)(y - row0) * N + x] = factor * acc[p];
     }
 }
 
 void launch_dft(cudaStream_t s, const double *u, const double *v, const double *w,
                 const double2 *vis, int64_t n, double *image, int grid_size, double theta,
-                int precision, double factor, int sm_count)
+                int precision, double factor, int sm_count, int row0, int nrows)
 {
     (void)sm_count;
-    dim3 grd((grid_size + TILE - 1) / TILE, (grid_size + TILE - 1) / TILE);
+    if (nrows < 0) {
+        row0 = 0;
+        nrows = grid_size;
+    }
+    if (nrows == 0) return;
+    dim3 grd((grid_size + TILE - 1) / TILE, (nrows + TILE - 1) / TILE);
     switch (precision) {
         case RG_DFT_FP32_NAIVE:
-            dft_kernel<RG_DFT_FP32_NAIVE><<<grd, 256, 0, s>>>(u, v, w, vis, n, image, grid_size, theta, factor);
+            dft_kernel<RG_DFT_FP32_NAIVE><<<grd, 256, 0, s>>>(u, v, w, vis, n, image, grid_size, theta, factor, row0,
+                                                                 nrows);
             break;
         case RG_DFT_FP64:
-            dft_kernel<RG_DFT_FP64><<<grd, 256, 0, s>>>(u, v, w, vis, n, image, grid_size, theta, factor);
+            dft_kernel<RG_DFT_FP64><<<grd, 256, 0, s>>>(u, v, w, vis, n, image, grid_size, theta, factor, row0,
+                                                                 nrows);
             break;
         default:
-            dft_kernel<RG_DFT_FP64_REDUCED><<<grd, 256, 0, s>>>(u, v, w, vis, n, image, grid_size, theta, factor);
+            dft_kernel<RG_DFT_FP64_REDUCED><<<grd, 256, 0, s>>>(u, v, w, vis, n, image, grid_size, theta, factor, row0,
+                                                                 nrows);
             break;
     }
 }

@@ -1359,17 +1359,26 @@ rg_status rg_fft2d(rg_context *ctx, void *data, int batch, int ny, int nx, int s
 rg_status rg_dft_image(rg_context *ctx, double *image_out, int grid_size, double theta,
                        const rg_vis *vis, int precision, double factor)
 {
+    return rg_dft_image_rows(ctx, image_out, grid_size, theta, vis, precision, factor, 0, grid_size);
+}
+
+rg_status rg_dft_image_rows(rg_context *ctx, double *image_out, int grid_size, double theta,
+                            const rg_vis *vis, int precision, double factor, int row0, int nrows)
+{
     if (!ctx || !image_out) return fail(RG_ERR_INVALID_ARGUMENT, "NULL argument");
     if (grid_size < 1 || grid_size > 65536) return fail(RG_ERR_INVALID_ARGUMENT, "bad grid_size");
     if (precision < 0 || precision > 2) return fail(RG_ERR_INVALID_ARGUMENT, "unknown precision mode");
+    if (row0 < 0 || nrows < 0 || row0 > grid_size || nrows > grid_size - row0)
+        return fail(RG_ERR_INVALID_ARGUMENT, "rows [row0, row0 + nrows) must lie in [0, grid_size)");
     RG_CHECK(check_vis(vis));
     RG_CUDA(cudaSetDevice(ctx->device));
+    if (nrows == 0) return RG_OK;
     DevVis dv;
     RG_CHECK(stage_vis(ctx, vis, &dv));
     OutView ov;
-    RG_CHECK(out_view(ctx, image_out, sizeof(double) * (size_t)grid_size * grid_size, "dft_out", false, &ov));
+    RG_CHECK(out_view(ctx, image_out, sizeof(double) * (size_t)nrows * grid_size, "dft_out", false, &ov));
     launch_dft(ctx->stream, dv.u, dv.v, dv.w, dv.vis, dv.n, (double *)ov.dev, grid_size, theta, precision,
-               factor, ctx->sm_count);
+               factor, ctx->sm_count, row0, nrows);
     RG_CHECK(check_launch("dft"));
     RG_CHECK(finish_out(ctx, ov));
     RG_CUDA(cudaStreamSynchronize(ctx->stream));

@@ -324,9 +324,11 @@ void launch_add_back(cudaStream_t s, const float2 *subimg, const int *tower_coun
                      int group_cap, int *poison = nullptr);
 
 // k_dft.cu
+// rows [row0, row0 + nrows) of the image into image (nrows x grid_size);
+// nrows < 0: the whole image
 void launch_dft(cudaStream_t s, const double *u, const double *v, const double *w,
                 const double2 *vis, int64_t n, double *image, int grid_size, double theta,
-                int precision, double factor, int sm_count);
+                int precision, double factor, int sm_count, int row0 = 0, int nrows = -1);
 
 // k_mlp.cu — learned w-kernel
 int mlp_param_count();

@@ -1,5 +1,7 @@
 """The project's FFT kernels against numpy and cuFFT, and the DFT imager's
 precision modes against the FP64 DFT oracle."""
+import importlib
+
 import numpy as np
 import pytest
 
@@ -99,3 +101,22 @@ def test_dft_single_visibility_fringe(rg, ctx):
     ph = u[0] * lm[None, :] + v[0] * lm[:, None] + w[0] * one_minus_n
     ref = 2 * (vis[0].real * np.cos(2 * np.pi * ph) + vis[0].imag * np.sin(2 * np.pi * ph))
     assert np.max(np.abs(img - ref)) < 1e-12
+
+
+def test_dft_row_bands_make_the_image(rg, ctx, sim):
+    """rg_dft_image_rows: bands starting on multiples of 32 (the partition of
+    sharding.dft_row_ranges) give the whole image's rows bit for bit; a band
+    starting elsewhere agrees to the mode's rounding; bad ranges are rejected."""
+    sharding = importlib.import_module("radio-gridders_b200.sharding")
+    obs = sim.wproj_plain(seed=5, n_dump=8)
+    u, v, w, vis = obs.flat()
+    n, th = 200, obs.meta["theta"]
+    V = rg.Visibilities(u, v, w, vis)
+    whole = ctx.dft_image(n, th, V)
+    bands = [ctx.dft_image_rows(n, th, V, r0, k) for r0, k in sharding.dft_row_ranges(n, 3)]
+    assert np.array_equal(np.concatenate(bands), whole)
+    odd = ctx.dft_image_rows(n, th, V, 17, 50)
+    assert np.max(np.abs(odd - whole[17:67])) < 1e-6 * np.abs(whole).max()
+    for r0, k in ((-1, 4), (190, 20), (0, -2)):
+        with pytest.raises(rg.RGError):
+            ctx.dft_image_rows(n, th, V, r0, k, image=np.empty((max(k, 1), n)))

@@ -1,13 +1,17 @@
-"""The multi-GPU path of bench.py, run as world_size-2 gloo ranks on CPU.
+"""The multi-GPU partitions (radio-gridders_b200/sharding.py, used by
+bench.py), run as world_size-2 gloo ranks on CPU.
 
-One observation's towers are split over the ranks by the library's own
-partition (rg_wtowers_partition, a host function: balanced by visibilities
-and active w-floors), each rank grids its share (the oracle's W-towers
-restricted to those towers stands in for rg_grid_wtowers_part, which needs a
-B200) and bench.reduce_master sums the FP64 master grids onto rank 0.  The
-towers are independent until the add-back, so the sum must equal gridding
-the whole observation on one rank to FP64 rounding; a rank that raises is
-reported as a failure, not a hang (short process-group timeout)."""
+W-towers: one observation's towers are split over the ranks by the library's
+own partition (rg_wtowers_partition, a host function: balanced by
+visibilities and active w-floors), each rank grids its share (the oracle's
+W-towers restricted to those towers stands in for rg_grid_wtowers_part,
+which needs a B200) and sharding.reduce_grid sums the FP64 master grids onto
+rank 0.  The towers are independent until the add-back, so the sum must
+equal gridding the whole observation on one rank to FP64 rounding.
+W-projection: contiguous visibility shares, gridded and reduced the same way.
+DFT: bands of image rows (the oracle's pixels stand in for
+rg_dft_image_rows), gathered on every rank.  A rank that raises is reported
+as a failure, not a hang (short process-group timeout)."""
 import datetime
 import importlib
 import os
@@ -43,8 +47,8 @@ def _worker(rank, world, port, out_path, fail_rank):
     import torch
     import torch.distributed as dist
 
-    import bench
     import oracle
+    sharding = importlib.import_module("radio-gridders_b200.sharding")
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world,
                             timeout=datetime.timedelta(seconds=30))
@@ -55,13 +59,27 @@ def _worker(rank, world, port, out_path, fail_rank):
             raise RuntimeError("injected failure on rank %d" % rank)
         n, th = meta["grid_size"], meta["theta"]
         nv, nf = oracle.wtowers_census(n, th, u, v, w, S, M, WINC)
-        parts = bench.tower_parts(nv, nf, world)
+        parts = sharding.tower_parts(nv, nf, world)
         g = oracle.grid_wtowers(n, th, u, v, w, vis, wk, S, M, WINC, towers=(parts == rank))
         t = torch.from_numpy(g)
-        bench.reduce_master(t, world)
+        sharding.reduce_grid(t, world)
+        # W-projection over contiguous visibility shares
+        b, e = sharding.vis_share(len(u), world, rank)
+        wkp = sim.wkernel_for(w, th, 10.0, size=8, oversampling=4)  # planes over the whole w range
+        gp = torch.from_numpy(oracle.grid_wprojection(n, th, u[b:e], v[b:e], w[b:e], vis[b:e], wkp))
+        sharding.reduce_grid(gp, world)
+        # DFT over bands of image rows, on a smaller image
+        nd = 96
+        ranges = sharding.dft_row_ranges(nd, world)
+        row0, nrows = ranges[rank]
+        py, px = np.divmod(np.arange(row0 * nd, (row0 + nrows) * nd), nd)
+        band = oracle.dft_pixels(nd, th, u, v, w, vis, px, py).reshape(nrows, nd)
+        img = sharding.gather_rows(torch.from_numpy(band), nd, ranges, world)
         if rank == 0:
             np.save(out_path, t.numpy())
             np.save(out_path + ".parts.npy", parts)
+            np.save(out_path + ".wproj.npy", gp.numpy())
+            np.save(out_path + ".dft.npy", img.numpy())
     finally:
         dist.destroy_process_group()
 
@@ -98,6 +116,29 @@ def test_two_ranks_tower_shares_sum_to_the_whole(sim, oracle, tmp_path):
     cost = nv + 2400.0 * nf
     loads = [cost[parts == r].sum() for r in range(2)]
     assert min(loads) > 0 and max(loads) <= 1.25 * np.mean(loads) + cost.max()
+    # W-projection shares sum to the whole, the DFT bands make the whole image
+    gp = np.load(out + ".wproj.npy")
+    refp = oracle.grid_wprojection(n, th, u, v, w, vis, sim.wkernel_for(w, th, 10.0, size=8, oversampling=4))
+    assert np.linalg.norm(gp - refp) / np.linalg.norm(refp) < 1e-12
+    img = np.load(out + ".dft.npy")
+    assert np.max(np.abs(img - oracle.dft_image(96, th, u, v, w, vis))) < 1e-9 * np.abs(img).max()
+
+
+def test_share_arithmetic():
+    """Visibility shares tile [0, n) with sizes one apart; row bands tile the
+    image, start on multiples of 32 and are as even as that allows."""
+    sharding = importlib.import_module("radio-gridders_b200.sharding")
+    for n, world in ((10, 3), (7, 8), (2_088_960, 8), (0, 2)):
+        spans = [sharding.vis_share(n, world, r) for r in range(world)]
+        assert spans[0][0] == 0 and spans[-1][1] == n
+        assert all(spans[r][1] == spans[r + 1][0] for r in range(world - 1))
+        sizes = [e - b for b, e in spans]
+        assert max(sizes) - min(sizes) <= 1
+    for n, world in ((2048, 8), (1000, 3), (96, 2), (50, 4)):
+        ranges = sharding.dft_row_ranges(n, world)
+        assert ranges[0][0] == 0 and sum(k for _, k in ranges) == n
+        assert all(ranges[r][0] + ranges[r][1] == ranges[r + 1][0] for r in range(world - 1))
+        assert all(r0 % 32 == 0 or k == 0 for r0, k in ranges)
 
 
 def test_partition_is_deterministic_and_balanced(rg):
