@@ -129,7 +129,9 @@ __global__ void __launch_bounds__(256) dft_kernel(const double *__restrict__ u,
 #pragma unroll
                 for (int p = 0; p < PIX; p++) {
                     float d = fmaf(uj, fl[p], fmaf(vj, fm[p], wj * fn[p]));
-                    d -= rintf(d);
+                    // nearest integer by the 1.5 * 2^23 shift (|d| < 2^22 turns):
+                    // two adds on the FMA pipe instead of a rounding instruction
+                    d -= (d + 12582912.f) - 12582912.f;
                     float s, c;
                     __sincosf(6.283185307179586f * d, &s, &c);
                     part[p] = fmaf(rj, c, fmaf(ij, s, part[p]));
