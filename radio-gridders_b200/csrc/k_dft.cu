@@ -35,7 +35,10 @@ __global__ void __launch_bounds__(256) dft_kernel(const double *__restrict__ u,
                                                   double *__restrict__ image, int N, double theta,
                                                   double factor, int row0, int nrows)
 {
-    __shared__ float su[DFT_BATCH], sv[DFT_BATCH], sw[DFT_BATCH], sr[DFT_BATCH], si[DFT_BATCH];
+    // FP32 modes: (u, v, w, Re V) as one 16-byte entry and Im V beside it, so a
+    // visibility is two shared-memory loads in the inner loop
+    __shared__ float4 s4[DFT_BATCH];
+    __shared__ float si[DFT_BATCH];
     __shared__ double du[DFT_BATCH], dv[DFT_BATCH], dw[DFT_BATCH], dr[DFT_BATCH], di[DFT_BATCH];
     const int tx = threadIdx.x % TILE, ty = threadIdx.x / TILE;  // ty in [0, 8)
     const int x0 = blockIdx.x * TILE, y0 = row0 + blockIdx.y * TILE;
@@ -74,16 +77,10 @@ __global__ void __launch_bounds__(256) dft_kernel(const double *__restrict__ u,
                 double s, c;
                 sincospi(2.0 * ph, &s, &c);
                 // V' = V exp(-2 pi i phi0)
-                sr[threadIdx.x] = (float)(z.x * c + z.y * s);
+                s4[threadIdx.x] = make_float4((float)uu, (float)vv, (float)ww, (float)(z.x * c + z.y * s));
                 si[threadIdx.x] = (float)(z.y * c - z.x * s);
-                su[threadIdx.x] = (float)uu;
-                sv[threadIdx.x] = (float)vv;
-                sw[threadIdx.x] = (float)ww;
             } else if (MODE == RG_DFT_FP32_NAIVE) {
-                su[threadIdx.x] = (float)uu;
-                sv[threadIdx.x] = (float)vv;
-                sw[threadIdx.x] = (float)ww;
-                sr[threadIdx.x] = (float)z.x;
+                s4[threadIdx.x] = make_float4((float)uu, (float)vv, (float)ww, (float)z.x);
                 si[threadIdx.x] = (float)z.y;
             } else {
                 du[threadIdx.x] = uu;
@@ -125,7 +122,8 @@ __global__ void __launch_bounds__(256) dft_kernel(const double *__restrict__ u,
             }
 #pragma unroll 4
             for (int j = 0; j < cnt; j++) {
-                const float uj = su[j], vj = sv[j], wj = sw[j], rj = sr[j], ij = si[j];
+                const float4 e = s4[j];
+                const float uj = e.x, vj = e.y, wj = e.z, rj = e.w, ij = si[j];
 #pragma unroll
                 for (int p = 0; p < PIX; p++) {
                     float d = fmaf(uj, fl[p], fmaf(vj, fm[p], wj * fn[p]));
