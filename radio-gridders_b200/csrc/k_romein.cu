@@ -98,7 +98,9 @@ __global__ void __launch_bounds__(K *K / P, (RomeinBounds<K, P>::min_ctas)) rome
                     for (int p = 0; p < P; p++) t[p] = __ldg(taps + r.z + ((cv0 + p * RS) & (K - 1)) * K + cu);
                 }
                 const float2 vz = svis[j];
-                if (r.x == cur_bin && r.y == cur_goff && r.w == cur_res) {
+                // in a sub-grid goff alone fixes the origin (its columns span
+                // chunk + 1 < S values), hence the residues
+                if (r.x == cur_bin && r.y == cur_goff && (STRIP || r.w == cur_res)) {
                     // same sub-grid and footprint origin: every point unchanged
 #pragma unroll
                     for (int p = 0; p < P; p++) {
