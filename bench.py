@@ -901,10 +901,61 @@ def winc_sweep(ctx, wincs=(10.0, 20.0, 40.0, 80.0), steps=120000):
 
 
 STUDIES = ("dft", "towers", "towers_ov", "learned", "learned_small", "baselines", "learned_towers",
-           "learned_towers_c4", "winc_sweep")
+           "learned_towers_c4", "winc_sweep", "pcie")
+
+
+def host_link(reps=10):
+    """The host link's bound on the end-to-end figure: pinned copies of one
+    benchmark step's bytes (its inputs in, 40 B per visibility, and its FP64
+    master grid out) host to device, device to host, and both at once on two
+    streams, timed with CUDA events."""
+    import torch
+    dev = torch.device("cuda", 0)
+    n_in, n_out = (40 * 2_088_960) // 8, (16 * GRID * GRID) // 8
+    hin = torch.empty(n_in, dtype=torch.float64).pin_memory()
+    hout = torch.empty(n_out, dtype=torch.float64).pin_memory()
+    din = torch.empty(n_in, dtype=torch.float64, device=dev)
+    dout = torch.empty(n_out, dtype=torch.float64, device=dev)
+    s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+
+    def h2d():
+        din.copy_(hin, non_blocking=True)
+
+    def d2h():
+        hout.copy_(dout, non_blocking=True)
+
+    def both():
+        cur = torch.cuda.current_stream(dev)
+        s_in.wait_stream(cur)
+        s_out.wait_stream(cur)
+        with torch.cuda.stream(s_in):
+            din.copy_(hin, non_blocking=True)
+        with torch.cuda.stream(s_out):
+            hout.copy_(dout, non_blocking=True)
+        cur.wait_stream(s_in)
+        cur.wait_stream(s_out)
+
+    out = {"in_bytes": n_in * 8, "out_bytes": n_out * 8}
+    for name, fn in (("h2d", h2d), ("d2h", d2h), ("both", both)):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        b.synchronize()
+        out[name + "_ms"] = a.elapsed_time(b) / reps
+    out["h2d_gbs"] = out["in_bytes"] / out["h2d_ms"] / 1e6
+    out["d2h_gbs"] = out["out_bytes"] / out["d2h_ms"] / 1e6
+    out["e2e_bound_vis_per_s"] = 2_088_960 / (out["both_ms"] * 1e-3)
+    return out
 
 
 def run_study(which):
+    if which == "pcie":
+        print(json.dumps({"study": "host_link", **host_link()}), flush=True)
+        return 0
     ctx = _RG().Context(0)
     if which == "dft":
         print(json.dumps({"study": "dft_precision", **dft_precision(ctx)}), flush=True)
