@@ -282,3 +282,51 @@ def test_point_source_at_phase_centre_image_on_gpu(rg, ctx, sim):
     img = ctx.image_from_grid(g)
     assert np.unravel_index(np.argmax(img), img.shape) == (n // 2, n // 2)
     assert img[n // 2, n // 2] > 0
+
+
+@pytest.mark.parametrize("ksize,ov,sub,margin", [(8, 8, 256, 16), (32, 4, 256, 32)])
+def test_wtowers_kernel_sizes_vs_oracle(rg, ctx, sim, oracle, wproj_data, ksize, ov, sub, margin):
+    """W-towers with 8- and 32-tap kernels (the gridder's other footprint
+    sizes) against the oracle, visibility counts included."""
+    obs, u, v, w, vis = wproj_data
+    n, th = obs.meta["grid_size"], obs.meta["theta"]
+    wkt = sim.generate_wkernel(th, np.arange(-6.0, 7.0, 1.0), ksize, ov)
+    g = np.zeros((n, n), np.complex128)
+    ctx.grid_wtowers(g, n, th, V(rg, u, v, w, vis), wkt, sub, margin, 10.0)
+    ref, counts = oracle.grid_wtowers(n, th, u, v, w, vis, wkt, sub, margin, 10.0, return_counts=True)
+    assert rel_rms(g, ref) < TOL
+    st = ctx.last_stats()
+    assert st["gridded"] == int(counts.sum()) and st["gridded"] + st["dropped"] == len(u)
+
+
+def test_wtowers_cuts_on_the_boundaries(rg, ctx, sim, oracle):
+    """Visibilities exactly on the half-open tower cuts in u and v and on the
+    w-floor cuts, and one ulp either side, formed in FP64 as the reference
+    forms them (grid.c:425-458 for the towers, :244-254 for the floors): the
+    device bins every one as the oracle does."""
+    n, th, S, M, winc = 512, 0.1, 128, 16, 10.0
+    chunk = S - M
+    nchunk = n // chunk + 1
+    cuts = np.array([(chunk * c - n // 2 - 0.5) / th for c in range(nchunk)])
+    fcuts = np.array([(wp - 0.5) * winc for wp in range(-4, 5)])
+    rng = np.random.default_rng(11)
+    m = 4000
+
+    def near(x):  # on the value, or one ulp below or above
+        step = rng.integers(-1, 2, len(x))
+        return np.where(step < 0, np.nextafter(x, -np.inf), np.where(step > 0, np.nextafter(x, np.inf), x))
+
+    u = near(cuts[rng.integers(1, nchunk, m)])
+    v = near(cuts[rng.integers(1, nchunk, m)])
+    w = near(fcuts[rng.integers(0, len(fcuts), m)])
+    # half of them off the cuts in one axis only
+    free = rng.random(m) < 0.5
+    u[free] = rng.uniform(-200, 200, free.sum()) / th
+    vis = rng.normal(size=m) + 1j * rng.normal(size=m)
+    wkt = sim.generate_wkernel(th, np.arange(-6.0, 7.0, 1.0))
+    g = np.zeros((n, n), np.complex128)
+    ctx.grid_wtowers(g, n, th, V(rg, u, v, w, vis), wkt, S, M, winc)
+    ref, counts = oracle.grid_wtowers(n, th, u, v, w, vis, wkt, S, M, winc, return_counts=True)
+    assert rel_rms(g, ref) < TOL
+    st = ctx.last_stats()
+    assert st["gridded"] == int(counts.sum()) and st["gridded"] + st["dropped"] == m
