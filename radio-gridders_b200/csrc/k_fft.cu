@@ -486,7 +486,7 @@ __global__ void __launch_bounds__(kRowThreads) tower_rows_kernel(
                     const int col = k2 + 32 * bitrevc(j, G::LB);
                     // -wp ph modulo one turn as a signed 32-bit fraction of a turn,
                     // rounded to 24 significant bits by the conversion (at most
-                    // 2^-25 turns off)
+                    // 64 units of 2^-32, 2^-26 turns, off)
                     const int k = (int)(mwp * P[r * N + col]);
                     float sn, cs;
                     __sincosf(__int2float_rn(k) * (6.28318530717958647f / 4294967296.f), &sn, &cs);
