@@ -508,6 +508,29 @@ def run_b200(args, rank, world, local_rank):
                             "frac": flops / (rows_ms * 1e-3) / 1e12 / fp32_peak,
                             "peak_source": "nominal FP32 (148 SMs x 128 lanes x 2 x 1.965 GHz); "
                                            "no measured FP32 peak on this pool"}
+    # The heavy kernels are bound by instruction issue: their warp instructions
+    # per launch (one-kernel ncu captures of the 128-station case, scaled to
+    # this workload by each kernel's work unit; not measured in this run) over
+    # the launch time, against 4 issues per SM per clock at the clock sampled
+    # during the timed steps.
+    issue_roofline = None
+    ipath = os.path.join(REPO, "profiles", "wtowers_instructions.json")
+    if os.path.exists(ipath) and args.stations == 256:
+        with open(ipath) as f:
+            idoc = json.load(f)
+        sm_hz = ((clk or {}).get("sm_mhz") or 1965.0) * 1e6
+        issue_peak = 148 * 4 * sm_hz / 1e12
+        issue_roofline = {"unit": "T warp instructions/s", "peak": issue_peak,
+                          "peak_source": "148 SMs x 4 schedulers x one issue per clock at the sampled SM clock",
+                          "instructions_source": "profiles/wtowers_instructions.json (ncu smsp__inst_executed.sum, "
+                                                 "128-station case scaled by work units; not this run)",
+                          "kernels": {}}
+        for k in ("tower_rows", "romein", "fft_cols_backward", "prepare"):
+            if k in idoc and k in kernel_stages:
+                rate = idoc[k]["warp_instructions"] / (kernel_stages[k] * 1e-3) / 1e12
+                issue_roofline["kernels"][k] = {"achieved": rate, "frac": rate / issue_peak,
+                                                "warp_instructions_per_launch": idoc[k]["warp_instructions"],
+                                                "launch_ms": kernel_stages[k]}
     line = {
         "impl": "b200", "metric": METRIC, "value": value, "unit": "vis/s", "n_gpus": world,
         "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step,
@@ -538,6 +561,7 @@ def run_b200(args, rank, world, local_rank):
                           "dense_equivalent_gbs": dense_bytes / (ms_per_step * 1e-3) / 1e9,
                           "dense_equivalent_frac": dense_bytes / (ms_per_step * 1e-3) / 1e9 / peak},
         "compute_roofline": compute_roofline,
+        "issue_roofline": issue_roofline,
         "step_ms_min_median_max": [round(min(step_ms), 4), round(statistics.median(step_ms), 4),
                                    round(max(step_ms), 4)],
         "stage_ms": {k: round(statistics.mean(v), 4) for k, v in stage_ms.items()},
