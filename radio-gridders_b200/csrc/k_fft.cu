@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(256) fft32_rows_kernel(float2 *__restrict__ da
 #pragma unroll
             for (int n2 = 0; n2 < 32; n2++) a[n2] = make_float2(0.f, 0.f);
         }
-        reg_fft<32, SIGN>(a);
+        reg_fft_dif<32, SIGN>(a);
 #pragma unroll
         for (int j = 0; j < 32; j++) {
             const int k2 = bitrevc(j, 5);
@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(256) fft32_rows_kernel(float2 *__restrict__ da
         float2 b[N1];
 #pragma unroll
         for (int n1 = 0; n1 < N1; n1++) b[n1] = T[(r * N1 + n1) * kPad + k2];
-        reg_fft<N1, SIGN>(b);
+        reg_fft_dif<N1, SIGN>(b);
         if (row < rows) {
             float2 *dst = data + row * N + k2;
 #pragma unroll
@@ -142,7 +142,7 @@ __device__ __forceinline__ void col_step1(const float2 *__restrict__ src, int ld
 #pragma unroll
             for (int n2 = 0; n2 < 32; n2++) dst[(int64_t)(n1 + n2 * N1) * ld + c] = make_float2(0.f, 0.f);
         }
-        reg_fft<32, SIGN>(a);
+        reg_fft_dif<32, SIGN>(a);
 #pragma unroll
         for (int j = 0; j < 32; j++) {
             const int k2 = bitrevc(j, 5);
@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(256) fft32_cols_kernel(float2 *__restrict__ da
         float2 b[N1];
 #pragma unroll
         for (int n1 = 0; n1 < N1; n1++) b[n1] = T[c * G::CS + n1 * kPad + k2];
-        reg_fft<N1, SIGN>(b);
+        reg_fft_dif<N1, SIGN>(b);
 #pragma unroll
         for (int j = 0; j < N1; j++) base[(int64_t)(k2 + 32 * bitrevc(j, G::LB)) * N + c] = b[j];
     }

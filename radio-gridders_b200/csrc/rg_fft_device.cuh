@@ -4,9 +4,9 @@
 // four-step method): 32-point transforms in registers over the stride-N1
 // subsequences, a twiddle multiply W_N^(n1 k2), an exchange through shared
 // memory, and N1-point transforms in registers.  Register transforms are
-// radix-2 decimation-in-frequency with compile-time indices, so all data stays
-// in registers; outputs come out in bit-reversed order and are stored to their
-// natural positions.  Twiddles are FP64-computed values rounded to FP32.
+// radix-2 with compile-time indices, so all data stays in registers; outputs
+// come out in bit-reversed order and are stored to their natural positions.
+// Twiddles are FP64-computed values rounded to FP32.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -58,10 +58,41 @@ __device__ __forceinline__ float2 cmulf(float2 a, float2 b)
 
 __device__ __forceinline__ float2 caddf(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 
-// In-register radix-2 DIF transform of N <= 32 points, sign SIGN (-1 forward,
+// exp(-2 pi i k / 32), k = 1..15 except 8, as scale x (1 + i ratio) when
+// |cos| >= |sin| (scale = cos, ratio = tan) or scale x (ratio + i) otherwise
+// (scale = sin, ratio = cot): |ratio| <= 1.  FP64-evaluated, rounded to FP32;
+// compile-time k only.
+struct TanTwiddle {
+    float scale, ratio;
+    bool cot;
+};
+__device__ __forceinline__ TanTwiddle tw32_tan(int k)
+{
+    switch (k) {
+        case 1: return {0.9807852506637573f, -0.1989123672246933f, false};
+        case 2: return {0.9238795042037964f, -0.4142135679721832f, false};
+        case 3: return {0.8314695954322815f, -0.6681786179542542f, false};
+        case 4: return {0.7071067690849304f, -1.0f, false};
+        case 5: return {-0.8314695954322815f, -0.6681786179542542f, true};
+        case 6: return {-0.9238795042037964f, -0.4142135679721832f, true};
+        case 7: return {-0.9807852506637573f, -0.1989123672246933f, true};
+        case 9: return {-0.9807852506637573f, 0.1989123672246933f, true};
+        case 10: return {-0.9238795042037964f, 0.4142135679721832f, true};
+        case 11: return {-0.8314695954322815f, 0.6681786179542542f, true};
+        case 12: return {-0.7071067690849304f, 1.0f, true};
+        case 13: return {-0.8314695954322815f, 0.6681786179542542f, false};
+        case 14: return {-0.9238795042037964f, 0.4142135679721832f, false};
+        case 15: return {-0.9807852506637573f, 0.1989123672246933f, false};
+        default: return {1.0f, 0.0f, false};
+    }
+}
+
+// In-register radix-2 transforms of N <= 32 points, sign SIGN (-1 forward,
 // +1 backward), unnormalised.  On return a[j] = X[bitrev(j)].
+//
+// reg_fft_dif: decimation in frequency, twiddles as complex multiplies.
 template <int N, int SIGN>
-__device__ __forceinline__ void reg_fft(float2 (&a)[N])
+__device__ __forceinline__ void reg_fft_dif(float2 (&a)[N])
 {
 #pragma unroll
     for (int span = N / 2; span >= 1; span >>= 1) {
@@ -83,6 +114,56 @@ __device__ __forceinline__ void reg_fft(float2 (&a)[N])
                         if (SIGN > 0) t.y = -t.y;
                         a[g + j + span] = cmulf(d, t);
                     }
+                }
+            }
+        }
+    }
+}
+
+// reg_fft: decimation in time over the view v[i] = a[bitrev(i)] (x in bit-reversed
+// order, so v ends in natural order, which is a[j] = X[bitrev(j)]); the view
+// is compile-time register renaming.  A twiddled butterfly x +- w y with
+// w = scale (1 + i ratio) takes u = y (1 + i ratio) in two fused multiply-adds
+// and x +- scale u in four (six instructions instead of a complex multiply's
+// four and the two complex additions' four; the tangent form of Goedecker,
+// SIAM J. Sci. Comput. 18 (1997), for multiply-add units).  It holds about ten
+// more registers than reg_fft_dif: the kernels whose occupancy those
+// registers would cut (the batched row and column transforms) keep the DIF
+// form, the sub-grid stages take this one (3 % off the row stage).
+template <int N, int SIGN>
+__device__ __forceinline__ void reg_fft(float2 (&a)[N])
+{
+    constexpr int LB = ilog2c(N);
+#pragma unroll
+    for (int span = 1; span < N; span <<= 1) {
+#pragma unroll
+        for (int g = 0; g < N; g += 2 * span) {
+#pragma unroll
+            for (int j = 0; j < span; j++) {
+                const int p = bitrevc(g + j, LB), q = bitrevc(g + j + span, LB);
+                const float2 x = a[p], y = a[q];
+                const int k = j * (32 / (2 * span));  // w = exp(SIGN 2 pi i k / 32)
+                if (k == 0) {
+                    a[p] = make_float2(x.x + y.x, x.y + y.y);
+                    a[q] = make_float2(x.x - y.x, x.y - y.y);
+                } else if (k == 8) {  // w = -+ i
+                    const float2 wy = SIGN < 0 ? make_float2(y.y, -y.x) : make_float2(-y.y, y.x);
+                    a[p] = make_float2(x.x + wy.x, x.y + wy.y);
+                    a[q] = make_float2(x.x - wy.x, x.y - wy.y);
+                } else {
+                    const TanTwiddle t = tw32_tan(k);
+                    const float c = t.scale, r = t.ratio;
+                    // u = y (1 + i r) or y (r + i); SIGN > 0 takes the conjugates,
+                    // y (1 - i r) or y (r - i)
+                    float2 u;
+                    if (!t.cot)
+                        u = SIGN < 0 ? make_float2(fmaf(-r, y.y, y.x), fmaf(r, y.x, y.y))
+                                     : make_float2(fmaf(r, y.y, y.x), fmaf(-r, y.x, y.y));
+                    else
+                        u = SIGN < 0 ? make_float2(fmaf(r, y.x, -y.y), fmaf(r, y.y, y.x))
+                                     : make_float2(fmaf(r, y.x, y.y), fmaf(r, y.y, -y.x));
+                    a[p] = make_float2(fmaf(c, u.x, x.x), fmaf(c, u.y, x.y));
+                    a[q] = make_float2(fmaf(-c, u.x, x.x), fmaf(-c, u.y, x.y));
                 }
             }
         }
