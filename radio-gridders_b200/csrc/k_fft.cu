@@ -490,9 +490,10 @@ __global__ void __launch_bounds__(kRowThreads) tower_rows_kernel(
                     const int k = (int)(mwp * P[r * N + col]);
                     float sn, cs;
                     __sincosf(__int2float_rn(k) * (6.28318530717958647f / 4294967296.f), &sn, &cs);
-                    // acc += b * (cs + i sn), two fused multiply-adds per component
-                    acc[q][j].x = fmaf(b[j].x, cs, fmaf(-b[j].y, sn, acc[q][j].x));
-                    acc[q][j].y = fmaf(b[j].x, sn, fmaf(b[j].y, cs, acc[q][j].y));
+                    // acc += b * (cs + i sn) as two packed-pair fused multiply-adds
+                    // (acc + b.x (cs, sn)) + b.y (-sn, cs)
+                    acc[q][j] = __ffma2_rn(make_float2(b[j].x, b[j].x), make_float2(cs, sn), acc[q][j]);
+                    acc[q][j] = __ffma2_rn(make_float2(b[j].y, b[j].y), make_float2(-sn, cs), acc[q][j]);
                 }
             }
         }

@@ -9,7 +9,9 @@
 // 8-byte vector atomic) when the point or the (tower, floor) sub-grid changes,
 // so visibilities that move slowly along a baseline track coalesce in
 // registers.  Per tap: sum += vis * conj(tap), the reference's
-// grid += v * conj(wk) (src/reference/grid.c:177-182).
+// grid += v * conj(wk) (src/reference/grid.c:177-182), as two packed-pair
+// fused multiply-adds: sum + tap.y (vis.y, -vis.x) + tap.x (vis.x, vis.y),
+// the same roundings as the scalar form.
 //
 // Sub-grids of the W-towers pass (STRIP): the linear index grid_offset + cv *
 // side + cu is the reference's grid_offset + y*size + x (grid.c:177-182),
@@ -98,14 +100,15 @@ __global__ void __launch_bounds__(K *K / P, (RomeinBounds<K, P>::min_ctas)) rome
                     for (int p = 0; p < P; p++) t[p] = __ldg(taps + r.z + ((cv0 + p * RS) & (K - 1)) * K + cu);
                 }
                 const float2 vz = svis[j];
+                const float2 vzr = make_float2(vz.y, -vz.x);
                 // in a sub-grid goff alone fixes the origin (its columns span
                 // chunk + 1 < S values), hence the residues
                 if (r.x == cur_bin && r.y == cur_goff && (STRIP || r.w == cur_res)) {
                     // same sub-grid and footprint origin: every point unchanged
 #pragma unroll
                     for (int p = 0; p < P; p++) {
-                        sum[p].x = fmaf(vz.x, t[p].x, fmaf(vz.y, t[p].y, sum[p].x));
-                        sum[p].y = fmaf(vz.y, t[p].x, fmaf(-vz.x, t[p].y, sum[p].y));
+                        sum[p] = __ffma2_rn(make_float2(t[p].y, t[p].y), vzr, sum[p]);
+                        sum[p] = __ffma2_rn(make_float2(t[p].x, t[p].x), vz, sum[p]);
                     }
                     continue;
                 }
@@ -154,8 +157,8 @@ __global__ void __launch_bounds__(K *K / P, (RomeinBounds<K, P>::min_ctas)) rome
                         cur_key[p] = key[p];
                         sum[p] = make_float2(0.f, 0.f);
                     }
-                    sum[p].x = fmaf(vz.x, t[p].x, fmaf(vz.y, t[p].y, sum[p].x));
-                    sum[p].y = fmaf(vz.y, t[p].x, fmaf(-vz.x, t[p].y, sum[p].y));
+                    sum[p] = __ffma2_rn(make_float2(t[p].y, t[p].y), vzr, sum[p]);
+                    sum[p] = __ffma2_rn(make_float2(t[p].x, t[p].x), vz, sum[p]);
                 }
             }
         }

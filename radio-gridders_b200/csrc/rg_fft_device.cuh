@@ -124,12 +124,15 @@ __device__ __forceinline__ void reg_fft_dif(float2 (&a)[N])
 // order, so v ends in natural order, which is a[j] = X[bitrev(j)]); the view
 // is compile-time register renaming.  A twiddled butterfly x +- w y with
 // w = scale (1 + i ratio) takes u = y (1 + i ratio) in two fused multiply-adds
-// and x +- scale u in four (six instructions instead of a complex multiply's
-// four and the two complex additions' four; the tangent form of Goedecker,
-// SIAM J. Sci. Comput. 18 (1997), for multiply-add units).  It holds about ten
-// more registers than reg_fft_dif: the kernels whose occupancy those
-// registers would cut (the batched row and column transforms) keep the DIF
-// form, the sub-grid stages take this one (3 % off the row stage).
+// and x +- scale u in two more on packed FP32 pairs (the tangent form of
+// Goedecker, SIAM J. Sci. Comput. 18 (1997), for multiply-add units); an
+// untwiddled one is one packed add and one packed multiply-add by -1 (exact).
+// Four instructions per twiddled butterfly and two per untwiddled one, against
+// eight and four for complex multiplies and scalar additions, with the same
+// results as their scalar forms.  It holds about ten more registers than
+// reg_fft_dif: the kernels whose occupancy those registers would cut (the
+// batched row and column transforms) keep the DIF form, the sub-grid stages
+// take this one.
 template <int N, int SIGN>
 __device__ __forceinline__ void reg_fft(float2 (&a)[N])
 {
@@ -143,9 +146,9 @@ __device__ __forceinline__ void reg_fft(float2 (&a)[N])
                 const int p = bitrevc(g + j, LB), q = bitrevc(g + j + span, LB);
                 const float2 x = a[p], y = a[q];
                 const int k = j * (32 / (2 * span));  // w = exp(SIGN 2 pi i k / 32)
-                if (k == 0) {
-                    a[p] = make_float2(x.x + y.x, x.y + y.y);
-                    a[q] = make_float2(x.x - y.x, x.y - y.y);
+                if (k == 0) {  // x + y, x - y = y (-1) + x
+                    a[p] = __fadd2_rn(x, y);
+                    a[q] = __ffma2_rn(y, make_float2(-1.f, -1.f), x);
                 } else if (k == 8) {  // w = -+ i
                     const float2 wy = SIGN < 0 ? make_float2(y.y, -y.x) : make_float2(-y.y, y.x);
                     a[p] = make_float2(x.x + wy.x, x.y + wy.y);
@@ -162,8 +165,8 @@ __device__ __forceinline__ void reg_fft(float2 (&a)[N])
                     else
                         u = SIGN < 0 ? make_float2(fmaf(r, y.x, -y.y), fmaf(r, y.y, y.x))
                                      : make_float2(fmaf(r, y.x, y.y), fmaf(r, y.y, -y.x));
-                    a[p] = make_float2(fmaf(c, u.x, x.x), fmaf(c, u.y, x.y));
-                    a[q] = make_float2(fmaf(-c, u.x, x.x), fmaf(-c, u.y, x.y));
+                    a[p] = __ffma2_rn(make_float2(c, c), u, x);
+                    a[q] = __ffma2_rn(make_float2(-c, -c), u, x);
                 }
             }
         }
