@@ -430,9 +430,15 @@ __global__ void __launch_bounds__(kRowThreads) tower_rows_kernel(
 #pragma unroll
         for (int j = 0; j < N1; j++) acc[q][j] = make_float2(0.f, 0.f);
 
+    // the next floor's strip mask is loaded a floor ahead, so only the strip
+    // loads wait on memory at the top of a floor
+    unsigned mnext = (threadIdx.x < G::WORDS && begin < end) ? masks[(int64_t)begin * G::WORDS + threadIdx.x] : 0u;
     for (int slot = begin; slot < end; slot++) {
         const uint32_t mwp = (uint32_t)(-(wp_min + bin_of_slot[slot] % nfloor));  // two's complement
-        if (threadIdx.x < G::WORDS) smask[threadIdx.x] = masks[(int64_t)slot * G::WORDS + threadIdx.x];
+        if (threadIdx.x < G::WORDS) {
+            smask[threadIdx.x] = mnext;
+            if (slot + 1 < end) mnext = masks[(int64_t)(slot + 1) * G::WORDS + threadIdx.x];
+        }
         __syncthreads();  // masks visible; the previous floor's step 2 is done with T
         // the slot's strip mask in two 64-bit registers (at most 128 strips)
         const unsigned long long m_lo = smask[0] | (G::WORDS > 1 ? (unsigned long long)smask[1] << 32 : 0ull);
