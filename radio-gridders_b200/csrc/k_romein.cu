@@ -47,10 +47,13 @@ struct RomeinBounds {
     static constexpr int min_ctas = want > 32 ? 32 : (want < 1 ? 1 : want);
 };
 
-template <int K, int P, bool STRIP>
+// F64 (row-major grids only): taps are read from the caller's FP64 table and
+// rounded to FP32 as they are loaded, exactly as the table conversion rounds
+// them, for calls whose taps are fewer than the table's entries.
+template <int K, int P, bool STRIP, bool F64 = false>
 __global__ void __launch_bounds__(K *K / P, (RomeinBounds<K, P>::min_ctas)) romein_kernel(
     const int4 *__restrict__ rec, const float2 *__restrict__ visf, int64_t n,
-    const float2 *__restrict__ taps, float2 *__restrict__ grids,
+    const float2 *__restrict__ taps, const double2 *__restrict__ taps64, float2 *__restrict__ grids,
     const int *__restrict__ slot_of_bin, int64_t grid_stride, int side, int64_t chunk, int slot_cap, int strip_lg)
 {
     constexpr int NT = K * K / P;     // threads
@@ -95,6 +98,12 @@ __global__ void __launch_bounds__(K *K / P, (RomeinBounds<K, P>::min_ctas)) rome
                     const float2 *tp = taps + 2 * (int64_t)r.z + cv0 * K + cu;
 #pragma unroll
                     for (int p = 0; p < P; p++) t[p] = __ldg(tp + p * RS * K);
+                } else if (F64) {
+#pragma unroll
+                    for (int p = 0; p < P; p++) {
+                        const double2 d = __ldg(taps64 + r.z + ((cv0 + p * RS) & (K - 1)) * K + cu);
+                        t[p] = make_float2((float)d.x, (float)d.y);
+                    }
                 } else {
 #pragma unroll
                     for (int p = 0; p < P; p++) t[p] = __ldg(taps + r.z + ((cv0 + p * RS) & (K - 1)) * K + cu);
@@ -172,38 +181,46 @@ __global__ void __launch_bounds__(K *K / P, (RomeinBounds<K, P>::min_ctas)) rome
 
 template <int K, int P>
 static void romein_launch(cudaStream_t s, const int4 *rec, const float2 *visf, int64_t n, const float2 *taps,
-                          float2 *grids, const int *slot_of_bin, int64_t grid_stride, int grid_side, int sm_count,
-                          int slot_cap, int strip_lg)
+                          const double2 *taps64, float2 *grids, const int *slot_of_bin, int64_t grid_stride,
+                          int grid_side, int sm_count, int slot_cap, int strip_lg)
 {
     // Every CTA resident at once, each with an equal contiguous run of
     // visibilities: occupancy, not the chunk size, decides the grid.
     constexpr int NT = K * K / P;
-    int per_sm = 0;  // of the instantiation that runs (the two register counts can differ)
+    int per_sm = 0;  // of the instantiation that runs (the register counts can differ)
     if (strip_lg)
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, romein_kernel<K, P, true>, NT, 0);
+    else if (taps64)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, romein_kernel<K, P, false, true>, NT, 0);
     else
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, romein_kernel<K, P, false>, NT, 0);
     if (per_sm < 1) per_sm = 1;
     int64_t blocks = (int64_t)sm_count * per_sm;
     int64_t chunk = (n + blocks - 1) / blocks;
-    if (chunk < 32) chunk = 32;
+    if (chunk < 8) chunk = 8;
     blocks = (n + chunk - 1) / chunk;
     if (blocks < 1) blocks = 1;
     if (strip_lg)
-        romein_kernel<K, P, true><<<(unsigned)blocks, NT, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin, grid_stride,
-                                                                  grid_side, chunk, slot_cap, strip_lg);
+        romein_kernel<K, P, true><<<(unsigned)blocks, NT, 0, s>>>(rec, visf, n, taps, nullptr, grids, slot_of_bin,
+                                                                  grid_stride, grid_side, chunk, slot_cap, strip_lg);
+    else if (taps64)
+        romein_kernel<K, P, false, true><<<(unsigned)blocks, NT, 0, s>>>(rec, visf, n, nullptr, taps64, grids,
+                                                                         slot_of_bin, grid_stride, grid_side, chunk,
+                                                                         slot_cap, 0);
     else
-        romein_kernel<K, P, false><<<(unsigned)blocks, NT, 0, s>>>(rec, visf, n, taps, grids, slot_of_bin,
+        romein_kernel<K, P, false><<<(unsigned)blocks, NT, 0, s>>>(rec, visf, n, taps, nullptr, grids, slot_of_bin,
                                                                    grid_stride, grid_side, chunk, slot_cap, 0);
 }
 
 void launch_romein(cudaStream_t s, const int4 *rec, const float2 *visf, int64_t n,
                    const float2 *taps, float2 *grids, const int *slot_of_bin, int64_t grid_stride,
-                   int grid_side, int ksize, int sm_count, int slot_cap, int points, int strip_lg)
+                   int grid_side, int ksize, int sm_count, int slot_cap, int points, int strip_lg,
+                   const double2 *taps64)
 {
+    if (strip_lg) taps64 = nullptr;  // sub-grids always read the converted, duplicated table
 #define RG_ROMEIN(K, P) \
-    romein_launch<K, P>(s, rec, visf, n, taps, grids, slot_of_bin, grid_stride, grid_side, sm_count, slot_cap, \
-                        strip_lg)
+    romein_launch<K, P>(s, rec, visf, n, taps, taps64, grids, slot_of_bin, grid_stride, grid_side, sm_count, \
+                        slot_cap, strip_lg)
     switch (ksize) {
         case 4: RG_ROMEIN(4, 1); break;
         case 8:

@@ -404,8 +404,21 @@ rg_status rg_grid_wprojection(rg_context *ctx, double *uvgrid, int grid_size, do
     DevVis dv;
     begin_stage(ctx, "stage_in");
     RG_CHECK(stage_vis(ctx, vis, &dv));
-    float2 *taps;
-    RG_CHECK(stage_taps(ctx, wkern, &taps));
+    // Gridding reads K^2 taps per visibility.  When those are fewer bytes
+    // (16 per FP64 tap) than converting the whole table moves (its FP64 read
+    // and FP32 write, 24 per entry), the gridder reads the FP64 table itself
+    // and rounds each tap as the conversion would.
+    float2 *taps = nullptr;
+    const double2 *taps64 = nullptr;
+    const int64_t ntaps =
+        (int64_t)wkern->plane_count * wkern->oversampling * wkern->oversampling * wkern->size * wkern->size;
+    if ((double)vis->n * wkern->size * wkern->size * 16.0 < 24.0 * (double)ntaps) {
+        const void *src;
+        RG_CHECK(stage_in(ctx, wkern->data, sizeof(double2) * ntaps, "in_wkern", &src));
+        taps64 = (const double2 *)src;
+    } else {
+        RG_CHECK(stage_taps(ctx, wkern, &taps));
+    }
     end_stage(ctx);
     Diag d;
     RG_CHECK(diag_begin(ctx, &d));
@@ -424,7 +437,7 @@ rg_status rg_grid_wprojection(rg_context *ctx, double *uvgrid, int grid_size, do
         end_stage(ctx);
         begin_stage(ctx, "romein");
         launch_romein(ctx->stream, (const int4 *)rec, (const float2 *)visf, dv.n, taps,
-                      (float2 *)grid32, (const int *)zero_slot, 0, N, wkern->size, ctx->sm_count);
+                      (float2 *)grid32, (const int *)zero_slot, 0, N, wkern->size, ctx->sm_count, 1, 0, 0, taps64);
         end_stage(ctx);
         ctx->launches += 2;
         RG_CHECK(check_launch("W-projection gridding"));

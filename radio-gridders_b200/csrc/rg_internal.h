@@ -282,10 +282,12 @@ void launch_compact_bins(cudaStream_t s, const int *active, const int *range, in
 // caller detects it from the slot count and reruns).
 // points: grid points per thread (0: the default for ksize).  strip_lg = 0:
 // row-major grids; otherwise log2(grid_side) and strip-major sub-grids.
+// taps64 (row-major grids only; taps unused then): the FP64 table itself, each
+// tap rounded to FP32 as it is loaded.
 void launch_romein(cudaStream_t s, const int4 *rec, const float2 *visf, int64_t n,
                    const float2 *taps, float2 *grids, const int *slot_of_bin,
                    int64_t grid_stride, int grid_side, int ksize, int sm_count, int slot_cap = 1,
-                   int points = 0, int strip_lg = 0);
+                   int points = 0, int strip_lg = 0, const double2 *taps64 = nullptr);
 
 // k_towers.cu
 void launch_fresnel_table(cudaStream_t s, uint32_t *phq, int subgrid, double theta, double winc);

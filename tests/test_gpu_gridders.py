@@ -57,6 +57,25 @@ def test_wprojection_vs_oracle(rg, ctx, sim, oracle, wproj_data, ksize, ov):
     assert rel_rms(g, ref) < TOL
 
 
+def test_wprojection_fp64_and_converted_taps(rg, ctx, sim, oracle, wproj_data):
+    """A call with fewer taps to read than its table holds reads the FP64
+    table directly; a larger one converts the table to FP32 first.  The same
+    visibilities sent twice take the second path; the grid must be twice the
+    first call's, and both must match the oracle."""
+    obs, u, v, w, vis = wproj_data
+    n, th = obs.meta["grid_size"], obs.meta["theta"]
+    wk = sim.wkernel_for(w, th, 10.0, size=16, oversampling=8)
+    ntaps = wk.plane_count * wk.oversampling ** 2 * wk.size ** 2
+    assert len(u) * 16 * 16 * 16 < 24 * ntaps <= 2 * len(u) * 16 * 16 * 16  # one call each side
+    g1 = np.zeros((n, n), np.complex128)
+    ctx.grid_wprojection(g1, n, th, V(rg, u, v, w, vis), wk)
+    dup = lambda a: np.ascontiguousarray(np.concatenate([a, a]))
+    g2 = np.zeros((n, n), np.complex128)
+    ctx.grid_wprojection(g2, n, th, V(rg, dup(u), dup(v), dup(w), dup(vis)), wk)
+    assert rel_rms(g2, 2 * g1) < 1e-6
+    assert rel_rms(g1, oracle.grid_wprojection(n, th, u, v, w, vis, wk)) < TOL
+
+
 @pytest.mark.parametrize("sub,margin,winc", [(128, 16, 10.0), (64, 16, 10.0), (256, 32, 20.0),
                                              (512, 16, 10.0), (128, 24, 3.0)])
 def test_wtowers_vs_oracle(rg, ctx, sim, oracle, wproj_data, sub, margin, winc):
