@@ -324,7 +324,8 @@ __global__ void __launch_bounds__(kSparseColThreads) sparse_cols_kernel(
 // ---------------------------------------------------------------------------
 // Row stage, in two kernels so uneven towers balance.
 //
-// tower_rows_kernel: CTA = (floor group, strip of R rows).  For each floor of
+// tower_rows_kernel: CTA = (floor group, R rows: four mirror pairs (y, N - y)
+// when R = 8, so each Fresnel factor serves two rows; else a strip).  For each floor of
 // the group: backward row transform of the column-transformed sub-grid (only
 // the slot's marked strips are read, then zeroed), times exp(-2 pi i wp
 // ph(l, m)) with ph = winc (1 - sqrt(1 - l^2 - m^2)) — the reference's
@@ -416,13 +417,27 @@ __global__ void __launch_bounds__(kRowThreads) tower_rows_kernel(
     uint32_t *P = reinterpret_cast<uint32_t *>(W + N);  // [R][N] Fresnel phase of the strip (turns, 2^-32)
     __shared__ unsigned smask[G::WORDS];
     const int rstrips = N / R;
-    const int group = blockIdx.x / rstrips, row0 = (blockIdx.x % rstrips) * R;
+    const int group = blockIdx.x / rstrips, blk = blockIdx.x % rstrips;
     if (group >= counts[1]) return;  // groups live on the device; grid sized for capacity
+    // MIRROR: the CTA's rows are four mirror pairs (y, N - y) — pair p is
+    // (p, N - p), pair 0 is (0, N/2) — local rows 0-3 the first rows and 4-7
+    // their mirrors.  ph(l, m) depends on m^2 only and the table's rows y and
+    // N - y hold the same values, so a thread's two step-2 items (the same
+    // column, rows r and r + 4) share each Fresnel factor, except in pair 0.
+    constexpr bool MIRROR = R == 8 && G::PER == 2 && G::ITEMS2 == 2 * kRowThreads;
+    auto row_of = [&](int r) -> int {
+        if constexpr (!MIRROR) {
+            return blk * R + r;
+        } else {
+            const int p = 4 * blk + (r & 3);
+            return r < 4 ? p : (p == 0 ? N / 2 : N - p);
+        }
+    };
     const int wp_min = range[0], nfloor = range[1];
     const int begin = group_begin[group];
     const int end = group_end[group] < slot_cap ? group_end[group] : slot_cap;
     load_twiddles<N1>(W, tw);
-    for (int e = threadIdx.x; e < R * N; e += blockDim.x) P[e] = phq[(int64_t)row0 * N + e];
+    for (int e = threadIdx.x; e < R * N; e += blockDim.x) P[e] = phq[(int64_t)row_of(e / N) * N + e % N];
 
     float2 acc[G::PER][N1];
 #pragma unroll
@@ -449,7 +464,7 @@ __global__ void __launch_bounds__(kRowThreads) tower_rows_kernel(
             // strip-major sub-grid: column col of row (row0 + r) at (col/8)*8N + row*8 + col%8;
             // for N1 >= 8 element n2 lies n2 * (N1/8) strips after the thread's first,
             // a compile-time offset from one per-thread base
-            float2 *row_base = slots + (int64_t)slot * N * N + (row0 + r) * kStripCols;
+            float2 *row_base = slots + (int64_t)slot * N * N + row_of(r) * kStripCols;
             float2 *src = row_base + (n1 / kStripCols) * (kStripCols * N) + n1 % kStripCols;
             auto elem = [&](int n2) -> float2 * {
                 if constexpr (N1 >= kStripCols) {
@@ -478,40 +493,77 @@ __global__ void __launch_bounds__(kRowThreads) tower_rows_kernel(
             }
         }
         __syncthreads();
+        // -wp ph modulo one turn as a signed 32-bit fraction of a turn, rounded
+        // to 24 significant bits by the conversion (at most 64 units of 2^-32,
+        // 2^-26 turns, off); acc += b * (cs + i sn) as two packed-pair fused
+        // multiply-adds, (acc + b.x (cs, sn)) + b.y (-sn, cs)
+        auto fresnel = [&](uint32_t phase, float &sn, float &cs) {
+            const int k = (int)(mwp * phase);
+            __sincosf(__int2float_rn(k) * (6.28318530717958647f / 4294967296.f), &sn, &cs);
+        };
+        auto accumulate = [&](float2 &a, float2 v, float sn, float cs) {
+            a = __ffma2_rn(make_float2(v.x, v.x), make_float2(cs, sn), a);
+            a = __ffma2_rn(make_float2(v.y, v.y), make_float2(-sn, cs), a);
+        };
+        if constexpr (MIRROR) {
+            const int k2 = threadIdx.x % 32, r = threadIdx.x / 32;  // items (k2, r) and (k2, r + 4)
+            float2 b0[N1], b1[N1];
 #pragma unroll
-        for (int q = 0; q < G::PER; q++) {
-            const int it = threadIdx.x + q * kRowThreads;
-            if (it < G::ITEMS2) {
-                const int k2 = it % 32, r = it / 32;
-                float2 b[N1];
-#pragma unroll
-                for (int n1 = 0; n1 < N1; n1++) b[n1] = T[(r * N1 + n1) * kPad + k2];
-                reg_fft<N1, +1>(b);
+            for (int n1 = 0; n1 < N1; n1++) {
+                b0[n1] = T[(r * N1 + n1) * kPad + k2];
+                b1[n1] = T[((r + 4) * N1 + n1) * kPad + k2];
+            }
+            reg_fft<N1, +1>(b0);
+            reg_fft<N1, +1>(b1);
+            if (blk != 0 || r != 0) {  // a mirror pair: one factor for both rows
 #pragma unroll
                 for (int j = 0; j < N1; j++) {
                     const int col = k2 + 32 * bitrevc(j, G::LB);
-                    // -wp ph modulo one turn as a signed 32-bit fraction of a turn,
-                    // rounded to 24 significant bits by the conversion (at most
-                    // 64 units of 2^-32, 2^-26 turns, off)
-                    const int k = (int)(mwp * P[r * N + col]);
                     float sn, cs;
-                    __sincosf(__int2float_rn(k) * (6.28318530717958647f / 4294967296.f), &sn, &cs);
-                    // acc += b * (cs + i sn) as two packed-pair fused multiply-adds
-                    // (acc + b.x (cs, sn)) + b.y (-sn, cs)
-                    acc[q][j] = __ffma2_rn(make_float2(b[j].x, b[j].x), make_float2(cs, sn), acc[q][j]);
-                    acc[q][j] = __ffma2_rn(make_float2(b[j].y, b[j].y), make_float2(-sn, cs), acc[q][j]);
+                    fresnel(P[r * N + col], sn, cs);
+                    accumulate(acc[0][j], b0[j], sn, cs);
+                    accumulate(acc[1][j], b1[j], sn, cs);
+                }
+            } else {  // pair 0: rows 0 and N/2
+#pragma unroll
+                for (int j = 0; j < N1; j++) {
+                    const int col = k2 + 32 * bitrevc(j, G::LB);
+                    float sn, cs;
+                    fresnel(P[r * N + col], sn, cs);
+                    accumulate(acc[0][j], b0[j], sn, cs);
+                    fresnel(P[(r + 4) * N + col], sn, cs);
+                    accumulate(acc[1][j], b1[j], sn, cs);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < G::PER; q++) {
+                const int it = threadIdx.x + q * kRowThreads;
+                if (it < G::ITEMS2) {
+                    const int k2 = it % 32, r = it / 32;
+                    float2 b[N1];
+#pragma unroll
+                    for (int n1 = 0; n1 < N1; n1++) b[n1] = T[(r * N1 + n1) * kPad + k2];
+                    reg_fft<N1, +1>(b);
+#pragma unroll
+                    for (int j = 0; j < N1; j++) {
+                        float sn, cs;
+                        fresnel(P[r * N + k2 + 32 * bitrevc(j, G::LB)], sn, cs);
+                        accumulate(acc[q][j], b[j], sn, cs);
+                    }
                 }
             }
         }
     }
-    float2 *out = partial + ((int64_t)group * N + row0) * N;
+    float2 *out = partial + (int64_t)group * N * N;
 #pragma unroll
     for (int q = 0; q < G::PER; q++) {
         const int it = threadIdx.x + q * kRowThreads;
         if (it < G::ITEMS2) {
             const int k2 = it % 32, r = it / 32;
+            float2 *o = out + (int64_t)row_of(r) * N + k2;
 #pragma unroll
-            for (int j = 0; j < N1; j++) out[(int64_t)r * N + k2 + 32 * bitrevc(j, G::LB)] = acc[q][j];
+            for (int j = 0; j < N1; j++) o[32 * bitrevc(j, G::LB)] = acc[q][j];
         }
     }
 }
