@@ -132,10 +132,19 @@ __global__ void __launch_bounds__(K *K / P, (RomeinBounds<K, P>::min_ctas)) rome
                     const int col = base & (side - 1);
                     const int colpart = ((col >> 3) << (strip_lg + 3)) + (col & 7);
                     const int rowb = base >> strip_lg;
+                    if (rowb >= 0 && rowb + K <= side) {
+                        // every footprint row inside: the thread's row offsets cv0 + p RS
+                        // (mod K) rise by RS and wrap once, at p = pw
+                        const int key0 = colpart + ((rowb + cv0) << 3);
+                        const int pw = (K - cv0 + RS - 1) / RS;
 #pragma unroll
-                    for (int p = 0; p < P; p++) {
-                        const int row = rowb + ((cv0 + p * RS) & (K - 1));
-                        key[p] = (unsigned)row < (unsigned)side ? colpart + (row << 3) : -1;
+                        for (int p = 0; p < P; p++) key[p] = key0 + ((p * RS) << 3) - (p >= pw ? (K << 3) : 0);
+                    } else {
+#pragma unroll
+                        for (int p = 0; p < P; p++) {
+                            const int row = rowb + ((cv0 + p * RS) & (K - 1));
+                            key[p] = (unsigned)row < (unsigned)side ? colpart + (row << 3) : -1;
+                        }
                     }
                 } else {
                     // per-axis check; -1 (never flushed) for a tap off the grid
